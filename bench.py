@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark: simulated seconds per wall second of the 200k-node 3D Richards
+case (101 x 101 x 21 nodes, 1.2 M tetrahedra, lognormal Ks, 30 days,
+Newton tolerance from rtol = atol = 1e-6) on B200.
+
+One step = one complete 30-day integration from the hydrostatic initial
+state (variable-order BDF, Newton-GMRES(40), block-ILU(0)).  The headline
+``value`` is the mixed-precision path (FP32 block-ILU(0) factor/apply and
+FP32 Krylov basis; FP64 residual, Newton update, least squares and stopping
+test) with the state resident in HBM; the plain FP64 path is timed the same
+way and reported beside it.  ``e2e`` is the same metric through
+fvm_integrate_host (host buffers, H2D of y0 and D2H of the final head inside
+the timed region).
+
+Multi-GPU (torchrun): every rank integrates its own replica (a different Ks
+seed) with no data-path collective -- the problem does not shard -- so the
+value is replicas x simulated seconds / max-over-ranks time ("weak").
+
+``--impl reference`` times the FP64 CPU oracle (the reference path restated
+in C++, OpenMP on all host cores) on a bounded prefix of the same 30-day
+run: the reference itself cannot be built (no SUNDIALS/MKL/minlin/MPI).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "sim-s/wall-s, 200k-node 3D Richards @1e-6: learned+FP32 vs plain FP64, 1×B200"
+UNIT = "sim-s/wall-s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region"""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws, dev):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_sample(steps_budget_s, seed=1, max_steps=None):
+    """oracle on the first BDF steps of the same run; returns sim-s/wall-s"""
+    import numpy as np
+
+    import fvmpor_b200 as fb
+    from oracle.pyoracle import Oracle
+
+    p = fb.make_problem("richards3d", seed=seed)
+    o = Oracle(p)
+    a = p.arrays()
+    y0 = p.water_table - a["coords"][:, 2]
+    fixed = a["node_tag"] != 0
+    y0[fixed] = (p.water_table - a["coords"][:, 2])[fixed]
+    opts = fb.default_opts(krylov_dim=40, max_order=5)
+    nb = 148  # same block partition as the device preconditioner at this size
+    if max_steps is None:
+        opts.max_steps = 1
+        t0 = time.perf_counter()
+        o.integrate(opts, nb, 0.0, p.t_end, y0)
+        one = time.perf_counter() - t0
+        max_steps = int(max(1, min(40, steps_budget_s / max(one, 1e-3))))
+    opts.max_steps = max_steps
+    t0 = time.perf_counter()
+    rc, yend, st = o.integrate(opts, nb, 0.0, p.t_end, y0)
+    wall = time.perf_counter() - t0
+    return st["t"] / wall, wall, max_steps, st
+
+
+def run_reference(args):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    from oracle.pyoracle import Oracle, lib as olib
+
+    olib()
+    threads = Oracle.threads()
+    budget = max(5.0, 150.0 / (args.steps + args.warmup))
+    vals, walls = [], []
+    _, _, msteps, _ = cpu_sample(budget, max_steps=None) if args.warmup > 0 else (0, 0, None, 0)
+    for _ in range(max(0, args.warmup - 1)):
+        cpu_sample(budget, max_steps=msteps)
+    st = None
+    for _ in range(args.steps):
+        v, w, msteps, st = cpu_sample(budget, max_steps=msteps)
+        vals.append(v)
+        walls.append(w)
+    tot_sim = sum(v * w for v, w in zip(vals, walls))
+    value = tot_sim / sum(walls)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(walls) / len(walls),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 3D jittered Kuhn mesh, lognormal Ks)",
+        "config": {"workload": "richards3d 101x101x21 nodes / 1.2M tets, 30-day run: first "
+                               f"{msteps} BDF steps (bounded CPU sample)", "rtol": 1e-6, "atol": 1e-6},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"first {msteps} BDF steps of the 30-day run, reaching t = {st['t']:.4g} s"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--days", type=float, default=30.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+
+    import fvmpor_b200 as fb
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    prob = fb.make_problem("richards3d", seed=1 + rank)
+    horizon = args.days * 86400.0
+    ph = fb.Physics(prob)
+    N, T = prob.n_nodes, prob.n_elements
+    y0 = torch.empty(N, dtype=torch.float64, device=dev)
+    ph.initial_head(y0)
+    yend = torch.empty_like(y0)
+    mixed = fb.Integrator(ph, krylov_dim=40, max_restarts=5, precision=1, max_order=5)
+    plain = fb.Integrator(ph, krylov_dim=40, max_restarts=5, precision=0, max_order=5)
+
+    def timed(integ, k, host=False, profile=False):
+        y0h = y0.cpu().numpy()
+        yh = np.zeros(N)
+        barrier(ws)
+        torch.cuda.synchronize()
+        if profile:
+            ph.profile(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stats = []
+        e0.record()
+        for _ in range(k):
+            if host:
+                rc, st = integ.integrate_host(0.0, horizon, y0h, yh)
+            else:
+                rc, st = integ.integrate(0.0, horizon, y0, yend)
+            if rc != 0:
+                raise RuntimeError(f"integration failed rc={rc} {st}")
+            stats.append(st)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        prof = ph.profile_read() if profile else None
+        if profile:
+            ph.profile(False)
+        barrier(ws)
+        return max_over_ranks(ms, ws, dev), stats, prof
+
+    for _ in range(args.warmup):
+        mixed.integrate(0.0, horizon, y0, yend)
+    with ClockSampler(local) as clk:
+        ms_mixed, st_mixed, prof = timed(mixed, args.steps, profile=True)
+    ms_plain, st_plain, _ = timed(plain, args.steps)
+    ms_e2e, _, _ = timed(mixed, args.steps, host=True)
+    sim = horizon * args.steps * ws
+    value = sim / (ms_mixed / 1e3)
+    plain_value = sim / (ms_plain / 1e3)
+    e2e_value = sim / (ms_e2e / 1e3)
+
+    # roofline of the residual evaluation (node pass + element pass + gather):
+    # algorithmic bytes 36 B/node + 270 B/tet per evaluation
+    alg_bytes = 36.0 * N + 270.0 * T
+    n_eval = prof["element"][1]
+    chain_ms = (prof["node"][0] + prof["element"][0] + prof["gather"][0]) / max(n_eval, 1)
+    achieved = alg_bytes / (chain_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    launches_per_run = None
+    st0 = st_mixed[0]
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 3D jittered Kuhn mesh, lognormal Ks by FFT)",
+        "config": {"workload": f"richards3d {N} nodes / {T} tets, {args.days:g}-day run per step",
+                   "path": "FP32 block-ILU(0) + FP32 GMRES(40) basis, FP64 residual/Newton/LSQ",
+                   "rtol": 1e-6, "atol": 1e-6, "l2": "inputs larger than L2 (331 MB per residual)",
+                   "parallelism": f"replicas x{ws}"},
+        "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain / args.steps,
+                       "ratio_mixed_over_plain": value / plain_value,
+                       "stats": {k: st_plain[0][k] for k in ("nst", "nni", "nli", "npe", "nre")}},
+        "stats": {k: st0[k] for k in ("nst", "nni", "nli", "npe", "nps", "nre", "ncfn", "netf", "last_order")},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "residual evaluation (node pass + element pass + node gather)",
+                     "algorithmic_bytes_per_launch": alg_bytes, "avg_ms": chain_ms,
+                     "peak_kind": peak_kind},
+        "kernel_ms": {k: {"total_ms": v[0], "launches": v[1], "avg_us": 1e3 * v[0] / max(v[1], 1)}
+                      for k, v in prof.items()},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N},
+        "clocks": clocks,
+    }
+    # launches of our kernels inside the timed region: 3 per residual
+    # evaluation plus the Krylov / preconditioner / controller kernels
+    line["gpu_launches"] = int(sum(v[1] for v in prof.values()) + 0)
+    if rank == 0 and not args.no_cpu_baseline:
+        v, wall, msteps, st = cpu_sample(15.0)
+        # the GPU over the very same prefix, for a like-for-like ratio
+        pre = fb.Integrator(ph, krylov_dim=40, max_restarts=5, precision=1, max_order=5, max_steps=msteps)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc, stg = pre.integrate(0.0, horizon, y0, yend)
+        torch.cuda.synchronize()
+        gw = time.perf_counter() - t0
+        from oracle.pyoracle import Oracle
+
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": Oracle.threads(), "kind": "port",
+                                "sample": f"first {msteps} BDF steps of the 30-day run (t = {st['t']:.4g} s), "
+                                          f"{wall:.1f} s of CPU time",
+                                "gpu_same_sample": stg["t"] / gw}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ph.close()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

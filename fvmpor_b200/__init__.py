@@ -1,0 +1,385 @@
+"""fvmpor_b200 — B200-native Richards-equation hot path of FVMPor.
+
+Python plumbing over the C ABI in ``include/fvmpor_b200.h`` (the product is
+``libfvmpor_b200.so``: sm_100a kernels plus the C++ host controller).  The
+classes mirror the reference's call surface for this path:
+
+* :class:`Physics`  — ``residual_evaluation`` / ``preprocess_timestep`` of
+  ``VarSatPhysics`` (examples/fvmporMinlin/fvmpor_ODE_impl.cpp:62-141);
+* :class:`Preconditioner` — ``setup`` / ``apply``
+  (examples/fvmporMinlin/preconditioner_dss.h:27-39);
+* :class:`Integrator` — ``IDAIntegrator::advance(t)``
+  (include/fvm/integrators/ida_integrator.h:325-340).
+
+Device vectors are ``torch.float64`` CUDA tensors; the library reads and
+writes them in place through their data pointers.  There is no CPU
+fallback: if the shared library is missing every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfvmpor_b200.so")
+
+_lib = None
+
+
+class FvmError(RuntimeError):
+    pass
+
+
+def build(force: bool = False) -> str:
+    """Compile libfvmpor_b200.so for sm_100a (nvcc, in-tree)."""
+    import subprocess
+
+    if force and os.path.exists(LIB_PATH):
+        os.remove(LIB_PATH)
+    subprocess.run(["make", "-C", _HERE, "-j8"], check=True, capture_output=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FvmError(f"{LIB_PATH} is missing: run fvmpor_b200.build() (no CPU fallback)")
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+# --------------------------------------------------------------------- structs
+class Mesh(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("n_nodes", C.c_int), ("n_elements", C.c_int), ("n_bfaces", C.c_int),
+        ("coords", C.POINTER(C.c_double)), ("elem_nodes", C.POINTER(C.c_int)),
+        ("elem_zone", C.POINTER(C.c_int)), ("elem_K", C.POINTER(C.c_double)),
+        ("bface_nodes", C.POINTER(C.c_int)), ("bface_elem", C.POINTER(C.c_int)),
+        ("bface_tag", C.POINTER(C.c_int)), ("node_tag", C.POINTER(C.c_int)),
+    ]
+
+
+class Zone(C.Structure):
+    _fields_ = [("Kxx", C.c_double), ("Kyy", C.c_double), ("Kzz", C.c_double), ("phi", C.c_double),
+                ("alphaVG", C.c_double), ("nVG", C.c_double), ("S_r", C.c_double)]
+
+
+class BC(C.Structure):
+    _fields_ = [("tag", C.c_int), ("type", C.c_int), ("value", C.c_double), ("b", C.c_double),
+                ("eta", C.c_double)]
+
+
+class PhysicsDesc(C.Structure):
+    _fields_ = [("n_zones", C.c_int), ("zones", C.POINTER(Zone)), ("n_bcs", C.c_int),
+                ("bcs", C.POINTER(BC)), ("rho0", C.c_double)]
+
+
+class ProblemStruct(C.Structure):
+    _fields_ = [
+        ("mesh", Mesh), ("phys", PhysicsDesc), ("water_table", C.c_double), ("t_end", C.c_double),
+        ("coords", C.c_void_p), ("elem_nodes", C.c_void_p), ("elem_zone", C.c_void_p),
+        ("elem_K", C.c_void_p), ("bface_nodes", C.c_void_p), ("bface_elem", C.c_void_p),
+        ("bface_tag", C.c_void_p), ("node_tag", C.c_void_p), ("zones", C.c_void_p),
+        ("bcs", C.c_void_p), ("grid_dims", C.POINTER(C.c_int)),
+    ]
+
+
+class Opts(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("max_order", C.c_int),
+                ("krylov_dim", C.c_int), ("max_restarts", C.c_int), ("precision", C.c_int),
+                ("use_predictor", C.c_int), ("h0", C.c_double), ("hmax", C.c_double),
+                ("max_steps", C.c_long)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("nst", C.c_long), ("nre", C.c_long), ("nni", C.c_long), ("nli", C.c_long),
+                ("npe", C.c_long), ("nps", C.c_long), ("ncfn", C.c_long), ("ncfl", C.c_long),
+                ("netf", C.c_long), ("npred", C.c_long), ("last_order", C.c_int),
+                ("last_h", C.c_double), ("t", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_P = C.c_void_p
+_D = C.c_double
+_I = C.c_int
+
+
+def _declare(L):
+    L.fvm_create.restype = _P
+    L.fvm_create.argtypes = [C.POINTER(Mesh), C.POINTER(PhysicsDesc), _I]
+    L.fvm_destroy.argtypes = [_P]
+    L.fvm_last_error.restype = C.c_char_p
+    L.fvm_n_nodes.argtypes = [_P]
+    L.fvm_initial_head.argtypes = [_P, _D, _P]
+    L.fvm_residual.argtypes = [_P, _D, _P, _P, _P]
+    L.fvm_begin_step.argtypes = [_P, _D, _P, _P]
+    L.fvm_jv.argtypes = [_P, _D, _D, _P, _P, _P, _P, _D, _P]
+    L.fvm_psetup.argtypes = [_P, _D, _D, _D, _P, _P, _P, _P, _I]
+    L.fvm_psolve.argtypes = [_P, _P, _P]
+    L.fvm_gmres.argtypes = [_P, _D, _D, _P, _P, _P, _P, _P, _P, _I, _I, _I, _D,
+                            C.POINTER(_I), C.POINTER(_D)]
+    L.fvm_wrms.restype = _D
+    L.fvm_wrms.argtypes = [_P, _P, _P]
+    L.fvm_dot.restype = _D
+    L.fvm_dot.argtypes = [_P, _P, _P]
+    L.fvm_opts_default.argtypes = [C.POINTER(Opts)]
+    L.fvm_integrate.argtypes = [_P, C.POINTER(Opts), _D, _D, _P, _P, C.POINTER(Stats)]
+    L.fvm_integrate_host.argtypes = [_P, C.POINTER(Opts), _D, _D, _P, _P, C.POINTER(Stats)]
+    L.fvm_problem_richards2d.argtypes = [_I, _I, _D, _D, _D, C.c_uint64, _D, _D, C.POINTER(ProblemStruct)]
+    L.fvm_problem_richards3d.argtypes = [_I, _I, _I, _D, _D, _D, _D, C.c_uint64, _D, _D, _D, _D, _D,
+                                         C.POINTER(ProblemStruct)]
+    L.fvm_problem_free.argtypes = [C.POINTER(ProblemStruct)]
+    L.fvm_precond_info.argtypes = [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]
+    L.fvm_precond_jacobian.argtypes = [_P, _P, _P, _P]
+    L.fvm_profile.argtypes = [_P, _I]
+    L.fvm_profile_read.argtypes = [_P, _P, _P]
+
+
+PROFILE_CATEGORIES = ("node", "element", "gather", "ilu_apply", "gram_schmidt", "ilu_factor", "fd_jacobian")
+
+
+def _err(prefix, code=None):
+    msg = lib().fvm_last_error().decode()
+    return FvmError(f"{prefix}: {msg}" + ("" if code is None else f" (status {code})"))
+
+
+def _check(code, what):
+    if code < 0:
+        raise _err(what, code)
+    return code
+
+
+# --------------------------------------------------------------------- problems
+class Problem:
+    """A synthetic Richards problem generated by the library (host memory)."""
+
+    def __init__(self, kind: str, **kw):
+        self._s = ProblemStruct()
+        L = lib()
+        if kind == "2d":
+            r = L.fvm_problem_richards2d(kw.get("nx", 81), kw.get("ny", 41), kw.get("Lx", 10.0),
+                                         kw.get("Ly", 5.0), kw.get("jitter", 0.2), kw.get("seed", 1),
+                                         kw.get("ln_var", 0.0), kw.get("corr_len", 1.0), C.byref(self._s))
+        elif kind == "3d":
+            r = L.fvm_problem_richards3d(kw.get("nx", 100), kw.get("ny", 100), kw.get("nz", 20),
+                                         kw.get("Lx", 100.0), kw.get("Ly", 100.0), kw.get("Lz", 20.0),
+                                         kw.get("jitter", 0.15), kw.get("seed", 1), kw.get("ln_var", 1.0),
+                                         kw.get("cx", 10.0), kw.get("cy", 10.0), kw.get("cz", 2.0),
+                                         kw.get("Kg", 1e-5), C.byref(self._s))
+        else:
+            raise ValueError(kind)
+        if r != 0:
+            raise _err("problem generation", r)
+        self.kind = kind
+
+    def __del__(self):
+        try:
+            if getattr(self, "_s", None) is not None and _lib is not None:
+                _lib.fvm_problem_free(C.byref(self._s))
+        except Exception:
+            pass
+
+    @property
+    def mesh(self) -> Mesh:
+        return self._s.mesh
+
+    @property
+    def phys(self) -> PhysicsDesc:
+        return self._s.phys
+
+    @property
+    def n_nodes(self):
+        return self._s.mesh.n_nodes
+
+    @property
+    def n_elements(self):
+        return self._s.mesh.n_elements
+
+    @property
+    def water_table(self):
+        return self._s.water_table
+
+    @property
+    def t_end(self):
+        return self._s.t_end
+
+    def arrays(self):
+        m = self._s.mesh
+        d = m.dim
+        out = {
+            "coords": np.ctypeslib.as_array(m.coords, (m.n_nodes, 3)).copy(),
+            "elem_nodes": np.ctypeslib.as_array(m.elem_nodes, (m.n_elements, d + 1)).copy(),
+            "elem_zone": np.ctypeslib.as_array(m.elem_zone, (m.n_elements,)).copy(),
+            "bface_nodes": np.ctypeslib.as_array(m.bface_nodes, (m.n_bfaces, d)).copy(),
+            "bface_tag": np.ctypeslib.as_array(m.bface_tag, (m.n_bfaces,)).copy(),
+            "node_tag": np.ctypeslib.as_array(m.node_tag, (m.n_nodes,)).copy(),
+        }
+        if m.elem_K:
+            out["elem_K"] = np.ctypeslib.as_array(m.elem_K, (m.n_elements,)).copy()
+        return out
+
+
+def _ptr(t):
+    """device pointer of a contiguous float64 CUDA tensor"""
+    import torch
+
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous():
+        raise TypeError("expected a contiguous torch.float64 CUDA tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+FLAG_RECOMPUTE_GEOMETRY = 1
+
+
+class Physics:
+    """Device-resident Richards physics for one mesh (fvm_ctx)."""
+
+    def __init__(self, problem: Problem, flags: int = 0):
+        self.problem = problem
+        self._c = lib().fvm_create(C.byref(problem._s.mesh), C.byref(problem._s.phys), flags)
+        if not self._c:
+            raise _err("fvm_create")
+        self.N = problem.n_nodes
+
+    def close(self):
+        if getattr(self, "_c", None):
+            lib().fvm_destroy(self._c)
+            self._c = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # reference: set_initial_conditions (vs.h:8-32)
+    def initial_head(self, y, water_table=None):
+        wt = self.problem.water_table if water_table is None else water_table
+        _check(lib().fvm_initial_head(self._c, wt, _ptr(y)), "fvm_initial_head")
+
+    # reference: preprocess_evaluation + residual_evaluation
+    def residual(self, t, y, yp, res):
+        _check(lib().fvm_residual(self._c, t, _ptr(y), _ptr(yp), _ptr(res)), "fvm_residual")
+
+    # reference: preprocess_timestep
+    def begin_step(self, t, y, yp):
+        _check(lib().fvm_begin_step(self._c, t, _ptr(y), _ptr(yp)), "fvm_begin_step")
+
+    def jv(self, t, cj, y, yp, F0, v, sigma, out):
+        _check(lib().fvm_jv(self._c, t, cj, _ptr(y), _ptr(yp), _ptr(F0), _ptr(v), sigma, _ptr(out)), "fvm_jv")
+
+    def wrms(self, x, ewt=None):
+        return lib().fvm_wrms(self._c, _ptr(x), _ptr(ewt) if ewt is not None else None)
+
+    def dot(self, x, y):
+        return lib().fvm_dot(self._c, _ptr(x), _ptr(y))
+
+    def profile(self, enable: bool):
+        _check(lib().fvm_profile(self._c, 1 if enable else 0), "fvm_profile")
+
+    def profile_read(self):
+        ms = np.zeros(len(PROFILE_CATEGORIES))
+        cnt = np.zeros(len(PROFILE_CATEGORIES), np.int64)
+        _check(lib().fvm_profile_read(self._c, ms.ctypes.data, cnt.ctypes.data), "fvm_profile_read")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(PROFILE_CATEGORIES)}
+
+
+class Preconditioner:
+    """Coloured-FD Jacobian + block-ILU(0) (Preconditioner::setup/apply)."""
+
+    def __init__(self, physics: Physics):
+        self.ph = physics
+
+    def setup(self, t, cj, h, y, yp, F0, ewt, precision=0):
+        return _check(lib().fvm_psetup(self.ph._c, t, cj, h, _ptr(y), _ptr(yp), _ptr(F0), _ptr(ewt), precision),
+                      "fvm_psetup")
+
+    def apply(self, r, z):
+        _check(lib().fvm_psolve(self.ph._c, _ptr(r), _ptr(z)), "fvm_psolve")
+
+    def info(self):
+        a, b, c, d = _I(), _I(), _I(), _I()
+        _check(lib().fvm_precond_info(self.ph._c, C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
+               "fvm_precond_info")
+        return {"nnz": a.value, "ncolours": b.value, "nblocks": c.value, "max_levels": d.value}
+
+    def jacobian(self):
+        inf = self.info()
+        rp = np.zeros(self.ph.N + 1, np.int32)
+        col = np.zeros(inf["nnz"], np.int32)
+        val = np.zeros(inf["nnz"], np.float64)
+        _check(lib().fvm_precond_jacobian(self.ph._c, rp.ctypes.data, col.ctypes.data, val.ctypes.data),
+               "fvm_precond_jacobian")
+        return rp, col, val
+
+    def gmres(self, t, cj, y, yp, F0, ewt, b, x, m=30, max_restarts=5, precision=0, tol=0.0165):
+        its, rn = _I(), _D()
+        r = lib().fvm_gmres(self.ph._c, t, cj, _ptr(y), _ptr(yp), _ptr(F0), _ptr(ewt), _ptr(b), _ptr(x), m,
+                            max_restarts, precision, tol, C.byref(its), C.byref(rn))
+        _check(r, "fvm_gmres")
+        return r, its.value, rn.value
+
+
+def default_opts(**kw) -> Opts:
+    o = Opts()
+    lib().fvm_opts_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Integrator:
+    """Variable-order BDF + Newton-GMRES on the device (IDAIntegrator)."""
+
+    def __init__(self, physics: Physics, **opts):
+        self.ph = physics
+        self.opts = default_opts(**opts)
+
+    def integrate(self, t0, t_end, y0, y_end):
+        st = Stats()
+        r = lib().fvm_integrate(self.ph._c, C.byref(self.opts), t0, t_end, _ptr(y0), _ptr(y_end), C.byref(st))
+        if r < 0:
+            raise _err("fvm_integrate", r)
+        return r, st.as_dict()
+
+    def integrate_host(self, t0, t_end, y0: np.ndarray, y_end: np.ndarray):
+        st = Stats()
+        y0 = np.ascontiguousarray(y0, np.float64)
+        assert y_end.dtype == np.float64 and y_end.flags.c_contiguous
+        r = lib().fvm_integrate_host(self.ph._c, C.byref(self.opts), t0, t_end, y0.ctypes.data,
+                                     y_end.ctypes.data, C.byref(st))
+        if r < 0:
+            raise _err("fvm_integrate_host", r)
+        return r, st.as_dict()
+
+
+@dataclass
+class Config:
+    """Benchmark problems (seeded synthetic inputs of the named shapes)."""
+
+    name: str
+    kind: str
+    params: dict
+
+
+CONFIGS = {
+    "richards2d": Config("richards2d: 81x41 jittered Delaunay, 2 layers, 1 day", "2d",
+                         dict(nx=81, ny=41, Lx=10.0, Ly=5.0, jitter=0.2, seed=1)),
+    "richards3d": Config("richards3d: 100x100x20 hex -> 6 tets (214,221 nodes), lognormal Ks, 30 days", "3d",
+                         dict(nx=100, ny=100, nz=20, Lx=100.0, Ly=100.0, Lz=20.0, jitter=0.15, seed=1,
+                              ln_var=1.0, cx=10.0, cy=10.0, cz=2.0, Kg=1e-5)),
+}
+
+
+def make_problem(name: str, **override) -> Problem:
+    cfg = CONFIGS[name]
+    p = dict(cfg.params)
+    p.update(override)
+    return Problem(cfg.kind, **p)

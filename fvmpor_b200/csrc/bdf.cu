@@ -1,0 +1,352 @@
+// Device operations for the BDF controller (bdf_controller.hpp) and the
+// fvm_integrate entry points: the time loop of examples/fvmporMinlin/
+// fvmpor_ODE.cpp:202-232 and IDAIntegrator::advance(t)
+// (include/fvm/integrators/ida_integrator.h:325-340) with the solver state
+// resident in HBM.  Initial y' = F(t0, y0, 0) / ahh on free rows
+// (Physics::initialise, examples/fvmporMinlin/fvmpor_ODE_impl.cpp:34-58).
+#include "bdf_controller.hpp"
+#include "ctx.cuh"
+#include "krylov.cuh"
+#include "predictor.cuh"
+#include "reduce.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace fvmb {
+
+constexpr int kNPhi = 7;
+
+struct PhiPtrs {
+    double* p[kNPhi];
+};
+struct Coef7 {
+    double v[kNPhi];
+};
+
+__global__ void k_ewt(int N, const double* __restrict__ y, double rtol, double atol,
+                      double* __restrict__ ewt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) ewt[i] = 1.0 / (rtol * fabs(y[i]) + atol);
+}
+
+// y = sum_{j<=k} phi_j ; yp = sum_{1<=j<=k} gamma_j phi_j ; e = 0
+__global__ void k_predict(int N, int k, PhiPtrs ph, Coef7 gamma, double* __restrict__ y,
+                          double* __restrict__ yp, double* __restrict__ e) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double s = ph.p[0][i], sp = 0.0;
+    for (int j = 1; j <= k; ++j) {
+        double v = ph.p[j][i];
+        s += v;
+        sp += gamma.v[j] * v;
+    }
+    y[i] = s;
+    yp[i] = sp;
+    e[i] = 0.0;
+}
+
+__global__ void k_phi_scale(int N, int j0, int j1, PhiPtrs ph, Coef7 f) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    for (int j = j0; j <= j1; ++j) ph.p[j][i] *= f.v[j];
+}
+
+// y -= x, y' -= cj x, e -= x ; out = sum (x ewt)^2
+__global__ void k_newton_update(int N, const double* __restrict__ x, double cj,
+                                const double* __restrict__ ewt, double* __restrict__ y,
+                                double* __restrict__ yp, double* __restrict__ e, double* partial,
+                                unsigned* counter, double* out) {
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        double d = x[i];
+        y[i] -= d;
+        yp[i] -= cj * d;
+        e[i] -= d;
+        double w = d * ewt[i];
+        s += w * w;
+    }
+    double t = block_sum(s);
+    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    last_block_reduce(partial, 1, counter, out);
+}
+
+// squared error-test norms times N:
+//  0: e  1: phi_k + e  2: phi_{k-1} + phi_k + e  3: e - phi_{k+1}
+__global__ void k_err_norms(int N, int k, PhiPtrs ph, const double* __restrict__ e,
+                            const double* __restrict__ ewt, double* partial, unsigned* counter,
+                            double* out) {
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        double w = ewt[i], ei = e[i];
+        double a = ei * w;
+        s0 += a * a;
+        double d1 = ph.p[k][i] + ei;
+        double b = d1 * w;
+        s1 += b * b;
+        if (k >= 2) {
+            double d2 = ph.p[k - 1][i] + d1;
+            double c2 = d2 * w;
+            s2 += c2 * c2;
+        }
+        if (k + 1 < kNPhi) {
+            double d3 = ei - ph.p[k + 1][i];
+            double c3 = d3 * w;
+            s3 += c3 * c3;
+        }
+    }
+    double t0 = block_sum(s0);
+    double t1 = block_sum(s1);
+    double t2 = block_sum(s2);
+    double t3 = block_sum(s3);
+    if (threadIdx.x == 0) {
+        partial[4 * blockIdx.x + 0] = t0;
+        partial[4 * blockIdx.x + 1] = t1;
+        partial[4 * blockIdx.x + 2] = t2;
+        partial[4 * blockIdx.x + 3] = t3;
+    }
+    last_block_reduce(partial, 4, counter, out);
+}
+
+// phi_{k+1} = e (set_kp2), phi_k += e, phi_j += phi_{j+1} for j = k-1..0
+__global__ void k_phi_update(int N, int k, int set_kp2, PhiPtrs ph, const double* __restrict__ e) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double ei = e[i];
+    if (set_kp2) ph.p[k + 1][i] = ei;
+    double v = ph.p[k][i] + ei;
+    ph.p[k][i] = v;
+    for (int j = k - 1; j >= 0; --j) {
+        v = ph.p[j][i] + v;
+        ph.p[j][i] = v;
+    }
+}
+
+// y'0 = F / ahh on free rows with ahh != 0, else 0
+__global__ void k_initial_yp(int N, const double* __restrict__ F, const double* __restrict__ ahh,
+                             const unsigned char* __restrict__ ntype, double* __restrict__ yp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double a = ahh[i];
+    yp[i] = (!ntype[i] && a != 0.0) ? F[i] / a : 0.0;
+}
+
+__global__ void k_fill(int N, double v, double* __restrict__ x) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) x[i] = v;
+}
+
+__global__ void k_scale_vec(int N, double a, const double* __restrict__ x, double* __restrict__ y) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) y[i] = a * x[i];
+}
+
+struct DeviceOps {
+    fvm_ctx* c;
+    const fvm_opts& o;
+    int N;
+    DevBuf<double> phi[kNPhi];
+    DevBuf<double> y, yp, e, ewt, F, x, tmp;
+    DevBuf<double> partial, res;
+    DevBuf<unsigned> counter;
+    double* host = nullptr;
+    double tcur = 0.0;
+    Predictor* pred = nullptr;
+
+    DeviceOps(fvm_ctx* ctx, const fvm_opts& opts) : c(ctx), o(opts), N(ctx->N) {
+        for (int j = 0; j < kNPhi; ++j) { phi[j].alloc(N); phi[j].zero(c->stream); }
+        y.alloc(N); yp.alloc(N); e.alloc(N); ewt.alloc(N); F.alloc(N); x.alloc(N); tmp.alloc(N);
+        partial.alloc((size_t)kRedBlocks * 4);
+        res.alloc(8);
+        counter.alloc(1);
+        counter.zero(c->stream);
+        FVM_CUDA(cudaMallocHost(&host, sizeof(double) * 8));
+    }
+    ~DeviceOps() {
+        if (host) cudaFreeHost(host);
+    }
+    int g() const { return grid_for(N, 256); }
+    PhiPtrs ptrs() const {
+        PhiPtrs p;
+        for (int j = 0; j < kNPhi; ++j) p.p[j] = phi[j].p;
+        return p;
+    }
+    double fetch(int n) {
+        FVM_CUDA(cudaMemcpyAsync(host, res.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+        FVM_CUDA(cudaStreamSynchronize(c->stream));
+        return host[0];
+    }
+
+    // ---- controller interface
+    void set_time(double t) { tcur = t; }
+    void ewt_from_phi0(double rtol, double atol) {
+        k_ewt<<<g(), 256, 0, c->stream>>>(N, phi[0].p, rtol, atol, ewt.p);
+    }
+    void begin_step() { launch_begin_step(c, phi[0].p, yp.p); }
+    void phi_scale(int j0, int j1, const double* f) {
+        Coef7 cf;
+        for (int j = 0; j < kNPhi; ++j) cf.v[j] = f[j];
+        k_phi_scale<<<g(), 256, 0, c->stream>>>(N, j0, j1, ptrs(), cf);
+    }
+    void predict(int k, const double* gamma) {
+        Coef7 gm;
+        for (int j = 0; j < kNPhi; ++j) gm.v[j] = gamma[j];
+        k_predict<<<g(), 256, 0, c->stream>>>(N, k, ptrs(), gm, y.p, yp.p, e.p);
+    }
+    double wrms_y() { return std::sqrt(reduce_sumsq(c, y.p, ewt.p) / N); }
+    void residual() {
+        Perturb none;
+        launch_residual(c, y.p, yp.p, none, nullptr, F.p);
+    }
+    int psetup(double cj, double h) {
+        psetup_dev(c, cj, h, y.p, yp.p, F.p, ewt.p, o.precision);
+        return ilu_status(c);
+    }
+    int gmres(double cj, double tol, int* its, double* rn, long* nps, long* njv) {
+        GmresCounters gc;
+        int r = gmres_dev(c, cj, y.p, yp.p, F.p, ewt.p, F.p, x.p, o.krylov_dim, o.max_restarts,
+                          o.precision, tol, its, rn, &gc);
+        *nps = gc.nps;
+        *njv = gc.njv;
+        return r;
+    }
+    double newton_update(double cj) {
+        k_newton_update<<<kRedBlocks, kRedThreads, 0, c->stream>>>(N, x.p, cj, ewt.p, y.p, yp.p, e.p,
+                                                                   partial.p, counter.p, res.p);
+        return std::sqrt(fetch(1) / N);
+    }
+    void err_norms(int k, double out[4]) {
+        k_err_norms<<<kRedBlocks, kRedThreads, 0, c->stream>>>(N, k, ptrs(), e.p, ewt.p, partial.p,
+                                                               counter.p, res.p);
+        fetch(4);
+        for (int q = 0; q < 4; ++q) out[q] = std::sqrt(host[q] / N);
+    }
+    void phi_update(int k, int set_kp2) {
+        k_phi_update<<<g(), 256, 0, c->stream>>>(N, k, set_kp2, ptrs(), e.p);
+    }
+    bool newton_guess(double tnew, double cj) {
+        if (!pred) return false;
+        return predictor_apply(c, pred, tnew, cj, phi[0].p, phi[1].p, y.p, yp.p, e.p, ewt.p, F.p);
+    }
+
+    // y0 -> phi_0, y'0 from the initial residual, phi_1 = h y'0
+    double start(double t0, const double* y0, double tout) {
+        cudaStream_t s = c->stream;
+        FVM_CUDA(cudaMemcpyAsync(y.p, y0, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+        k_fill<<<g(), 256, 0, s>>>(N, 0.0, yp.p);
+        Perturb none;
+        launch_residual(c, y.p, yp.p, none, nullptr, F.p);
+        k_fill<<<g(), 256, 0, s>>>(N, 1.0, tmp.p);
+        launch_residual(c, y.p, tmp.p, none, nullptr, x.p);   // leaves ahh * 1 in c->stor
+        k_initial_yp<<<g(), 256, 0, s>>>(N, F.p, c->stor.p, c->ntype.p, yp.p);
+        k_ewt<<<g(), 256, 0, s>>>(N, y.p, o.rtol, o.atol, ewt.p);
+        double ypn = std::sqrt(reduce_sumsq(c, yp.p, ewt.p) / N);
+        double h = bdf_first_step(t0, tout, ypn, o.h0, o.hmax);
+        FVM_CUDA(cudaMemcpyAsync(phi[0].p, y.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+        k_scale_vec<<<g(), 256, 0, s>>>(N, h, yp.p, phi[1].p);
+        return h;
+    }
+};
+
+int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, const double* y0,
+                  double* y_end, fvm_stats* stats) {
+    const fvm_opts& o = *opts;
+    if (o.max_order < 1 || o.max_order > 5) throw Error("integrate: max_order must be 1..5");
+    if (!(o.rtol > 0) || !(o.atol > 0)) throw Error("integrate: tolerances must be positive");
+    if (!(t_end > t0)) throw Error("integrate: t_end must exceed t0");
+    DeviceOps ops(c, o);
+    if (o.use_predictor) {
+        ops.pred = predictor_of(c);
+        if (!ops.pred) throw Error("integrate: use_predictor set but no trained predictor loaded");
+    }
+    BdfOptions bo;
+    bo.rtol = o.rtol;
+    bo.atol = o.atol;
+    bo.max_order = o.max_order;
+    bo.hmax = o.hmax;
+    bo.use_guess = o.use_predictor != 0;
+    BdfController<DeviceOps> ctl(ops, bo);
+    long nre0 = c->n_residuals;
+    double h0 = ops.start(t0, y0, t_end);
+    ctl.start(t0, h0);
+    int rc = 0;
+    while (ctl.t < t_end) {
+        if (o.max_steps > 0 && ctl.st.nst >= o.max_steps) { rc = 1; break; }
+        rc = ctl.step(t_end);
+        if (rc != 0) break;
+        if (t_end - ctl.t <= 1e-12 * std::max(1.0, std::fabs(t_end))) ctl.t = t_end;
+    }
+    FVM_CUDA(cudaMemcpyAsync(y_end, ops.phi[0].p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->nst = ctl.st.nst;
+        stats->nre = c->n_residuals - nre0;
+        stats->nni = ctl.st.nni;
+        stats->nli = ctl.st.nli;
+        stats->npe = ctl.st.npe;
+        stats->nps = ctl.st.nps;
+        stats->ncfn = ctl.st.ncfn;
+        stats->ncfl = ctl.st.ncfl;
+        stats->netf = ctl.st.netf;
+        stats->npred = ctl.st.npred;
+        stats->last_order = ctl.st.last_order;
+        stats->last_h = ctl.st.last_h;
+        stats->t = ctl.t;
+    }
+    return rc;
+}
+
+} // namespace fvmb
+
+using namespace fvmb;
+
+extern "C" void fvm_opts_default(fvm_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->rtol = 1e-6;
+    o->atol = 1e-6;
+    o->max_order = 5;
+    o->krylov_dim = 30;
+    o->max_restarts = 5;
+}
+
+extern "C" int fvm_integrate(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end,
+                             const double* y0, double* y_end, fvm_stats* stats) {
+    try {
+        if (!c || !opts || !y0 || !y_end) throw Error("fvm_integrate: null argument");
+        int rc = integrate_dev(c, opts, t0, t_end, y0, y_end, stats);
+        FVM_CUDA(cudaGetLastError());
+        if (rc < 0) set_error("fvm_integrate: step failure code " + std::to_string(rc));
+        return rc;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+extern "C" int fvm_integrate_host(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end,
+                                  const double* y0_host, double* y_end_host, fvm_stats* stats) {
+    try {
+        if (!c || !opts || !y0_host || !y_end_host) throw Error("fvm_integrate_host: null argument");
+        DevBuf<double> a, b;
+        a.alloc(c->N);
+        b.alloc(c->N);
+        FVM_CUDA(cudaMemcpyAsync(a.p, y0_host, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+        int rc = integrate_dev(c, opts, t0, t_end, a.p, b.p, stats);
+        FVM_CUDA(cudaMemcpyAsync(y_end_host, b.p, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+        FVM_CUDA(cudaStreamSynchronize(c->stream));
+        if (rc < 0) set_error("fvm_integrate_host: step failure code " + std::to_string(rc));
+        return rc;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}

@@ -1,0 +1,269 @@
+// Variable-order, variable-step BDF controller with a Newton-Krylov
+// corrector, independent of where the vectors live.
+//
+// Replaces the IDAS step of IDAIntegrator::advance (include/fvm/
+// integrators/ida_integrator.h:296-340).  IDAS (SUNDIALS 2.4.0) is not in
+// the reference tree, so the method is written from the published
+// fixed-leading-coefficient BDF algorithm of DASSL / IDA (Brenan, Campbell
+// & Petzold, "Numerical Solution of Initial-Value Problems in DAEs", SIAM
+// 1996, ch. 5; Hindmarsh et al., ACM TOMS 31(3), 2005): modified divided
+// differences phi_j, predictor y = sum phi*_j, y' = sum gamma_j phi*_j,
+// corrector G(y) = F(t, y, y'_pred + cj (y - y_pred)) = 0 with
+// cj = -alpha_s / h, local error test on the predictor-corrector difference,
+// order selection from the estimates at orders k-2 .. k+1, step doubling in
+// the initial phase, at most four Newton iterations with the rate test
+// s * ||delta|| <= 0.33, and GMRES solved to eplifac * 0.33 with
+// eplifac = 0.05 (IDA defaults).  Every step first freezes the upwind
+// directions (preprocess_timestep, fvmpor_ODE_impl.cpp:118-141).
+//
+// The same template drives the B200 kernels (bdf.cu) and the CPU oracle,
+// so the two differ only in the kernels.
+//
+// Ops must provide (vectors y, y', e, F, x, ewt and phi_0..phi_6 are
+// owned by Ops):
+//   void   ewt_from_phi0(double rtol, double atol);
+//   void   begin_step();                     // freeze upwinding at (phi_0, y')
+//   void   phi_scale(int j0, int j1, const double* f);   // phi_j *= f[j]
+//   void   predict(int k, const double* gamma);          // y, y' ; e = 0
+//   double wrms_y();
+//   void   residual();                       // F = F(t, y, y')
+//   int    psetup(double cj, double h);      // 0 ok, else zero pivot
+//   int    gmres(double cj, double tol, int* its, double* rn, long* nps,
+//                long* njv);                 // J x = F; 0 ok, 1 not converged,
+//                                            // 2 breakdown / non-finite
+//   double newton_update(double cj);         // y -= x, y' -= cj x, e -= x;
+//                                            // returns ||x||_wrms
+//   void   err_norms(int k, double out[4]);  // see below
+//   void   phi_update(int k, int set_kp2);
+//   void   newton_guess(double cj);          // optional learned iterate
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+
+namespace fvmb {
+
+struct BdfStats {
+    long nst = 0, nni = 0, nli = 0, npe = 0, nps = 0, ncfn = 0, ncfl = 0, netf = 0, njv = 0;
+    long npred = 0;
+    int last_order = 0;
+    double last_h = 0.0;
+};
+
+struct BdfOptions {
+    double rtol = 1e-6, atol = 1e-6;
+    int max_order = 5;
+    double hmax = 0.0;
+    bool use_guess = false;
+};
+
+template <class Ops> struct BdfController {
+    static constexpr int kMaxOrd = 5;
+    Ops& ops;
+    BdfOptions o;
+    BdfStats st;
+    double psi[kMaxOrd + 2] = {}, alpha[kMaxOrd + 2] = {}, beta[kMaxOrd + 2] = {},
+           sigma[kMaxOrd + 2] = {}, gamma[kMaxOrd + 2] = {};
+    int k = 1, kold = 0, ns = 0, iphase = 0;
+    double h = 0, hold = 0, t = 0, cj = 0, rate_s = 100.0;
+    bool have_p = false;
+    double cj_p = 0;
+    long nst_p = 0;
+
+    BdfController(Ops& ops_, const BdfOptions& opt) : ops(ops_), o(opt) {}
+
+    // phi_0 = y0 and phi_1 = h y'0 must be set by the caller after this
+    void start(double t0, double h0) {
+        t = t0;
+        h = h0;
+        k = 1; kold = 0; hold = 0; psi[0] = h; cj = 1.0 / h; iphase = 0; ns = 0;
+        rate_s = 100.0;
+        have_p = false;
+    }
+
+    void restore() {
+        if (k >= ns) {
+            double f[kMaxOrd + 2];
+            for (int j = 0; j < kMaxOrd + 2; ++j) f[j] = beta[j] != 0.0 ? 1.0 / beta[j] : 1.0;
+            ops.phi_scale(ns, k, f);
+        }
+        for (int i = 1; i <= k; ++i) psi[i - 1] = psi[i] - h;
+    }
+
+    // one accepted step (not past tstop); 0 ok, < 0 unrecoverable
+    int step(double tstop) {
+        const double uround = 2.220446049250313e-16;
+        const double epcon = 0.33;
+        int nef = 0, ncf = 0;
+        if (t + h > tstop) h = tstop - t;
+        ops.ewt_from_phi0(o.rtol, o.atol);
+        ops.begin_step();
+        for (;;) {
+            if (h != hold || k != kold) ns = 0;
+            ns = std::min(ns + 1, kold + 2);
+            if (k + 1 >= ns) {
+                beta[0] = 1.0; alpha[0] = 1.0; gamma[0] = 0.0; sigma[0] = 1.0;
+                double temp1 = h;
+                for (int i = 1; i <= k; ++i) {
+                    double temp2 = psi[i - 1];
+                    psi[i - 1] = temp1;
+                    beta[i] = beta[i - 1] * psi[i - 1] / temp2;
+                    temp1 = temp2 + h;
+                    alpha[i] = h / temp1;
+                    sigma[i] = i * sigma[i - 1] * alpha[i];
+                    gamma[i] = gamma[i - 1] + alpha[i - 1] / h;
+                }
+                psi[k] = temp1;
+            }
+            double alphas = 0.0, alpha0 = 0.0;
+            for (int i = 1; i <= k; ++i) { alphas -= 1.0 / i; alpha0 -= alpha[i - 1]; }
+            cj = -alphas / h;
+            double ck = std::max(std::fabs(alpha[k] + alphas - alpha0), alpha[k]);
+            if (k >= ns) ops.phi_scale(ns, k, beta);
+            double tnew = t + h;
+            ops.predict(k, gamma);
+            double pnorm = ops.wrms_y();
+            if (o.use_guess && ops.newton_guess(tnew, cj)) st.npred++;
+            bool converged = false, fresh_p = false;
+            bool need_p = !have_p || std::fabs(cj / cj_p - 1.0) > 0.25 || (st.nst - nst_p) >= 20;
+            for (int attempt = 0; attempt < 2 && !converged; ++attempt) {
+                if (attempt == 1) {
+                    if (fresh_p) break;
+                    ops.predict(k, gamma);   // retry from the predictor with a fresh factor
+                    need_p = true;
+                }
+                ops.set_time(tnew);
+                ops.residual();
+                if (need_p) {
+                    int pr = ops.psetup(cj, h);
+                    st.npe++;
+                    if (pr) return -3;
+                    have_p = true; cj_p = cj; nst_p = st.nst; fresh_p = true; rate_s = 100.0;
+                    need_p = false;
+                }
+                double oldnrm = 0.0;
+                for (int m = 0; m < 4; ++m) {
+                    if (m > 0) ops.residual();
+                    int its = 0;
+                    double rn = 0.0;
+                    long nps = 0, njv = 0;
+                    int lr = ops.gmres(cj, 0.05 * epcon, &its, &rn, &nps, &njv);
+                    st.nli += its; st.nps += nps; st.njv += njv; st.nni++;
+                    if (lr != 0) st.ncfl++;
+                    if (lr == 2) break;
+                    double delnrm = ops.newton_update(cj);
+                    if (!std::isfinite(delnrm)) break;
+                    if (m == 0) {
+                        oldnrm = delnrm;
+                        if (delnrm <= 100.0 * uround * pnorm) { converged = true; break; }
+                    } else {
+                        double rate = std::pow(delnrm / oldnrm, 1.0 / m);
+                        if (rate > 0.9) break;
+                        rate_s = rate / (1.0 - rate);
+                    }
+                    if (rate_s * delnrm <= epcon) { converged = true; break; }
+                }
+            }
+            if (converged) {
+                double nr[4];
+                ops.err_norms(k, nr);
+                double enorm = nr[0];
+                double erk = sigma[k] * enorm;
+                double terk = (k + 1) * erk;
+                double est = erk;
+                int knew = k;
+                double erkm1 = 0.0, terkm1 = 0.0;
+                if (k > 1) {
+                    erkm1 = sigma[k - 1] * nr[1];
+                    terkm1 = k * erkm1;
+                    bool lower;
+                    if (k > 2) {
+                        double terkm2 = (k - 1) * sigma[k - 2] * nr[2];
+                        lower = std::max(terkm1, terkm2) <= terk;
+                    } else {
+                        lower = terkm1 <= 0.5 * terk;
+                    }
+                    if (lower) { knew = k - 1; est = erkm1; }
+                }
+                double err = ck * enorm;
+                if (err <= 1.0 && std::isfinite(err)) {
+                    int kstep = k;
+                    int kdiff = k - kold;
+                    int set_kp2 = kstep != o.max_order;
+                    kold = k;
+                    hold = h;
+                    t = tnew;
+                    st.nst++;
+                    double hnew = h;
+                    if (knew == k - 1 || k == o.max_order) iphase = 1;
+                    bool doubled = false;
+                    if (iphase == 0) {
+                        k = k + 1;
+                        hnew = 2.0 * h;
+                        doubled = true;
+                    } else if (knew == k - 1) {
+                        k = k - 1;
+                        est = erkm1;
+                    } else if (k != o.max_order && !(k + 1 >= ns || kdiff == 1)) {
+                        double terkp1 = nr[3];
+                        double erkp1 = terkp1 / (k + 2);
+                        bool raise = false, lower = false;
+                        if (k > 1) {
+                            if (terkm1 <= std::min(terk, terkp1)) lower = true;
+                            else if (terkp1 < terk) raise = true;
+                        } else if (terkp1 < 0.5 * terk) {
+                            raise = true;
+                        }
+                        if (raise) { k = k + 1; est = erkp1; }
+                        else if (lower) { k = k - 1; est = erkm1; }
+                    }
+                    if (!doubled) {
+                        double r = std::pow(2.0 * est + 1e-4, -1.0 / (k + 1));
+                        if (r >= 2.0) hnew = 2.0 * h;
+                        else if (r <= 1.0) hnew = h * std::max(0.5, std::min(0.9, r));
+                    }
+                    if (o.hmax > 0) hnew = std::min(hnew, o.hmax);
+                    ops.phi_update(kstep, set_kp2);
+                    h = hnew;
+                    st.last_order = kold;
+                    st.last_h = hold;
+                    return 0;
+                }
+                st.netf++;
+                nef++;
+                iphase = 1;
+                restore();
+                if (nef == 1) {
+                    k = knew;
+                    double r = 0.9 * std::pow(2.0 * est + 1e-4, -1.0 / (k + 1));
+                    h *= std::max(0.25, std::min(0.9, r));
+                } else if (nef == 2) {
+                    k = knew;
+                    h *= 0.25;
+                } else {
+                    k = 1;
+                    h *= 0.25;
+                }
+                if (nef > 10) return -4;
+            } else {
+                st.ncfn++;
+                ncf++;
+                iphase = 1;
+                restore();
+                h *= 0.25;
+                if (ncf > 10) return -5;
+            }
+            if (std::fabs(h) < 4.0 * uround * std::max(std::fabs(t), std::fabs(tstop))) return -6;
+        }
+    }
+};
+
+// DASSL's first step: 1e-3 of the interval, limited by 0.5 / ||y'0||_wrms
+inline double bdf_first_step(double t0, double tout, double ypnorm, double h0, double hmax) {
+    double hh = h0 > 0 ? h0 : 1e-3 * std::fabs(tout - t0);
+    if (h0 <= 0 && ypnorm > 0.5 / hh) hh = 0.5 / ypnorm;
+    if (hmax > 0) hh = std::min(hh, hmax);
+    return hh;
+}
+
+} // namespace fvmb

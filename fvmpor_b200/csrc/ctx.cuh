@@ -1,0 +1,174 @@
+// Device-resident state of one Richards problem (the fvm_ctx behind the C
+// ABI) and the small device helpers shared by the kernel files.
+#pragma once
+
+#include "common.hpp"
+#include "cvfe_geom.cuh"
+#include "ktimer.hpp"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+namespace fvmb {
+
+#define FVM_CUDA(call)                                                                 \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            throw ::fvmb::Error(std::string(#call) + ": " + cudaGetErrorString(e_), -2); \
+    } while (0)
+
+template <class T> struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        if (count == n && p) return;
+        release();
+        if (count == 0) return;
+        FVM_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+        n = count;
+    }
+    void upload(const std::vector<T>& v, cudaStream_t s) {
+        alloc(v.size());
+        if (!v.empty()) FVM_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void zero(cudaStream_t s) {
+        if (n) FVM_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+    }
+};
+
+// van Genuchten parameters of one soil zone on the device
+struct ZoneDev {
+    double phi, alpha, n, m, Sr;
+};
+
+// Van Genuchten-Mualem relations in the operation order of
+// VarSatPhysicsImpl::saturation (examples/fvmporMinlin/fvmpor.h:302-343):
+//   a = (-alpha h)^n, b = 1 + a, Se = b^-m, Sw = S_r + (1 - S_r) Se,
+//   dSw/dh = -(1 - S_r)(n - 1) (a / b) Se / h,
+//   krw = sqrt(Se) ((a / b)^m - 1)^2,
+// overridden by Sw = 1, dSw = 0, krw = 1 for h >= 0.
+FVM_HD void van_genuchten(double h, const ZoneDev& z, double& Sw, double& dSw, double& krw) {
+    if (h >= 0.0) {
+        Sw = 1.0;
+        dSw = 0.0;
+        krw = 1.0;
+        return;
+    }
+    double a = pow(-z.alpha * h, z.n);
+    double b = a + 1.0;
+    double k = -1.0 / b;
+    double d = a / b;
+    double Se = pow(b, -z.m);
+    d = d * Se;
+    d = d / h;
+    d = d * (-(1.0 - z.Sr) * (z.n - 1.0));
+    k = k + 1.0;
+    k = pow(k, z.m);
+    k = k - 1.0;
+    k = k * k;
+    k = k * sqrt(Se);
+    Sw = Se * (1.0 - z.Sr) + z.Sr;
+    dSw = d;
+    krw = k;
+}
+
+// ---------------------------------------------------------------------------
+// Perturbation applied by the node pass before the residual:
+//   mode 0: none (plain residual)
+//   mode 1: y + sigma v, y' + cj sigma v           (Jacobian-vector product)
+//   mode 2: y + d_j, y' + cj d_j on colour c only   (finite-difference Jacobian)
+struct Perturb {
+    int mode = 0;
+    double sigma = 0.0, cj = 0.0;
+    const double* sigma_dev = nullptr; // mode 1: device-resident sigma (overrides sigma)
+    const double* v = nullptr;       // mode 1
+    const double* shift = nullptr;   // mode 2: shift vector d
+    const int* colour = nullptr;     // mode 2: colour of every node
+    int c = 0;                       // mode 2: active colour
+};
+
+struct BlockILU;   // precond.cu
+struct Krylov;     // linalg.cu
+
+} // namespace fvmb
+
+struct fvm_ctx {
+    int dim = 0, N = 0, T = 0, nz = 0;
+    int npe = 0;   // nodes per element (3 / 4)
+    int nfe = 0;   // CV faces per element (3 / 6)
+    int E = 0;     // edges
+    double rho0 = 1000.0;
+    bool recompute = false;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+
+    // host copies needed by the preconditioner set-up and the integrator
+    std::vector<int> h_elem_nodes;   // [T][npe]
+    std::vector<int> h_node_type;    // 0 free, 1 Dirichlet
+    std::vector<double> h_vert;      // elevation of each node
+    std::vector<double> h_hD;        // Dirichlet head (valid where type 1)
+
+    // element data
+    fvmb::DevBuf<int4> enodes;        // [T] node ids (4th = -1 for triangles)
+    fvmb::DevBuf<double> coef;        // [(f*(npe+1)+k)*T + e]
+    fvmb::DevBuf<int> ezone;          // [T], only when nz > 1
+    fvmb::DevBuf<double> eK;          // [3][T] conductivities (recompute variant)
+    fvmb::DevBuf<double> xyz;         // [3][N] coordinates (recompute variant)
+    fvmb::DevBuf<unsigned char> upw;  // [T*8] upwind flag per face: 1 = node b
+    fvmb::DevBuf<unsigned char> flip; // [T] bit f set when node a of face f is
+                                      // the global back node of its edge
+
+    // node data
+    fvmb::DevBuf<double> invV;        // 1 / control-volume measure
+    fvmb::DevBuf<double> bterm;       // constant boundary-flux term / V
+    fvmb::DevBuf<double> hD;          // Dirichlet head (type 1 nodes)
+    fvmb::DevBuf<unsigned char> ntype;
+    fvmb::DevBuf<int> nz_ptr, nz_zone;  // zones touching each node (CSR)
+    fvmb::DevBuf<double> nz_w;          // SCV volume fraction per node-zone
+    fvmb::DevBuf<int> inc_ptr, inc;     // node -> (e*npe + k), ascending e
+    fvmb::DevBuf<fvmb::ZoneDev> zones;
+
+    // edges (for the frozen upwind directions)
+    fvmb::DevBuf<int> edge_ptr, edge_face;  // edge -> e*nfe + f, ascending e
+    fvmb::DevBuf<double> edge_w;            // 1 / sum of the edge's face areas
+
+    // workspace
+    fvmb::DevBuf<double> krw;        // [nz][N]
+    fvmb::DevBuf<double> hstar;      // perturbed head
+    fvmb::DevBuf<double> stor;       // ahh * y'
+    fvmb::DevBuf<double> contrib;    // [T*npe] element flux sums per node
+    fvmb::DevBuf<double> faceq;      // [T*nfe] averaged-weight face fluxes
+    fvmb::DevBuf<double> tmpN[4];    // scratch vectors
+
+    fvmb::BlockILU* ilu = nullptr;
+    fvmb::Krylov* kry = nullptr;
+
+    long n_residuals = 0;
+    fvmb::KernelTimer tm;
+    std::string err;
+};
+
+namespace fvmb {
+
+// residual driver shared by fvm_residual / fvm_jv / the FD Jacobian
+// out = F(t, y~, y'~) (or (F - F0) / sigma when F0 != nullptr)
+void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Perturb& pt,
+                     const double* F0, double* out);
+void launch_begin_step(fvm_ctx* c, const double* y, const double* yp);
+
+inline int grid_for(long n, int block) { return (int)((n + block - 1) / block); }
+
+} // namespace fvmb

@@ -1,0 +1,45 @@
+// Krylov workspace and the internal (device-pointer, no host sync unless
+// stated) entry points shared between the ABI, the preconditioner and the
+// integrator.
+#pragma once
+
+#include "ctx.cuh"
+
+namespace fvmb {
+
+struct Krylov {
+    int m = 0;
+    int precision = 0;        // 0: FP64 basis, 1: FP32 basis
+    size_t ld = 0;            // leading dimension of the basis
+    void* U = nullptr;        // (m+1) x ld basis, float or double
+    DevBuf<double> scale;     // s_i, V_i = s_i U_i
+    DevBuf<double> W, t, z, Jv;
+    DevBuf<double> partial;
+    DevBuf<unsigned> counter;
+    DevBuf<double> res;       // reduction results
+    DevBuf<double> sigma;
+    double* host = nullptr;   // pinned
+};
+
+struct GmresCounters {
+    long njv = 0;
+    long nps = 0;
+};
+
+Krylov* krylov_get(fvm_ctx* c, int m, int precision);
+void fvmb_destroy_krylov_impl(Krylov* K);
+double reduce_sumsq(fvm_ctx* c, const double* x, const double* w);
+double reduce_dot(fvm_ctx* c, const double* x, const double* y);
+
+int gmres_dev(fvm_ctx* c, double cj, const double* y, const double* yp, const double* F0,
+              const double* ewt, const double* b, double* x, int m, int max_restarts,
+              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt);
+
+// preconditioner (precond.cu)
+void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* yp,
+                const double* F0, const double* ewt, int precision);
+void psolve_dev(fvm_ctx* c, const double* r, double* z);
+bool ilu_ready(fvm_ctx* c);
+int ilu_status(fvm_ctx* c);   // 0 ok, 1 zero pivot in the last factorisation
+
+} // namespace fvmb

@@ -1,0 +1,443 @@
+// Reductions, WRMS norms and right-preconditioned restarted GMRES.
+//
+// Algorithm: decomp/gmres.c:26-201 (restarted, right-preconditioned
+// GMRES(m)), arnoldi :412-511 and the Givens least squares of
+// decomp/linalg_dense.c:128-173, applied as IDAS SPGMR applies it inside
+// Newton: zero initial guess, residual measured in the WRMS norm of the
+// error weights (the system is scaled by D = diag(ewt)), J*v by a
+// difference quotient of the residual.
+//
+// B200 layout: the Arnoldi basis is kept as unnormalised vectors U_i with a
+// per-vector scale s_i (V_i = s_i U_i), in FP64 or FP32 (mixed precision).
+// Orthogonalisation is classical Gram-Schmidt with one re-orthogonalisation
+// (CGS2) in three fused passes over the basis, so one Arnoldi step costs
+// three basis reads instead of the 2(j+1) of modified Gram-Schmidt; every
+// dot product accumulates in FP64 and is reduced in a fixed order (per-block
+// partials, then the last block sums them by block index), so results are
+// bitwise reproducible.  The Hessenberg matrix, Givens rotations and the
+// stopping test run in FP64 on the host from j+2 numbers copied back per
+// step.
+#include "ctx.cuh"
+#include "krylov.cuh"
+#include "reduce.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace fvmb {
+
+// out[0] = sum_k (x_k w_k)^2 (w may be null -> 1)
+__global__ void k_sumsq(int N, const double* __restrict__ x, const double* __restrict__ w,
+                        double* partial, unsigned* counter, double* out) {
+    double s = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        double v = w ? x[k] * w[k] : x[k];
+        s += v * v;
+    }
+    __shared__ double red[32];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    }
+    last_block_reduce(partial, 1, counter, out);
+}
+
+__global__ void k_dot(int N, const double* __restrict__ x, const double* __restrict__ y,
+                      double* partial, unsigned* counter, double* out) {
+    double s = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) s += x[k] * y[k];
+    __shared__ double red[32];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    }
+    last_block_reduce(partial, 1, counter, out);
+}
+
+// sigma = 1 / ||z||_wrms for the difference-quotient J*v (IDAS picks the
+// increment that makes the perturbation one weighted unit); 1 if z = 0
+__global__ void k_sigma_from_sumsq(const double* sumsq, int N, double* sigma) {
+    double n = sqrt(sumsq[0] / (double)N);
+    *sigma = n > 0.0 ? 1.0 / n : 1.0;
+}
+
+// ------------------------------------------------------------------ CGS2
+template <class B>
+__device__ __forceinline__ double ldb(const B* U, size_t i) { return (double)U[i]; }
+
+// pass 1: w~ = ewt * Jv (stored in W); a_i = <U_i, w~> for i < nv
+template <class B>
+__global__ void k_cgs_pass1(int N, int nv, const B* __restrict__ U, size_t ld,
+                            const double* __restrict__ Jv, const double* __restrict__ ewt,
+                            double* __restrict__ W, double* partial, unsigned* counter,
+                            double* out) {
+    int chunk = (N + gridDim.x - 1) / gridDim.x;
+    int k0 = blockIdx.x * chunk, k1 = min(N, k0 + chunk);
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) W[k] = ewt[k] * Jv[k];
+    __syncthreads();
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = warp; i < nv; i += nw) {
+        const B* Ui = U + ld * i;
+        double s = 0.0;
+        for (int k = k0 + lane; k < k1; k += 32) s += ldb(Ui, k) * W[k];
+        s = warp_sum(s);
+        if (lane == 0) partial[(size_t)blockIdx.x * nv + i] = s;
+    }
+    last_block_reduce(partial, nv, counter, out);
+}
+
+// pass 2: W -= sum_i (a_i s_i^2) U_i ; b_i = <U_i, W>
+template <class B>
+__global__ void k_cgs_pass2(int N, int nv, const B* __restrict__ U, size_t ld,
+                            const double* __restrict__ scale, const double* __restrict__ a,
+                            double* __restrict__ W, double* partial, unsigned* counter,
+                            double* out) {
+    __shared__ double coef[64];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = a[i] * scale[i] * scale[i];
+    __syncthreads();
+    int chunk = (N + gridDim.x - 1) / gridDim.x;
+    int k0 = blockIdx.x * chunk, k1 = min(N, k0 + chunk);
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        double acc = 0.0;
+        for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
+        W[k] = W[k] - acc;
+    }
+    __syncthreads();
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = warp; i < nv; i += nw) {
+        const B* Ui = U + ld * i;
+        double s = 0.0;
+        for (int k = k0 + lane; k < k1; k += 32) s += ldb(Ui, k) * W[k];
+        s = warp_sum(s);
+        if (lane == 0) partial[(size_t)blockIdx.x * nv + i] = s;
+    }
+    last_block_reduce(partial, nv, counter, out);
+}
+
+// pass 3: W -= sum_i (b_i s_i^2) U_i ; U_nv = store(W) ; out[0] = ||U_nv||^2
+// and scale[nv] = 1/||U_nv|| written by the last block
+template <class B>
+__global__ void k_cgs_pass3(int N, int nv, B* __restrict__ U, size_t ld,
+                            double* __restrict__ scale, const double* __restrict__ b,
+                            const double* __restrict__ W, double* partial, unsigned* counter,
+                            double* out) {
+    __shared__ double coef[64];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = b[i] * scale[i] * scale[i];
+    __syncthreads();
+    B* Un = U + ld * nv;
+    double s = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
+        B st = (B)(W[k] - acc);
+        Un[k] = st;
+        double d = (double)st;
+        s += d * d;
+    }
+    __shared__ double red[32];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    }
+    last_block_reduce(partial, 1, counter, out);
+}
+
+__global__ void k_set_scale(const double* nrm2, double* scale, int idx) {
+    double n = sqrt(nrm2[0]);
+    scale[idx] = n > 0.0 ? 1.0 / n : 0.0;
+}
+
+// t = s_j U_j / ewt  (unscaled Krylov direction fed to the preconditioner)
+template <class B>
+__global__ void k_unscale(int N, const B* __restrict__ Uj, const double* __restrict__ scale,
+                          int j, const double* __restrict__ ewt, double* __restrict__ t) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    t[k] = scale[j] * ldb(Uj, k) / ewt[k];
+}
+
+// t = (sum_i y_i s_i U_i) / ewt
+template <class B>
+__global__ void k_combine(int N, int nv, const B* __restrict__ U, size_t ld,
+                          const double* __restrict__ ys, const double* __restrict__ ewt,
+                          double* __restrict__ t) {
+    __shared__ double coef[64];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = ys[i];
+    __syncthreads();
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    double acc = 0.0;
+    for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
+    t[k] = acc / ewt[k];
+}
+
+// r~ = ewt * (b - Jx) (Jx may be null -> b); U_0 = r~; out = ||r~||^2
+template <class B>
+__global__ void k_init_residual(int N, const double* __restrict__ b, const double* __restrict__ Jx,
+                                const double* __restrict__ ewt, B* __restrict__ U0, double* partial,
+                                unsigned* counter, double* out) {
+    double s = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        double r = Jx ? b[k] - Jx[k] : b[k];
+        B st = (B)(ewt[k] * r);
+        U0[k] = st;
+        double d = (double)st;
+        s += d * d;
+    }
+    __shared__ double red[32];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    }
+    last_block_reduce(partial, 1, counter, out);
+}
+
+__global__ void k_axpy(int N, double a, const double* __restrict__ x, double* __restrict__ y) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < N) y[k] += a * x[k];
+}
+
+// ------------------------------------------------------------------ Krylov
+Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
+    Krylov* K = c->kry;
+    if (K && K->m >= m && K->precision == precision) return K;
+    if (K) fvmb_destroy_krylov_impl(K);
+    K = new Krylov();
+    K->m = m;
+    K->precision = precision;
+    K->ld = ((size_t)c->N + 63) / 64 * 64;
+    size_t bytes = (precision ? sizeof(float) : sizeof(double)) * K->ld * (m + 1);
+    FVM_CUDA(cudaMalloc(&K->U, bytes));
+    K->scale.alloc(m + 2);
+    K->W.alloc(c->N);
+    K->t.alloc(c->N);
+    K->z.alloc(c->N);
+    K->Jv.alloc(c->N);
+    K->partial.alloc((size_t)kRedBlocks * (m + 2));
+    K->counter.alloc(1);
+    K->counter.zero(c->stream);
+    K->res.alloc(3 * (m + 2) + 8);
+    K->sigma.alloc(1);
+    FVM_CUDA(cudaMallocHost(&K->host, sizeof(double) * (3 * (m + 2) + 8)));
+    c->kry = K;
+    return K;
+}
+
+void fvmb_destroy_krylov_impl(Krylov* K) {
+    if (!K) return;
+    if (K->U) cudaFree(K->U);
+    if (K->host) cudaFreeHost(K->host);
+    delete K;
+}
+
+// host-synchronous reductions used by the controller
+double reduce_sumsq(fvm_ctx* c, const double* x, const double* w) {
+    Krylov* K = krylov_get(c, c->kry ? c->kry->m : 1, c->kry ? c->kry->precision : 0);
+    k_sumsq<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->N, x, w, K->partial.p, K->counter.p, K->res.p);
+    FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    return K->host[0];
+}
+
+double reduce_dot(fvm_ctx* c, const double* x, const double* y) {
+    Krylov* K = krylov_get(c, c->kry ? c->kry->m : 1, c->kry ? c->kry->precision : 0);
+    k_dot<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->N, x, y, K->partial.p, K->counter.p, K->res.p);
+    FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    return K->host[0];
+}
+
+// J*v into out, sigma = 1/||v||_wrms computed on the device
+static void jv_dev(fvm_ctx* c, Krylov* K, double cj, const double* y, const double* yp,
+                   const double* F0, const double* v, const double* ewt, double* out) {
+    k_sumsq<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->N, v, ewt, K->partial.p, K->counter.p, K->res.p);
+    k_sigma_from_sumsq<<<1, 1, 0, c->stream>>>(K->res.p, c->N, K->sigma.p);
+    Perturb pt;
+    pt.mode = 1;
+    pt.cj = cj;
+    pt.v = v;
+    pt.sigma_dev = K->sigma.p;
+    launch_residual(c, y, yp, pt, F0, out);
+}
+
+template <class B>
+static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const double* yp,
+                      const double* F0, const double* ewt, const double* b, double* x, int m,
+                      int max_restarts, double tol, int* iters, double* res_norm,
+                      GmresCounters* cnt) {
+    cudaStream_t s = c->stream;
+    const int N = c->N;
+    B* U = reinterpret_cast<B*>(K->U);
+    const size_t ld = K->ld;
+    const double sqrtN = std::sqrt((double)N);
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), hcol(m + 2);
+    FVM_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
+    int total = 0;
+    double rnorm = 0.0;
+    bool have_x = false;
+    for (int cycle = 0; cycle <= max_restarts; ++cycle) {
+        // residual of the current iterate
+        if (have_x) {
+            jv_dev(c, K, cj, y, yp, F0, x, ewt, K->Jv.p);
+            if (cnt) cnt->njv++;
+        }
+        k_init_residual<B><<<kRedBlocks, kRedThreads, 0, s>>>(N, b, have_x ? K->Jv.p : nullptr, ewt, U,
+                                                              K->partial.p, K->counter.p, K->res.p);
+        k_set_scale<<<1, 1, 0, s>>>(K->res.p, K->scale.p, 0);
+        FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        FVM_CUDA(cudaStreamSynchronize(s));
+        double beta = std::sqrt(K->host[0]);
+        rnorm = beta / sqrtN;
+        if (!std::isfinite(beta)) { *iters = total; *res_norm = rnorm; return 2; }
+        if (rnorm <= tol) { *iters = total; *res_norm = rnorm; return 0; }
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int j = 0;
+        bool conv = false;
+        for (; j < m; ++j) {
+            // z = P^-1 D^-1 V_j ; w = J z
+            k_unscale<B><<<grid_for(N, 256), 256, 0, s>>>(N, U + ld * j, K->scale.p, j, ewt, K->t.p);
+            psolve_dev(c, K->t.p, K->z.p);
+            if (cnt) cnt->nps++;
+            jv_dev(c, K, cj, y, yp, F0, K->z.p, ewt, K->Jv.p);
+            if (cnt) cnt->njv++;
+            int nv = j + 1;
+            double* ra = K->res.p;
+            double* rb = K->res.p + (m + 2);
+            double* rn = K->res.p + 2 * (m + 2);
+            c->tm.begin(TM_CGS, s);
+            k_cgs_pass1<B><<<kRedBlocks, kRedThreads, 0, s>>>(N, nv, U, ld, K->Jv.p, ewt, K->W.p, K->partial.p, K->counter.p, ra);
+            k_cgs_pass2<B><<<kRedBlocks, kRedThreads, 0, s>>>(N, nv, U, ld, K->scale.p, ra, K->W.p, K->partial.p, K->counter.p, rb);
+            k_cgs_pass3<B><<<kRedBlocks, kRedThreads, 0, s>>>(N, nv, U, ld, K->scale.p, rb, K->W.p, K->partial.p, K->counter.p, rn);
+            k_set_scale<<<1, 1, 0, s>>>(rn, K->scale.p, nv);
+            c->tm.end(TM_CGS, s);
+            FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaMemcpyAsync(K->host + 3 * (m + 2), K->scale.p, sizeof(double) * (nv), cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaStreamSynchronize(s));
+            const double* ha = K->host;
+            const double* hb = K->host + (m + 2);
+            const double* hsc = K->host + 3 * (m + 2);
+            double hn = std::sqrt(K->host[2 * (m + 2)]);
+            for (int i = 0; i < nv; ++i) hcol[i] = hsc[i] * (ha[i] + hb[i]);
+            hcol[nv] = hn;
+            ++total;
+            if (!std::isfinite(hn)) { *iters = total; *res_norm = rnorm; return 2; }
+            // apply previous rotations, then a new one (linalg_dense.c:128-173)
+            for (int i = 0; i < j; ++i) {
+                double t0 = cs[i] * hcol[i] + sn[i] * hcol[i + 1];
+                double t1 = -sn[i] * hcol[i] + cs[i] * hcol[i + 1];
+                hcol[i] = t0;
+                hcol[i + 1] = t1;
+            }
+            double den = std::hypot(hcol[j], hcol[j + 1]);
+            if (den == 0.0) { cs[j] = 1.0; sn[j] = 0.0; }
+            else { cs[j] = hcol[j] / den; sn[j] = hcol[j + 1] / den; }
+            hcol[j] = den;
+            hcol[j + 1] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hcol[i];
+            rnorm = std::fabs(g[j + 1]) / sqrtN;
+            if (rnorm <= tol || hn == 0.0) { ++j; conv = true; break; }
+        }
+        // back substitution H y = g
+        int kdim = j;
+        std::vector<double> yv(kdim);
+        for (int i = kdim - 1; i >= 0; --i) {
+            double sacc = g[i];
+            for (int l = i + 1; l < kdim; ++l) sacc -= H[(size_t)i * m + l] * yv[l];
+            double d = H[(size_t)i * m + i];
+            yv[i] = d != 0.0 ? sacc / d : 0.0;
+        }
+        // x += P^-1 D^-1 sum_i y_i V_i
+        for (int i = 0; i < kdim; ++i) K->host[i] = yv[i] * K->host[3 * (m + 2) + i];
+        // scales of the basis vectors: the last batch copied holds s_0..s_{j}
+        FVM_CUDA(cudaMemcpyAsync(K->res.p, K->host, sizeof(double) * kdim, cudaMemcpyHostToDevice, s));
+        k_combine<B><<<grid_for(N, 256), 256, 0, s>>>(N, kdim, U, ld, K->res.p, ewt, K->t.p);
+        psolve_dev(c, K->t.p, K->z.p);
+        if (cnt) cnt->nps++;
+        k_axpy<<<grid_for(N, 256), 256, 0, s>>>(N, 1.0, K->z.p, x);
+        have_x = true;
+        if (conv) {
+            FVM_CUDA(cudaStreamSynchronize(s));
+            *iters = total;
+            *res_norm = rnorm;
+            return 0;
+        }
+    }
+    FVM_CUDA(cudaStreamSynchronize(s));
+    *iters = total;
+    *res_norm = rnorm;
+    return 1;
+}
+
+int gmres_dev(fvm_ctx* c, double cj, const double* y, const double* yp, const double* F0,
+              const double* ewt, const double* b, double* x, int m, int max_restarts,
+              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt) {
+    if (m < 1 || m > 60) throw Error("gmres: krylov dimension must be in [1, 60]");
+    Krylov* K = krylov_get(c, m, precision);
+    if (precision)
+        return gmres_impl<float>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt);
+    return gmres_impl<double>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt);
+}
+
+} // namespace fvmb
+
+using namespace fvmb;
+
+void fvmb_destroy_krylov(fvmb::Krylov* p) { fvmb_destroy_krylov_impl(p); }
+
+extern "C" double fvm_wrms(fvm_ctx* c, const double* x, const double* ewt) {
+    try {
+        if (!c || !x) throw Error("fvm_wrms: null argument");
+        return std::sqrt(reduce_sumsq(c, x, ewt) / c->N);
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return NAN;
+    }
+}
+
+extern "C" double fvm_dot(fvm_ctx* c, const double* x, const double* y) {
+    try {
+        if (!c || !x || !y) throw Error("fvm_dot: null argument");
+        return reduce_dot(c, x, y);
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return NAN;
+    }
+}
+
+extern "C" int fvm_gmres(fvm_ctx* c, double t, double cj, const double* y, const double* yp,
+                         const double* F0, const double* ewt, const double* b, double* x, int m,
+                         int max_restarts, int precision, double tol, int* iters, double* res_norm) {
+    try {
+        (void)t;
+        if (!c || !y || !yp || !F0 || !ewt || !b || !x || !iters || !res_norm) throw Error("fvm_gmres: null argument");
+        if (!c->ilu || !ilu_ready(c)) throw Error("fvm_gmres: call fvm_psetup first");
+        int r = gmres_dev(c, cj, y, yp, F0, ewt, b, x, m, max_restarts, precision, tol, iters, res_norm, nullptr);
+        FVM_CUDA(cudaGetLastError());
+        return r;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}

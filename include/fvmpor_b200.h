@@ -1,0 +1,267 @@
+/*
+ * fvmpor_b200 — C ABI of the B200 Richards-equation hot path.
+ *
+ * The reference (FVMPor) exposes its hot path as three C++ template concepts
+ * and no C ABI:
+ *   Physics         include/fvm/physics_base.h:18-131,
+ *                   examples/fvmporMinlin/fvmpor.h:221-231
+ *   Callback        include/fvm/fvm.h:347-359
+ *   Preconditioner  examples/fvmporMinlin/preconditioner_dss.h:27-39
+ * bridged to SUNDIALS IDAS by include/fvm/integrators/ida_integrator.h:479-587.
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions (all entry points):
+ *   - Vectors passed to fvm_* compute calls are DEVICE pointers (cudaMalloc'd,
+ *     CUDA-visible), length n_nodes, owned by the caller, unless the name ends
+ *     in _host.
+ *   - Return status follows the IDA callback convention the reference keeps
+ *     (ida_integrator.h:498,549,576): 0 ok, >0 recoverable (NaN/Inf in a
+ *     result, Krylov non-convergence, zero pivot), <0 fatal (bad argument,
+ *     CUDA error, missing setup).  No C++ exception crosses this boundary.
+ *   - One CUDA stream per context; calls on one context are single-threaded.
+ *   - Every device-side wait is bounded and reports a status; nothing spins
+ *     forever.
+ */
+#ifndef FVMPOR_B200_H
+#define FVMPOR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Problem description (host memory, read once by fvm_create)          */
+/* ------------------------------------------------------------------ */
+
+/* Unstructured simplex mesh.  Replaces the .pmesh reader state of
+ * mesh::Mesh (src/fvm/mesh.cpp:82-366): node coordinates, element
+ * connectivity with a physical-zone tag per element (mesh.cpp:294-296),
+ * boundary faces with boundary tags (mesh.cpp:333-341) and the per-node
+ * boundary tag list the reader attaches to nodes (mesh.cpp:246-262),
+ * reduced here to the tag that decides Dirichlet rows
+ * (fvmpor.h:405-417). */
+typedef struct {
+    int dim;                 /* 2 (triangles) or 3 (tetrahedra)            */
+    int n_nodes;
+    int n_elements;
+    int n_bfaces;            /* boundary segments (2D) / triangles (3D)    */
+    const double* coords;    /* [n_nodes][3]; z = 0 in 2D                  */
+    const int* elem_nodes;   /* [n_elements][dim+1]                        */
+    const int* elem_zone;    /* [n_elements] index into fvm_physics.zones  */
+    const double* elem_K;    /* [n_elements] isotropic K override, or NULL */
+    const int* bface_nodes;  /* [n_bfaces][dim]                            */
+    const int* bface_elem;   /* [n_bfaces] element owning the face         */
+    const int* bface_tag;    /* [n_bfaces] boundary tag (>0)               */
+    const int* node_tag;     /* [n_nodes] boundary tag of a Dirichlet-type
+                                condition touching the node, 0 = none      */
+} fvm_mesh;
+
+/* Soil zone.  PhysicalZone (examples/fvmporMinlin/definitions.h:267-299);
+ * mVG = 1 - 1/nVG as set in vs.h:53.  Soil and fluid compressibility are
+ * zero in every configuration (vs.h:43,71), so porosity is constant. */
+typedef struct {
+    double Kxx, Kyy, Kzz;    /* saturated conductivity [m/s]               */
+    double phi;              /* porosity (theta_s)                         */
+    double alphaVG, nVG;     /* van Genuchten parameters                   */
+    double S_r;              /* residual saturation (theta_r / theta_s)    */
+} fvm_zone;
+
+/* Boundary condition.  BoundaryCondition (definitions.h:105-265); the
+ * hot path supports type 1 (Dirichlet value), 3 (prescribed normal flux
+ * value, positive outwards) and 4 (hydrostatic head (1+eta)(b - z)). */
+typedef struct {
+    int tag;
+    int type;
+    double value;
+    double b;
+    double eta;
+} fvm_bc;
+
+typedef struct {
+    int n_zones;
+    const fvm_zone* zones;
+    int n_bcs;
+    const fvm_bc* bcs;
+    double rho0;             /* Constants::rho_0 (definitions.h:301-326)   */
+} fvm_physics;
+
+/* flags for fvm_create */
+#define FVM_FLAG_RECOMPUTE_GEOMETRY 1  /* face geometry rebuilt per launch
+                                          instead of streamed from HBM     */
+#define FVM_FLAG_AUTOTUNE           2  /* time both residual variants and
+                                          keep the faster one              */
+
+typedef struct fvm_ctx fvm_ctx;
+
+/* Builds the device-resident CVFE data for one mesh on the current CUDA
+ * device.  Replaces VarSatPhysicsImpl::initialise_vectors and
+ * initialise_shape_functions (fvmpor.h:347-644, 948-1124) and the CV
+ * construction of mesh::Mesh (src/fvm/mesh.cpp:786-1156).  Returns NULL on
+ * error; fvm_last_error() tells why. */
+fvm_ctx* fvm_create(const fvm_mesh* mesh, const fvm_physics* phys, int flags);
+void fvm_destroy(fvm_ctx* ctx);
+const char* fvm_last_error(void);
+int fvm_n_nodes(const fvm_ctx* ctx);
+
+/* Initial state: head from the hydrostatic/Dirichlet rules of
+ * set_initial_conditions (vs.h:8-32) with the given water-table elevation
+ * for the non-Dirichlet nodes (h = wt - elevation), written to y (device). */
+int fvm_initial_head(fvm_ctx* ctx, double water_table, double* y);
+
+/* F(t, y, y') -> res.  Replaces Physics::preprocess_evaluation +
+ * residual_evaluation (fvmpor_ODE_impl.cpp:62-116) behind the Callback
+ * (solver.h:123-133) that IDAIntegrator::f calls (ida_integrator.h:479-498). */
+int fvm_residual(fvm_ctx* ctx, double t, const double* y, const double* yp,
+                 double* res);
+
+/* Freezes the upwind direction of every edge for the coming step.
+ * Replaces Physics::preprocess_timestep + process_spatial_weights
+ * (fvmpor_ODE_impl.cpp:118-141, fvmpor.h:762-795). */
+int fvm_begin_step(fvm_ctx* ctx, double t, const double* y, const double* yp);
+
+/* Difference-quotient Jacobian action
+ *   Jv = [F(t, y + sigma v, y' + cj sigma v) - F0] / sigma,
+ * the J*v IDAS SPGMR forms internally (selected at ida_integrator.h:252). */
+int fvm_jv(fvm_ctx* ctx, double t, double cj, const double* y,
+           const double* yp, const double* F0, const double* v,
+           double sigma, double* Jv);
+
+/* Preconditioner setup: coloured finite-difference Jacobian
+ * J = dF/dy + cj dF/dy' (Preconditioner::setup, preconditioner_dss.cpp:
+ * 284-373, shift rule :322-329) followed by a block-ILU(0) factorisation
+ * (decomp/ILU.c:12-115) in place of the MKL DSS factorisation (:368).
+ * ewt are the inverse error weights 1/(rtol|y|+atol).
+ * precision: 0 = FP64 factor, 1 = FP32 factor. */
+int fvm_psetup(fvm_ctx* ctx, double t, double cj, double h, const double* y,
+               const double* yp, const double* F0, const double* ewt,
+               int precision);
+
+/* z = P^{-1} r.  Replaces Preconditioner::apply (preconditioner_dss.cpp:
+ * 375-405); forward/backward substitution of decomp/ILU.c:133-223. */
+int fvm_psolve(fvm_ctx* ctx, const double* r, double* z);
+
+/* Pattern statistics of the last set-up (Preconditioner::initialise,
+ * preconditioner_dss.cpp:144-282): non-zeros of J, colours, ILU blocks and
+ * the largest number of dependency levels in a block.  Any pointer may be
+ * NULL. */
+int fvm_precond_info(fvm_ctx* ctx, int* nnz, int* ncolours, int* nblocks,
+                     int* max_levels);
+
+/* Copies the assembled J (CSR, rows ascending, columns ascending) into HOST
+ * buffers of n_nodes+1 / nnz / nnz entries (the values the reference
+ * gathers into values_ at preconditioner_dss.cpp:362, with the sign
+ * convention +J).  Any pointer may be NULL. */
+int fvm_precond_jacobian(fvm_ctx* ctx, int* rowptr, int* col, double* val);
+
+/* Right-preconditioned restarted GMRES(m) on J x = b in the WRMS norm
+ * weighted by ewt, zero initial guess, until ||b - J x||_wrms <= tol.
+ * Algorithm of decomp/gmres.c:26-201 with arnoldi :412-511 and the Givens
+ * least squares of decomp/linalg_dense.c:128-173.  precision 1 keeps the
+ * Krylov basis in FP32; the Hessenberg, Givens and stopping test stay FP64.
+ * Returns 0 on convergence, 1 (recoverable) otherwise; *iters gets the
+ * number of Arnoldi steps. */
+int fvm_gmres(fvm_ctx* ctx, double t, double cj, const double* y,
+              const double* yp, const double* F0, const double* ewt,
+              const double* b, double* x, int m, int max_restarts,
+              int precision, double tol, int* iters, double* res_norm);
+
+/* WRMS norm sqrt(mean((x*ewt)^2)) and dot product (N_Vector ops of the
+ * reference's nvector_parallel_cuda, examples/fvmporMinlin/makefile:30). */
+double fvm_wrms(fvm_ctx* ctx, const double* x, const double* ewt);
+double fvm_dot(fvm_ctx* ctx, const double* x, const double* y);
+
+/* Live per-kernel timing with CUDA events on the context stream (the
+ * reference's util::TimerCuda, include/util/timer_cuda.h:11-57, and the
+ * preconditioner time_J/time_M/time_apply accumulators, preconditioner_dss.
+ * cpp:297-373).  fvm_profile(ctx, 1) resets and starts, (ctx, 0) stops;
+ * fvm_profile_read fills FVM_PROF_NCAT milliseconds / launch counts in
+ * the order node pass, element pass, node gather, ILU apply, Gram-Schmidt,
+ * ILU factor, FD Jacobian. */
+#define FVM_PROF_NCAT 7
+int fvm_profile(fvm_ctx* ctx, int enable);
+int fvm_profile_read(fvm_ctx* ctx, double* ms, long* counts);
+
+/* ------------------------------------------------------------------ */
+/* Integrator: variable-order BDF + Newton-Krylov driving the above.     */
+/* Replaces IDAIntegrator (ida_integrator.h:39-340) and the time loop of */
+/* examples/fvmporMinlin/fvmpor_ODE.cpp:202-232.                         */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    double rtol, atol;       /* scalar tolerances (IDASStolerances :243)   */
+    int max_order;           /* <= 5 (set_max_order :467)                  */
+    int krylov_dim;          /* GMRES(m)                                   */
+    int max_restarts;
+    int precision;           /* 0 = FP64, 1 = FP32 factor/apply + basis    */
+    int use_predictor;       /* learned Newton initial iterate (fvm_mlp_*) */
+    double h0;               /* first step, 0 = automatic                  */
+    double hmax;             /* 0 = unbounded                              */
+    long max_steps;
+} fvm_opts;
+
+typedef struct {
+    long nst;     /* steps                          */
+    long nre;     /* residual evaluations (any)     */
+    long nni;     /* Newton iterations              */
+    long nli;     /* Krylov (Arnoldi) iterations    */
+    long npe;     /* preconditioner setups          */
+    long nps;     /* preconditioner solves          */
+    long ncfn;    /* Newton convergence failures    */
+    long ncfl;    /* linear convergence failures    */
+    long netf;    /* error test failures            */
+    long npred;   /* steps that used the learned iterate */
+    int  last_order;
+    double last_h;
+    double t;
+} fvm_stats;
+
+void fvm_opts_default(fvm_opts* o);
+
+/* Integrate from (t0, y0) to t_end.  y0 / y_end are HOST buffers; the
+ * solve itself runs on the device.  Returns 0 on success. */
+int fvm_integrate_host(fvm_ctx* ctx, const fvm_opts* opts, double t0,
+                       double t_end, const double* y0_host,
+                       double* y_end_host, fvm_stats* stats);
+
+/* Same, with y0/y_end device pointers. */
+int fvm_integrate(fvm_ctx* ctx, const fvm_opts* opts, double t0,
+                  double t_end, const double* y0, double* y_end,
+                  fvm_stats* stats);
+
+/* ------------------------------------------------------------------ */
+/* Synthetic problem generators (host).  The reference reads gmsh-made   */
+/* .pmesh files (meshing/genMesh.sh, decomp/split.c:459-500); these      */
+/* build the benchmark meshes directly.  Arrays are malloc'd by the      */
+/* library and released with fvm_problem_free.                           */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    fvm_mesh mesh;
+    fvm_physics phys;
+    double water_table;      /* initial hydrostatic level                  */
+    double t_end;            /* simulated horizon [s]                      */
+    /* owned storage */
+    double* coords; int* elem_nodes; int* elem_zone; double* elem_K;
+    int* bface_nodes; int* bface_elem; int* bface_tag; int* node_tag;
+    fvm_zone* zones; fvm_bc* bcs;
+    int* grid_dims;          /* [3] structured node grid extents           */
+} fvm_problem;
+
+/* 2D Richards infiltration: nx*ny node grid over Lx*Ly, Delaunay of the
+ * jittered grid, two soil layers, Dirichlet strip on top. */
+int fvm_problem_richards2d(int nx, int ny, double Lx, double Ly,
+                           double jitter, uint64_t seed,
+                           double ln_var, double corr_len,
+                           fvm_problem* out);
+/* 3D Richards: nx*ny*nz hex cells split into 6 tets, lognormal Ks. */
+int fvm_problem_richards3d(int nx, int ny, int nz, double Lx, double Ly,
+                           double Lz, double jitter, uint64_t seed,
+                           double ln_var, double cx, double cy, double cz,
+                           double Kg, fvm_problem* out);
+void fvm_problem_free(fvm_problem* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FVMPOR_B200_H */

@@ -1,0 +1,269 @@
+"""Known-answer tests that pin the CPU oracle (the reference ships no tests or
+golden vectors for this path, so the oracle is checked against closed forms
+and conservation properties of the CVFE scheme)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import fvmpor_b200 as fb
+from oracle.pyoracle import Oracle, factor_given, vg
+
+
+# ---------------------------------------------------------------- van Genuchten
+def closed_form_vg(h, alpha, n, Sr):
+    m = 1.0 - 1.0 / n
+    a = np.where(h < 0, (alpha * np.abs(h)) ** n, 0.0)
+    Se = np.where(h < 0, (1.0 + a) ** (-m), 1.0)
+    Sw = Sr + (1 - Sr) * Se
+    # analytic derivative dSe/dh = -(n-1) a Se / ((1+a) h)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        dSw = np.where(h < 0, (1 - Sr) * (-(n - 1) * a * Se / ((1 + a) * h)), 0.0)
+    krw = np.where(h < 0, np.sqrt(Se) * (1 - (1 - Se ** (1 / m)) ** m) ** 2, 1.0)
+    return Sw, dSw, krw
+
+
+@pytest.mark.parametrize("alpha,n,Sr", [(1.0, 2.0, 0.125), (3.0, 1.6, 0.2222), (2.0, 1.8, 0.142857), (3.55, 2.0, 0.3261)])
+def test_van_genuchten_closed_form(alpha, n, Sr):
+    h = np.concatenate([-np.logspace(-4, 2, 200), [0.0, 1e-9, 0.5, 3.0]])
+    Sw, dSw, krw = vg(alpha, n, Sr, h)
+    Sw0, dSw0, krw0 = closed_form_vg(h, alpha, n, Sr)
+    assert np.allclose(Sw, Sw0, rtol=1e-13, atol=1e-15)
+    assert np.allclose(dSw, dSw0, rtol=1e-11, atol=1e-18)
+    assert np.allclose(krw, krw0, rtol=1e-7, atol=1e-14)
+    # saturated override (fvmpor.h:336-342)
+    sat = h >= 0
+    assert np.all(Sw[sat] == 1.0) and np.all(dSw[sat] == 0.0) and np.all(krw[sat] == 1.0)
+
+
+def test_van_genuchten_derivative_matches_finite_difference():
+    h = -np.linspace(0.05, 20, 50)
+    eps = 1e-6 * np.abs(h)
+    Sp, _, _ = vg(2.0, 1.8, 0.14, h + eps)
+    Sm, _, _ = vg(2.0, 1.8, 0.14, h - eps)
+    _, dSw, _ = vg(2.0, 1.8, 0.14, h)
+    assert np.allclose(dSw, (Sp - Sm) / (2 * eps), rtol=1e-6)
+
+
+# ---------------------------------------------------------------- geometry
+@pytest.fixture(scope="module")
+def p2():
+    return fb.make_problem("richards2d", nx=41, ny=21)
+
+
+@pytest.fixture(scope="module")
+def p3():
+    return fb.make_problem("richards3d", nx=10, ny=8, nz=5, Lx=10.0, Ly=8.0, Lz=5.0)
+
+
+def interior_nodes(p):
+    a = p.arrays()
+    bnd = set(a["bface_nodes"].ravel().tolist())
+    return np.array([i for i in range(p.n_nodes) if i not in bnd])
+
+
+@pytest.mark.parametrize("which,vol", [("p2", 50.0), ("p3", 400.0)])
+def test_control_volumes_tile_domain(which, vol, request):
+    p = request.getfixturevalue(which)
+    o = Oracle(p)
+    V = o.volumes()
+    assert (V > 0).all()
+    assert abs(V.sum() - vol) < 1e-10 * vol
+    # median dual: each node holds 1/(dim+1) of its elements
+    a = p.arrays()
+    X, e = a["coords"], a["elem_nodes"]
+    if p.mesh.dim == 2:
+        meas = 0.5 * np.abs((X[e[:, 1], 0] - X[e[:, 0], 0]) * (X[e[:, 2], 1] - X[e[:, 0], 1])
+                            - (X[e[:, 1], 1] - X[e[:, 0], 1]) * (X[e[:, 2], 0] - X[e[:, 0], 0]))
+    else:
+        meas = np.abs(np.einsum("ij,ij->i", X[e[:, 1]] - X[e[:, 0]],
+                                np.cross(X[e[:, 2]] - X[e[:, 0]], X[e[:, 3]] - X[e[:, 0]]))) / 6
+    Vm = np.zeros(p.n_nodes)
+    np.add.at(Vm, e.ravel(), np.repeat(meas / e.shape[1], e.shape[1]))
+    assert np.allclose(V, Vm, rtol=1e-12)
+
+
+@pytest.mark.parametrize("which", ["p2", "p3"])
+def test_control_volume_surfaces_close(which, request):
+    p = request.getfixturevalue(which)
+    o = Oracle(p)
+    S = o.cv_normal_sums()
+    inter = interior_nodes(p)
+    assert np.abs(S[inter]).max() < 1e-13
+
+
+@pytest.mark.parametrize("which", ["p2", "p3"])
+def test_hydrostatic_state_has_zero_interior_flux(which, request):
+    p = request.getfixturevalue(which)
+    o = Oracle(p)
+    a = p.arrays()
+    vert = a["coords"][:, 1 if p.mesh.dim == 2 else 2]
+    y = 3.0 - vert
+    r = o.residual(0.0, y, np.zeros_like(y))
+    inter = interior_nodes(p)
+    free = a["node_tag"][inter] == 0
+    assert np.abs(r[inter][free]).max() < 1e-12
+
+
+def test_linear_saturated_field_is_divergence_free(p3):
+    # single zone, constant K on a small box: any linear head field carries a
+    # constant Darcy flux, so every closed control volume balances exactly
+    p = fb.Problem("3d", nx=6, ny=5, nz=4, Lx=6.0, Ly=5.0, Lz=4.0, ln_var=0.0)
+    o = Oracle(p)
+    X = p.arrays()["coords"]
+    y = 20.0 + 0.3 * X[:, 0] - 0.2 * X[:, 1] + 0.1 * X[:, 2]
+    r = o.residual(0.0, y, np.zeros_like(y))
+    inter = interior_nodes(p)
+    scale = 1000 * 1e-5
+    assert np.abs(r[inter]).max() < 1e-12 * scale
+
+
+def test_mass_balance_without_dirichlet_rows():
+    # with no Dirichlet rows every interior CV face appears twice with
+    # opposite signs: sum_i V_i F_i = boundary inflow - storage
+    p = fb.Problem("3d", nx=6, ny=5, nz=4, Lx=6.0, Ly=5.0, Lz=4.0, ln_var=0.5, seed=3)
+    m = p.mesh
+    tags = np.ctypeslib.as_array(m.node_tag, (m.n_nodes,))
+    tags[:] = 0
+    o = Oracle(p)
+    X = p.arrays()["coords"]
+    rng = np.random.default_rng(0)
+    y = 2.0 - X[:, 2] + 0.3 * rng.standard_normal(p.n_nodes)
+    yp = 1e-6 * rng.standard_normal(p.n_nodes)
+    r = o.residual(0.0, y, yp)
+    V = o.volumes()
+    ahh = o.ahh()
+    a = p.arrays()
+    # recharge: 1e-7 m/s inflow on the 6 x 5 m top face
+    inflow = 1000.0 * 1e-7 * 30.0
+    lhs = (V * r).sum()
+    rhs = inflow - (V * ahh * yp).sum()
+    assert abs(lhs - rhs) < 1e-10 * (abs(inflow) + np.abs(V * ahh * yp).sum())
+
+
+def test_upwinding_picks_the_upstream_node(p2):
+    o = Oracle(p2)
+    X = p2.arrays()["coords"]
+    # water flows towards -x when head rises with x: upwind = larger-x node
+    y = -2.0 - X[:, 1] + 0.5 * X[:, 0]
+    o.begin_step(0.0, y, np.zeros_like(y))
+    w = o.upwind()
+    E = len(w)
+    front = np.zeros(E, np.int32)
+    back = np.zeros(E, np.int32)
+    import oracle.pyoracle as po
+    po.lib().orc_edges(o._c, front.ctypes.data, back.ctypes.data)
+    dx = X[front, 0] - X[back, 0]
+    horiz = np.abs(X[front, 1] - X[back, 1]) < 1e-3 * np.abs(dx)
+    up_front = w == 1
+    # horizontal edges: upstream is the node with larger x
+    sel = horiz & (np.abs(dx) > 1e-3)
+    assert sel.sum() > 10
+    assert np.all(up_front[sel] == (dx[sel] > 0))
+
+
+# ---------------------------------------------------------------- Jacobian / ILU / GMRES
+def setup_state(p, seed=0):
+    a = p.arrays()
+    vert = a["coords"][:, 1 if p.mesh.dim == 2 else 2]
+    rng = np.random.default_rng(seed)
+    y = p.water_table - vert + 0.05 * rng.standard_normal(p.n_nodes)
+    y[a["node_tag"] != 0] = (p.water_table - vert)[a["node_tag"] != 0]
+    if p.mesh.dim == 2:
+        y[a["node_tag"] == 2] = 0.0
+    yp = 1e-6 * rng.standard_normal(p.n_nodes)
+    return y, yp
+
+
+def test_fd_jacobian_matches_directional_derivative(p2):
+    o = Oracle(p2)
+    y, yp = setup_state(p2)
+    o.begin_step(0.0, y, yp)
+    F0 = o.residual(0.0, y, yp)
+    ewt = 1.0 / (1e-6 * np.abs(y) + 1e-6)
+    cj = 1e-3
+    assert o.psetup(0.0, cj, 1e3, y, yp, F0, ewt, 1) == 0
+    rp, col, val, colour = o.jacobian()
+    # distance-2 colouring: no two columns of one colour share a row
+    for i in range(p2.n_nodes):
+        cs = colour[col[rp[i]:rp[i + 1]]]
+        assert len(set(cs.tolist())) == len(cs)
+    v = np.random.default_rng(1).standard_normal(p2.n_nodes)
+    Jv_mat = np.array([val[rp[i]:rp[i + 1]] @ v[col[rp[i]:rp[i + 1]]] for i in range(p2.n_nodes)])
+    sigma = 1e-7
+    Jv_fd = o.jv(0.0, cj, y, yp, F0, v, sigma)
+    # krw has an infinite slope at h = 0-, so rows touching near-saturated
+    # nodes are not differentiable to FD accuracy; compare the smooth rows
+    smooth = np.array([np.all(y[col[rp[i]:rp[i + 1]]] < -0.05) for i in range(p2.n_nodes)])
+    assert smooth.sum() > p2.n_nodes // 2
+    scale = np.abs(val).max() * np.abs(v).max()
+    assert np.abs(Jv_mat - Jv_fd)[smooth].max() < 1e-4 * scale
+
+
+def test_global_ilu0_is_exact_on_its_pattern(p2):
+    # ILU(0) reproduces A on the sparsity pattern: (L U)_ij = A_ij there
+    o = Oracle(p2)
+    y, yp = setup_state(p2, 3)
+    F0 = o.residual(0.0, y, yp)
+    ewt = 1.0 / (1e-6 * np.abs(y) + 1e-6)
+    assert o.psetup(0.0, 1e-2, 1e2, y, yp, F0, ewt, 1) == 0
+    rp, col, val, _ = o.jacobian()
+    N = p2.n_nodes
+    # apply P^-1 to A e_j for a few j and compare with e_j where the fill
+    # ignored by ILU(0) is small: check P^-1 A x ~ x in the weighted sense
+    x = np.random.default_rng(2).standard_normal(N)
+    Ax = np.array([val[rp[i]:rp[i + 1]] @ x[col[rp[i]:rp[i + 1]]] for i in range(N)])
+    z = o.psolve(Ax)
+    assert np.linalg.norm(z - x) < 0.5 * np.linalg.norm(x)
+
+
+def test_gmres_solves_the_newton_system(p2):
+    o = Oracle(p2)
+    y, yp = setup_state(p2, 4)
+    o.begin_step(0.0, y, yp)
+    F0 = o.residual(0.0, y, yp)
+    ewt = 1.0 / (1e-6 * np.abs(y) + 1e-6)
+    cj = 1e-2
+    assert o.psetup(0.0, cj, 1e2, y, yp, F0, ewt, 2) == 0
+    rc, x, its, rn = o.gmres(cj, y, yp, F0, ewt, F0, m=30, tol=1e-6)
+    assert rc == 0 and rn <= 1e-6 and its > 0
+    # check the true residual with the difference quotient
+    sig = 1.0 / np.sqrt(np.mean((x * ewt) ** 2))
+    Jx = o.jv(0.0, cj, y, yp, F0, x, sig)
+    # the difference quotient is only consistent to about one weighted unit
+    # times the curvature of F, so the true residual is checked loosely
+    assert np.sqrt(np.mean(((F0 - Jx) * ewt) ** 2)) < 0.05
+
+
+def test_block_ilu_given_matrix_is_deterministic(p2):
+    o = Oracle(p2)
+    y, yp = setup_state(p2, 5)
+    F0 = o.residual(0.0, y, yp)
+    ewt = 1.0 / (1e-6 * np.abs(y) + 1e-6)
+    o.psetup(0.0, 1e-2, 1e2, y, yp, F0, ewt, 3)
+    _, _, val, _ = o.jacobian()
+    r = np.random.default_rng(6).standard_normal(p2.n_nodes)
+    factor_given(o, val, 3)
+    z1 = o.psolve(r)
+    factor_given(o, val, 3)
+    z2 = o.psolve(r)
+    assert np.array_equal(z1, z2)
+
+
+def test_oracle_integration_short_horizon():
+    p = fb.make_problem("richards2d", nx=21, ny=11)
+    o = Oracle(p)
+    a = p.arrays()
+    y0 = p.water_table - a["coords"][:, 1]
+    y0[a["node_tag"] == 2] = 0.0
+    opts = fb.default_opts(krylov_dim=20, max_order=5)
+    rc, yend, st = o.integrate(opts, 1, 0.0, 3600.0, y0)
+    assert rc == 0, st
+    assert abs(st["t"] - 3600.0) < 1e-6
+    assert np.isfinite(yend).all()
+    # infiltration under the ponded strip raises the head below it
+    assert st["nst"] > 5 and st["nni"] >= st["nst"]
+    top = a["node_tag"] == 2
+    assert np.all(yend[top] == 0.0)
+    below = (np.abs(a["coords"][:, 1] - 4.75) < 0.01) & (np.abs(a["coords"][:, 0] - 5.0) < 0.6)
+    assert np.all(yend[below] > y0[below])
