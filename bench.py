@@ -197,7 +197,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--days", type=float, default=30.0)
@@ -234,6 +234,7 @@ def main():
         torch.cuda.synchronize()
         if profile:
             ph.profile(True)
+        c0 = ph.counters()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         stats = []
         e0.record()
@@ -248,9 +249,11 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
+        c1 = ph.counters()
         prof = ph.profile_read() if profile else None
         if profile:
             ph.profile(False)
+            prof["_launches"] = (0.0, c1["launches"] - c0["launches"])
         barrier(ws)
         return max_over_ranks(ms, ws, dev), stats, prof
 
@@ -258,12 +261,16 @@ def main():
         mixed.integrate(0.0, horizon, y0, yend)
     with ClockSampler(local) as clk:
         ms_mixed, st_mixed, prof = timed(mixed, args.steps, profile=True)
-    ms_plain, st_plain, _ = timed(plain, args.steps)
-    ms_e2e, _, _ = timed(mixed, args.steps, host=True)
+    # the plain FP64 path and the host-buffer path are timed on fewer runs
+    # (each run is a whole 30-day integration) to keep the bench short
+    k_extra = max(1, args.steps // 2)
+    plain.integrate(0.0, horizon, y0, yend)   # warm the FP64 factor/basis buffers
+    ms_plain, st_plain, _ = timed(plain, k_extra)
+    ms_e2e, _, _ = timed(mixed, k_extra, host=True)
     sim = horizon * args.steps * ws
     value = sim / (ms_mixed / 1e3)
-    plain_value = sim / (ms_plain / 1e3)
-    e2e_value = sim / (ms_e2e / 1e3)
+    plain_value = horizon * k_extra * ws / (ms_plain / 1e3)
+    e2e_value = horizon * k_extra * ws / (ms_e2e / 1e3)
 
     # roofline of the residual evaluation (node pass + element pass + gather):
     # algorithmic bytes 36 B/node + 270 B/tet per evaluation
@@ -284,7 +291,7 @@ def main():
                    "path": "FP32 block-ILU(0) + FP32 GMRES(40) basis, FP64 residual/Newton/LSQ",
                    "rtol": 1e-6, "atol": 1e-6, "l2": "inputs larger than L2 (331 MB per residual)",
                    "parallelism": f"replicas x{ws}"},
-        "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain / args.steps,
+        "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain / k_extra, "runs": k_extra,
                        "ratio_mixed_over_plain": value / plain_value,
                        "stats": {k: st_plain[0][k] for k in ("nst", "nni", "nli", "npe", "nre")}},
         "stats": {k: st0[k] for k in ("nst", "nni", "nli", "npe", "nps", "nre", "ncfn", "netf", "last_order")},
@@ -298,9 +305,10 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N},
         "clocks": clocks,
     }
-    # launches of our kernels inside the timed region: 3 per residual
-    # evaluation plus the Krylov / preconditioner / controller kernels
-    line["gpu_launches"] = int(sum(v[1] for v in prof.values()) + 0)
+    # every kernel launch of the library inside the timed region (counted by
+    # the context: residual chain, Krylov, preconditioner, controller)
+    line["gpu_launches"] = int(prof.pop("_launches")[1])
+    line["kernel_ms"].pop("_launches", None)
     if rank == 0 and not args.no_cpu_baseline:
         v, wall, msteps, st = cpu_sample(15.0)
         # the GPU over the very same prefix, for a like-for-like ratio

@@ -140,6 +140,7 @@ def _declare(L):
     L.fvm_precond_jacobian.argtypes = [_P, _P, _P, _P]
     L.fvm_profile.argtypes = [_P, _I]
     L.fvm_profile_read.argtypes = [_P, _P, _P]
+    L.fvm_counters.argtypes = [_P, C.POINTER(C.c_long), C.POINTER(C.c_long)]
 
 
 PROFILE_CATEGORIES = ("node", "element", "gather", "ilu_apply", "gram_schmidt", "ilu_factor", "fd_jacobian")
@@ -283,6 +284,11 @@ class Physics:
 
     def profile(self, enable: bool):
         _check(lib().fvm_profile(self._c, 1 if enable else 0), "fvm_profile")
+
+    def counters(self):
+        a, b = C.c_long(), C.c_long()
+        _check(lib().fvm_counters(self._c, C.byref(a), C.byref(b)), "fvm_counters")
+        return {"launches": a.value, "residuals": b.value}
 
     def profile_read(self):
         ms = np.zeros(len(PROFILE_CATEGORIES))

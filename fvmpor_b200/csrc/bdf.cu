@@ -181,18 +181,18 @@ struct DeviceOps {
     // ---- controller interface
     void set_time(double t) { tcur = t; }
     void ewt_from_phi0(double rtol, double atol) {
-        k_ewt<<<g(), 256, 0, c->stream>>>(N, phi[0].p, rtol, atol, ewt.p);
+        fvm_launch(c, k_ewt, g(), 256, 0, c->stream, N, phi[0].p, rtol, atol, ewt.p);
     }
     void begin_step() { launch_begin_step(c, phi[0].p, yp.p); }
     void phi_scale(int j0, int j1, const double* f) {
         Coef7 cf;
         for (int j = 0; j < kNPhi; ++j) cf.v[j] = f[j];
-        k_phi_scale<<<g(), 256, 0, c->stream>>>(N, j0, j1, ptrs(), cf);
+        fvm_launch(c, k_phi_scale, g(), 256, 0, c->stream, N, j0, j1, ptrs(), cf);
     }
     void predict(int k, const double* gamma) {
         Coef7 gm;
         for (int j = 0; j < kNPhi; ++j) gm.v[j] = gamma[j];
-        k_predict<<<g(), 256, 0, c->stream>>>(N, k, ptrs(), gm, y.p, yp.p, e.p);
+        fvm_launch(c, k_predict, g(), 256, 0, c->stream, N, k, ptrs(), gm, y.p, yp.p, e.p);
     }
     double wrms_y() { return std::sqrt(reduce_sumsq(c, y.p, ewt.p) / N); }
     void residual() {
@@ -212,18 +212,18 @@ struct DeviceOps {
         return r;
     }
     double newton_update(double cj) {
-        k_newton_update<<<kRedBlocks, kRedThreads, 0, c->stream>>>(N, x.p, cj, ewt.p, y.p, yp.p, e.p,
+        fvm_launch(c, k_newton_update, kRedBlocks, kRedThreads, 0, c->stream, N, x.p, cj, ewt.p, y.p, yp.p, e.p,
                                                                    partial.p, counter.p, res.p);
         return std::sqrt(fetch(1) / N);
     }
     void err_norms(int k, double out[4]) {
-        k_err_norms<<<kRedBlocks, kRedThreads, 0, c->stream>>>(N, k, ptrs(), e.p, ewt.p, partial.p,
+        fvm_launch(c, k_err_norms, kRedBlocks, kRedThreads, 0, c->stream, N, k, ptrs(), e.p, ewt.p, partial.p,
                                                                counter.p, res.p);
         fetch(4);
         for (int q = 0; q < 4; ++q) out[q] = std::sqrt(host[q] / N);
     }
     void phi_update(int k, int set_kp2) {
-        k_phi_update<<<g(), 256, 0, c->stream>>>(N, k, set_kp2, ptrs(), e.p);
+        fvm_launch(c, k_phi_update, g(), 256, 0, c->stream, N, k, set_kp2, ptrs(), e.p);
     }
     bool newton_guess(double tnew, double cj) {
         if (!pred) return false;
@@ -234,17 +234,18 @@ struct DeviceOps {
     double start(double t0, const double* y0, double tout) {
         cudaStream_t s = c->stream;
         FVM_CUDA(cudaMemcpyAsync(y.p, y0, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
-        k_fill<<<g(), 256, 0, s>>>(N, 0.0, yp.p);
+        reset_upwind(c);   // averaged weights for the initial residual
+        fvm_launch(c, k_fill, g(), 256, 0, s, N, 0.0, yp.p);
         Perturb none;
         launch_residual(c, y.p, yp.p, none, nullptr, F.p);
-        k_fill<<<g(), 256, 0, s>>>(N, 1.0, tmp.p);
+        fvm_launch(c, k_fill, g(), 256, 0, s, N, 1.0, tmp.p);
         launch_residual(c, y.p, tmp.p, none, nullptr, x.p);   // leaves ahh * 1 in c->stor
-        k_initial_yp<<<g(), 256, 0, s>>>(N, F.p, c->stor.p, c->ntype.p, yp.p);
-        k_ewt<<<g(), 256, 0, s>>>(N, y.p, o.rtol, o.atol, ewt.p);
+        fvm_launch(c, k_initial_yp, g(), 256, 0, s, N, F.p, c->stor.p, c->ntype.p, yp.p);
+        fvm_launch(c, k_ewt, g(), 256, 0, s, N, y.p, o.rtol, o.atol, ewt.p);
         double ypn = std::sqrt(reduce_sumsq(c, yp.p, ewt.p) / N);
         double h = bdf_first_step(t0, tout, ypn, o.h0, o.hmax);
         FVM_CUDA(cudaMemcpyAsync(phi[0].p, y.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
-        k_scale_vec<<<g(), 256, 0, s>>>(N, h, yp.p, phi[1].p);
+        fvm_launch(c, k_scale_vec, g(), 256, 0, s, N, h, yp.p, phi[1].p);
         return h;
     }
 };

@@ -125,7 +125,11 @@ template <class Ops> struct BdfController {
             double pnorm = ops.wrms_y();
             if (o.use_guess && ops.newton_guess(tnew, cj)) st.npred++;
             bool converged = false, fresh_p = false;
-            bool need_p = !have_p || std::fabs(cj / cj_p - 1.0) > 0.25 || (st.nst - nst_p) >= 20;
+            // refresh the preconditioner on the first step, when cj has moved
+            // by more than a factor of two since the last factorisation, every
+            // 20 steps, and (below) after a corrector failure with a stale one
+            double cjr = have_p ? cj / cj_p : 0.0;
+            bool need_p = !have_p || cjr < 0.5 || cjr > 2.0 || (st.nst - nst_p) >= 20;
             for (int attempt = 0; attempt < 2 && !converged; ++attempt) {
                 if (attempt == 1) {
                     if (fresh_p) break;

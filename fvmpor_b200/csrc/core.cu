@@ -91,7 +91,8 @@ __global__ void __launch_bounds__(256) k_elem_tet(int T, int N, const int4* __re
                                                    const double* __restrict__ krw,
                                                    const double* __restrict__ h,
                                                    const unsigned char* __restrict__ upw,
-                                                   double rho0, double* __restrict__ contrib) {
+                                                   double rho0, const int4* __restrict__ epos,
+                                                   double* __restrict__ slots) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= T) return;
     int4 nd = en[e];
@@ -114,9 +115,11 @@ __global__ void __launch_bounds__(256) k_elem_tet(int T, int N, const int4* __re
         c[a] -= flux;
         c[b] += flux;
     }
-    double2* out = reinterpret_cast<double2*>(contrib + (size_t)4 * e);
-    out[0] = make_double2(c[0], c[1]);
-    out[1] = make_double2(c[2], c[3]);
+    int4 ps = epos[e];
+    slots[ps.x] = c[0];
+    slots[ps.y] = c[1];
+    slots[ps.z] = c[2];
+    slots[ps.w] = c[3];
 }
 
 // recompute-geometry element pass, tetrahedra: the face coefficients are
@@ -129,7 +132,8 @@ __global__ void __launch_bounds__(256) k_elem_tet_rc(int T, int N, const int4* _
                                                       const double* __restrict__ krw,
                                                       const double* __restrict__ h,
                                                       const unsigned char* __restrict__ upw,
-                                                      double rho0, double* __restrict__ contrib) {
+                                                      double rho0, const int4* __restrict__ epos,
+                                                      double* __restrict__ slots) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= T) return;
     int4 nd = en[e];
@@ -161,9 +165,11 @@ __global__ void __launch_bounds__(256) k_elem_tet_rc(int T, int N, const int4* _
         c[a] -= flux;
         c[b] += flux;
     }
-    double2* out = reinterpret_cast<double2*>(contrib + (size_t)4 * e);
-    out[0] = make_double2(c[0], c[1]);
-    out[1] = make_double2(c[2], c[3]);
+    int4 ps = epos[e];
+    slots[ps.x] = c[0];
+    slots[ps.y] = c[1];
+    slots[ps.z] = c[2];
+    slots[ps.w] = c[3];
 }
 
 template <bool MULTIZONE>
@@ -173,7 +179,8 @@ __global__ void __launch_bounds__(256) k_elem_tri(int T, int N, const int4* __re
                                                    const double* __restrict__ krw,
                                                    const double* __restrict__ h,
                                                    const unsigned char* __restrict__ upw,
-                                                   double rho0, double* __restrict__ contrib) {
+                                                   double rho0, const int4* __restrict__ epos,
+                                                   double* __restrict__ slots) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= T) return;
     int4 nd = en[e];
@@ -195,15 +202,18 @@ __global__ void __launch_bounds__(256) k_elem_tri(int T, int N, const int4* __re
         c[a] -= flux;
         c[b] += flux;
     }
-    double* out = contrib + (size_t)3 * e;
-    out[0] = c[0];
-    out[1] = c[1];
-    out[2] = c[2];
+    int4 ps = epos[e];
+    slots[ps.x] = c[0];
+    slots[ps.y] = c[1];
+    slots[ps.z] = c[2];
 }
 
-// node gather; F0 != nullptr turns the result into (F - F0) * inv_sigma
-__global__ void k_gather(int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc,
-                         const double* __restrict__ contrib, const double* __restrict__ invV,
+// node gather: the element pass left node i's partials in the contiguous
+// slot range [inc_ptr[i], inc_ptr[i+1]) in ascending element order; sum
+// them in that order.  F0 != nullptr turns the result into
+// (F - F0) * inv_sigma.
+__global__ void k_gather(int N, const int* __restrict__ inc_ptr,
+                         const double* __restrict__ slots, const double* __restrict__ invV,
                          const double* __restrict__ bterm, const double* __restrict__ hD,
                          const unsigned char* __restrict__ ntype, const double* __restrict__ h,
                          const double* __restrict__ stor, const double* __restrict__ F0,
@@ -217,7 +227,7 @@ __global__ void k_gather(int N, const int* __restrict__ inc_ptr, const int* __re
     } else {
         double s = 0.0;
         int p1 = inc_ptr[i + 1];
-        for (int p = inc_ptr[i]; p < p1; ++p) s += contrib[inc[p]];
+        for (int p = inc_ptr[i]; p < p1; ++p) s += slots[p];
         r = s * invV[i];
         r = r + bterm[i];
         r = r - stor[i];
@@ -287,7 +297,7 @@ void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Pertur
     cudaStream_t s = c->stream;
     const double* h = pt.mode ? c->hstar.p : y;
     c->tm.begin(TM_NODE, s);
-    k_node<<<grid_for(c->N, kBlock), kBlock, 0, s>>>(c->N, y, yp, pt, c->zones.p, c->nz, c->nz_ptr.p,
+    fvm_launch(c, k_node, grid_for(c->N, kBlock), kBlock, 0, s, c->N, y, yp, pt, c->zones.p, c->nz, c->nz_ptr.p,
                                                       c->nz_zone.p, c->nz_w.p, c->rho0, c->krw.p,
                                                       c->hstar.p, c->stor.p);
     c->tm.end(TM_NODE, s);
@@ -296,26 +306,26 @@ void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Pertur
     if (c->dim == 3) {
         if (c->recompute) {
             if (c->nz > 1)
-                k_elem_tet_rc<true><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->xyz.p, c->eK.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->contrib.p);
+                fvm_launch(c, k_elem_tet_rc<true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->xyz.p, c->eK.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
             else
-                k_elem_tet_rc<false><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->xyz.p, c->eK.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->contrib.p);
+                fvm_launch(c, k_elem_tet_rc<false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->xyz.p, c->eK.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
         } else {
             if (c->nz > 1)
-                k_elem_tet<true><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->contrib.p);
+                fvm_launch(c, k_elem_tet<true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
             else
-                k_elem_tet<false><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->contrib.p);
+                fvm_launch(c, k_elem_tet<false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
         }
     } else {
         if (c->nz > 1)
-            k_elem_tri<true><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->contrib.p);
+            fvm_launch(c, k_elem_tri<true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
         else
-            k_elem_tri<false><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->contrib.p);
+            fvm_launch(c, k_elem_tri<false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
     }
     c->tm.end(TM_ELEM, s);
     double inv_sigma = 0.0;
     if (F0 && !pt.sigma_dev) inv_sigma = 1.0 / pt.sigma;
     c->tm.begin(TM_GATHER, s);
-    k_gather<<<grid_for(c->N, kBlock), kBlock, 0, s>>>(c->N, c->inc_ptr.p, c->inc.p, c->contrib.p,
+    fvm_launch(c, k_gather, grid_for(c->N, kBlock), kBlock, 0, s, c->N, c->inc_ptr.p, c->slots.p,
                                                         c->invV.p, c->bterm.p, c->hD.p, c->ntype.p,
                                                         h, c->stor.p, F0, inv_sigma,
                                                         F0 ? pt.sigma_dev : nullptr, out);
@@ -326,19 +336,23 @@ void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Pertur
 void launch_begin_step(fvm_ctx* c, const double* y, const double* yp) {
     cudaStream_t s = c->stream;
     Perturb none;
-    k_node<<<grid_for(c->N, kBlock), kBlock, 0, s>>>(c->N, y, yp, none, c->zones.p, c->nz, c->nz_ptr.p,
+    fvm_launch(c, k_node, grid_for(c->N, kBlock), kBlock, 0, s, c->N, y, yp, none, c->zones.p, c->nz, c->nz_ptr.p,
                                                       c->nz_zone.p, c->nz_w.p, c->rho0, c->krw.p,
                                                       c->hstar.p, c->stor.p);
     int gb = grid_for(c->T, kBlock);
     if (c->dim == 3) {
-        if (c->nz > 1) k_faceq<4, 6, true><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
-        else k_faceq<4, 6, false><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
+        if (c->nz > 1) fvm_launch(c, k_faceq<4, 6, true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
+        else fvm_launch(c, k_faceq<4, 6, false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
     } else {
-        if (c->nz > 1) k_faceq<3, 3, true><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
-        else k_faceq<3, 3, false><<<gb, kBlock, 0, s>>>(c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
+        if (c->nz > 1) fvm_launch(c, k_faceq<3, 3, true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
+        else fvm_launch(c, k_faceq<3, 3, false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
     }
-    k_edge_upwind<<<grid_for(c->E, kBlock), kBlock, 0, s>>>(c->E, c->nfe, c->edge_ptr.p, c->edge_face.p,
+    fvm_launch(c, k_edge_upwind, grid_for(c->E, kBlock), kBlock, 0, s, c->E, c->nfe, c->edge_ptr.p, c->edge_face.p,
                                                               c->edge_w.p, c->faceq.p, c->flip.p, c->upw.p);
+}
+
+void reset_upwind(fvm_ctx* c) {
+    FVM_CUDA(cudaMemsetAsync(c->upw.p, 2, c->upw.n, c->stream));
 }
 
 // ------------------------------------------------------------------ set-up
@@ -542,6 +556,16 @@ static void build(fvm_ctx* c, const fvm_mesh* m, const fvm_physics* ph, int flag
     c->nz_w.upload(nz_w, s);
     c->inc_ptr.upload(inc_ptr, s);
     c->inc.upload(inc, s);
+    {
+        // slot of (e, k) in the node-ordered partial array: the inverse of inc
+        std::vector<int4> epos(T, make_int4(0, 0, 0, 0));
+        for (size_t p = 0; p < inc.size(); ++p) {
+            int e = inc[p] / npe, k = inc[p] % npe;
+            int* q = reinterpret_cast<int*>(&epos[e]);
+            q[k] = (int)p;
+        }
+        c->epos.upload(epos, s);
+    }
     std::vector<ZoneDev> zd(ph->n_zones);
     for (int z = 0; z < ph->n_zones; ++z) {
         const fvm_zone& Z = ph->zones[z];
@@ -559,7 +583,7 @@ static void build(fvm_ctx* c, const fvm_mesh* m, const fvm_physics* ph, int flag
     c->krw.zero(s);
     c->hstar.alloc(N);
     c->stor.alloc(N);
-    c->contrib.alloc((size_t)T * npe);
+    c->slots.alloc((size_t)T * npe);
     c->faceq.alloc((size_t)T * nfe);
     for (auto& b : c->tmpN) b.alloc(N);
     FVM_CUDA(cudaStreamSynchronize(s));
@@ -681,6 +705,15 @@ extern "C" int fvm_profile_read(fvm_ctx* c, double* ms, long* counts) {
         if (ms) ms[k] = c->tm.ms[k];
         if (counts) counts[k] = c->tm.count[k];
     }
+    return 0;
+    FVM_API_END
+}
+
+extern "C" int fvm_counters(fvm_ctx* c, long* launches, long* residuals) {
+    FVM_API_BEGIN
+    if (!c) throw Error("fvm_counters: null context");
+    if (launches) *launches = c->launches;
+    if (residuals) *residuals = c->n_residuals;
     return 0;
     FVM_API_END
 }

@@ -10,6 +10,7 @@
 
 #include <cmath>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace fvmb {
@@ -54,12 +55,20 @@ struct ZoneDev {
     double phi, alpha, n, m, Sr;
 };
 
-// Van Genuchten-Mualem relations in the operation order of
-// VarSatPhysicsImpl::saturation (examples/fvmporMinlin/fvmpor.h:302-343):
+// Van Genuchten-Mualem relations of VarSatPhysicsImpl::saturation
+// (examples/fvmporMinlin/fvmpor.h:302-343):
 //   a = (-alpha h)^n, b = 1 + a, Se = b^-m, Sw = S_r + (1 - S_r) Se,
 //   dSw/dh = -(1 - S_r)(n - 1) (a / b) Se / h,
 //   krw = sqrt(Se) ((a / b)^m - 1)^2,
 // overridden by Sw = 1, dSw = 0, krw = 1 for h >= 0.
+// The reference evaluates three pow() calls; here the powers share their
+// logarithms: with L = ln(-alpha h) and lb = ln(1 + a),
+//   a = exp(n L), Se = exp(-m lb), (a/b)^m = exp(m (n L - lb)),
+// one log, one log1p, two exp and one expm1 instead of three pow (each a
+// log and an exp in extended precision); expm1 also removes the
+// cancellation in (a/b)^m - 1 that the pow form suffers for dry nodes.  The
+// FP64 node pass is bound by these transcendentals; values agree with the
+// pow() form to a few ulp (more where pow() cancels).
 FVM_HD void van_genuchten(double h, const ZoneDev& z, double& Sw, double& dSw, double& krw) {
     if (h >= 0.0) {
         Sw = 1.0;
@@ -67,17 +76,16 @@ FVM_HD void van_genuchten(double h, const ZoneDev& z, double& Sw, double& dSw, d
         krw = 1.0;
         return;
     }
-    double a = pow(-z.alpha * h, z.n);
-    double b = a + 1.0;
-    double k = -1.0 / b;
-    double d = a / b;
-    double Se = pow(b, -z.m);
+    double L = log(-z.alpha * h);
+    double nL = z.n * L;
+    double a = exp(nL);
+    double lb = log1p(a);
+    double Se = exp(-z.m * lb);
+    double d = a / (1.0 + a);
     d = d * Se;
     d = d / h;
     d = d * (-(1.0 - z.Sr) * (z.n - 1.0));
-    k = k + 1.0;
-    k = pow(k, z.m);
-    k = k - 1.0;
+    double k = expm1(z.m * (nL - lb));   // (a / b)^m - 1 without cancellation
     k = k * k;
     k = k * sqrt(Se);
     Sw = Se * (1.0 - z.Sr) + z.Sr;
@@ -149,7 +157,8 @@ struct fvm_ctx {
     fvmb::DevBuf<double> krw;        // [nz][N]
     fvmb::DevBuf<double> hstar;      // perturbed head
     fvmb::DevBuf<double> stor;       // ahh * y'
-    fvmb::DevBuf<double> contrib;    // [T*npe] element flux sums per node
+    fvmb::DevBuf<double> slots;      // [T*npe] element partials in node order
+    fvmb::DevBuf<int4> epos;         // [T] slot of each element node (4th = 0 in 2D)
     fvmb::DevBuf<double> faceq;      // [T*nfe] averaged-weight face fluxes
     fvmb::DevBuf<double> tmpN[4];    // scratch vectors
 
@@ -157,17 +166,29 @@ struct fvm_ctx {
     fvmb::Krylov* kry = nullptr;
 
     long n_residuals = 0;
+    long launches = 0;               // kernels launched on this context
     fvmb::KernelTimer tm;
     std::string err;
 };
 
 namespace fvmb {
 
+// every kernel of the library is launched through this, so the context
+// can report how many of its kernels ran
+template <typename... KArgs, typename... Args>
+inline void fvm_launch(fvm_ctx* c, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t s, Args&&... args) {
+    k<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+    c->launches++;
+}
+
 // residual driver shared by fvm_residual / fvm_jv / the FD Jacobian
 // out = F(t, y~, y'~) (or (F - F0) / sigma when F0 != nullptr)
 void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Perturb& pt,
                      const double* F0, double* out);
 void launch_begin_step(fvm_ctx* c, const double* y, const double* yp);
+// back to the averaged 0.5/0.5 face weights used before the first step
+void reset_upwind(fvm_ctx* c);
 
 inline int grid_for(long n, int block) { return (int)((n + block - 1) / block); }
 

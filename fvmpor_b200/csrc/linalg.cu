@@ -1,11 +1,15 @@
-// Reductions, WRMS norms and right-preconditioned restarted GMRES.
+// Reductions, WRMS norms and preconditioned restarted GMRES.
 //
-// Algorithm: decomp/gmres.c:26-201 (restarted, right-preconditioned
-// GMRES(m)), arnoldi :412-511 and the Givens least squares of
-// decomp/linalg_dense.c:128-173, applied as IDAS SPGMR applies it inside
-// Newton: zero initial guess, residual measured in the WRMS norm of the
-// error weights (the system is scaled by D = diag(ewt)), J*v by a
-// difference quotient of the residual.
+// Algorithm: restarted GMRES(m) with Arnoldi and the Givens least squares
+// of decomp/gmres.c:26-201, :412-511 and decomp/linalg_dense.c:128-173,
+// applied the way IDAS SPGMR applies it inside the Newton iteration (the
+// solver the reference's hot path actually runs, ida_integrator.h:248-254):
+// zero initial guess, LEFT preconditioning, scaling by D = diag(ewt), so
+// the stopping test sees ||D P^-1 (b - J x)||_wrms -- a head-space quantity
+// comparable with the Newton tolerance.  (decomp's stand-alone gmres.c is
+// right-preconditioned; with the unscaled residual F of this problem that
+// variant measures mass-flux units against head weights.)  J*v is the
+// difference quotient of the residual with sigma = 1/||v||_wrms.
 //
 // B200 layout: the Arnoldi basis is kept as unnormalised vectors U_i with a
 // per-vector scale s_i (V_i = s_i U_i), in FP64 or FP32 (mixed precision).
@@ -213,6 +217,12 @@ __global__ void k_axpy(int N, double a, const double* __restrict__ x, double* __
     if (k < N) y[k] += a * x[k];
 }
 
+__global__ void k_sub(int N, const double* __restrict__ a, const double* __restrict__ b,
+                      double* __restrict__ out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < N) out[k] = a[k] - b[k];
+}
+
 // ------------------------------------------------------------------ Krylov
 Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
     Krylov* K = c->kry;
@@ -234,7 +244,8 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
     K->counter.zero(c->stream);
     K->res.alloc(3 * (m + 2) + 8);
     K->sigma.alloc(1);
-    FVM_CUDA(cudaMallocHost(&K->host, sizeof(double) * (3 * (m + 2) + 8)));
+    // results of the three passes plus the m+1 basis scales
+    FVM_CUDA(cudaMallocHost(&K->host, sizeof(double) * (4 * (m + 2) + 8)));
     c->kry = K;
     return K;
 }
@@ -249,7 +260,7 @@ void fvmb_destroy_krylov_impl(Krylov* K) {
 // host-synchronous reductions used by the controller
 double reduce_sumsq(fvm_ctx* c, const double* x, const double* w) {
     Krylov* K = krylov_get(c, c->kry ? c->kry->m : 1, c->kry ? c->kry->precision : 0);
-    k_sumsq<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->N, x, w, K->partial.p, K->counter.p, K->res.p);
+    fvm_launch(c, k_sumsq, kRedBlocks, kRedThreads, 0, c->stream, c->N, x, w, K->partial.p, K->counter.p, K->res.p);
     FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     FVM_CUDA(cudaStreamSynchronize(c->stream));
     return K->host[0];
@@ -257,7 +268,7 @@ double reduce_sumsq(fvm_ctx* c, const double* x, const double* w) {
 
 double reduce_dot(fvm_ctx* c, const double* x, const double* y) {
     Krylov* K = krylov_get(c, c->kry ? c->kry->m : 1, c->kry ? c->kry->precision : 0);
-    k_dot<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->N, x, y, K->partial.p, K->counter.p, K->res.p);
+    fvm_launch(c, k_dot, kRedBlocks, kRedThreads, 0, c->stream, c->N, x, y, K->partial.p, K->counter.p, K->res.p);
     FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     FVM_CUDA(cudaStreamSynchronize(c->stream));
     return K->host[0];
@@ -266,8 +277,8 @@ double reduce_dot(fvm_ctx* c, const double* x, const double* y) {
 // J*v into out, sigma = 1/||v||_wrms computed on the device
 static void jv_dev(fvm_ctx* c, Krylov* K, double cj, const double* y, const double* yp,
                    const double* F0, const double* v, const double* ewt, double* out) {
-    k_sumsq<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->N, v, ewt, K->partial.p, K->counter.p, K->res.p);
-    k_sigma_from_sumsq<<<1, 1, 0, c->stream>>>(K->res.p, c->N, K->sigma.p);
+    fvm_launch(c, k_sumsq, kRedBlocks, kRedThreads, 0, c->stream, c->N, v, ewt, K->partial.p, K->counter.p, K->res.p);
+    fvm_launch(c, k_sigma_from_sumsq, 1, 1, 0, c->stream, K->res.p, c->N, K->sigma.p);
     Perturb pt;
     pt.mode = 1;
     pt.cj = cj;
@@ -292,14 +303,19 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
     double rnorm = 0.0;
     bool have_x = false;
     for (int cycle = 0; cycle <= max_restarts; ++cycle) {
-        // residual of the current iterate
+        // preconditioned residual of the current iterate: z = P^-1 (b - J x)
         if (have_x) {
             jv_dev(c, K, cj, y, yp, F0, x, ewt, K->Jv.p);
             if (cnt) cnt->njv++;
+            fvm_launch(c, k_sub, grid_for(N, 256), 256, 0, s, N, b, K->Jv.p, K->t.p);
+            psolve_dev(c, K->t.p, K->z.p);
+        } else {
+            psolve_dev(c, b, K->z.p);
         }
-        k_init_residual<B><<<kRedBlocks, kRedThreads, 0, s>>>(N, b, have_x ? K->Jv.p : nullptr, ewt, U,
+        if (cnt) cnt->nps++;
+        fvm_launch(c, k_init_residual<B>, kRedBlocks, kRedThreads, 0, s, N, K->z.p, nullptr, ewt, U,
                                                               K->partial.p, K->counter.p, K->res.p);
-        k_set_scale<<<1, 1, 0, s>>>(K->res.p, K->scale.p, 0);
+        fvm_launch(c, k_set_scale, 1, 1, 0, s, K->res.p, K->scale.p, 0);
         FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, s));
         FVM_CUDA(cudaStreamSynchronize(s));
         double beta = std::sqrt(K->host[0]);
@@ -311,21 +327,21 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         int j = 0;
         bool conv = false;
         for (; j < m; ++j) {
-            // z = P^-1 D^-1 V_j ; w = J z
-            k_unscale<B><<<grid_for(N, 256), 256, 0, s>>>(N, U + ld * j, K->scale.p, j, ewt, K->t.p);
-            psolve_dev(c, K->t.p, K->z.p);
-            if (cnt) cnt->nps++;
-            jv_dev(c, K, cj, y, yp, F0, K->z.p, ewt, K->Jv.p);
+            // w = D P^-1 J D^-1 V_j (left preconditioning, scaled by D = ewt)
+            fvm_launch(c, k_unscale<B>, grid_for(N, 256), 256, 0, s, N, U + ld * j, K->scale.p, j, ewt, K->t.p);
+            jv_dev(c, K, cj, y, yp, F0, K->t.p, ewt, K->Jv.p);
             if (cnt) cnt->njv++;
+            psolve_dev(c, K->Jv.p, K->z.p);
+            if (cnt) cnt->nps++;
             int nv = j + 1;
             double* ra = K->res.p;
             double* rb = K->res.p + (m + 2);
             double* rn = K->res.p + 2 * (m + 2);
             c->tm.begin(TM_CGS, s);
-            k_cgs_pass1<B><<<kRedBlocks, kRedThreads, 0, s>>>(N, nv, U, ld, K->Jv.p, ewt, K->W.p, K->partial.p, K->counter.p, ra);
-            k_cgs_pass2<B><<<kRedBlocks, kRedThreads, 0, s>>>(N, nv, U, ld, K->scale.p, ra, K->W.p, K->partial.p, K->counter.p, rb);
-            k_cgs_pass3<B><<<kRedBlocks, kRedThreads, 0, s>>>(N, nv, U, ld, K->scale.p, rb, K->W.p, K->partial.p, K->counter.p, rn);
-            k_set_scale<<<1, 1, 0, s>>>(rn, K->scale.p, nv);
+            fvm_launch(c, k_cgs_pass1<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->z.p, ewt, K->W.p, K->partial.p, K->counter.p, ra);
+            fvm_launch(c, k_cgs_pass2<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->scale.p, ra, K->W.p, K->partial.p, K->counter.p, rb);
+            fvm_launch(c, k_cgs_pass3<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->scale.p, rb, K->W.p, K->partial.p, K->counter.p, rn);
+            fvm_launch(c, k_set_scale, 1, 1, 0, s, rn, K->scale.p, nv);
             c->tm.end(TM_CGS, s);
             FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, s));
             FVM_CUDA(cudaMemcpyAsync(K->host + 3 * (m + 2), K->scale.p, sizeof(double) * (nv), cudaMemcpyDeviceToHost, s));
@@ -365,14 +381,12 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
             double d = H[(size_t)i * m + i];
             yv[i] = d != 0.0 ? sacc / d : 0.0;
         }
-        // x += P^-1 D^-1 sum_i y_i V_i
+        // x += D^-1 sum_i y_i V_i  (scales of V_0..V_{kdim-1} are in the last
+        // batch copied back)
         for (int i = 0; i < kdim; ++i) K->host[i] = yv[i] * K->host[3 * (m + 2) + i];
-        // scales of the basis vectors: the last batch copied holds s_0..s_{j}
         FVM_CUDA(cudaMemcpyAsync(K->res.p, K->host, sizeof(double) * kdim, cudaMemcpyHostToDevice, s));
-        k_combine<B><<<grid_for(N, 256), 256, 0, s>>>(N, kdim, U, ld, K->res.p, ewt, K->t.p);
-        psolve_dev(c, K->t.p, K->z.p);
-        if (cnt) cnt->nps++;
-        k_axpy<<<grid_for(N, 256), 256, 0, s>>>(N, 1.0, K->z.p, x);
+        fvm_launch(c, k_combine<B>, grid_for(N, 256), 256, 0, s, N, kdim, U, ld, K->res.p, ewt, K->t.p);
+        fvm_launch(c, k_axpy, grid_for(N, 256), 256, 0, s, N, 1.0, K->t.p, x);
         have_x = true;
         if (conv) {
             FVM_CUDA(cudaStreamSynchronize(s));

@@ -52,7 +52,11 @@ struct BlockILU {
     DevBuf<int> status;
     int* h_status = nullptr;  // pinned
     int nlevels_max = 0;
+    size_t smem_stage[2] = {0, 0};   // staged apply: shared bytes for FP64 / FP32, 0 = not possible
 };
+
+// largest dynamic shared-memory carve-out a CTA may request on sm_100
+constexpr size_t kMaxDynSmem = 227 * 1024;
 
 // ------------------------------------------------------------------ kernels
 __global__ void k_shift(int N, const double* __restrict__ y, const double* __restrict__ yp,
@@ -158,6 +162,68 @@ __global__ void __launch_bounds__(128) k_ilu_apply(const int* __restrict__ bstar
         __syncthreads();
     }
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) z[i] = (double)x[i - r0];
+}
+
+// Staged variant: the CTA first copies its block's factor (values, local
+// column indices, row pointers, pivot positions) and right-hand side into
+// shared memory with coalesced loads, then runs the level loops entirely in
+// shared memory, so each level costs a few shared-memory latencies and a
+// barrier instead of a dependent chain of L2/HBM loads.
+// Shared layout: x[T nrows] | val[T nnz] | col[u16 nnz] | rp[u16 nrows+1] |
+// dg[u16 nrows]
+template <class T>
+__global__ void __launch_bounds__(256) k_ilu_apply_smem(const int* __restrict__ bstart,
+                                                        const int* __restrict__ lu_ptr,
+                                                        const int* __restrict__ lu_diag,
+                                                        const unsigned short* __restrict__ lu_col,
+                                                        const int* __restrict__ lvl_ptr,
+                                                        const int* __restrict__ lvl_rows,
+                                                        const int* __restrict__ blk_lvl,
+                                                        const int* __restrict__ ulvl_ptr,
+                                                        const int* __restrict__ ulvl_rows,
+                                                        const int* __restrict__ blk_ulvl,
+                                                        const T* __restrict__ lu,
+                                                        const double* __restrict__ r,
+                                                        double* __restrict__ z) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int b = blockIdx.x;
+    const int r0 = bstart[b], r1 = bstart[b + 1], nr = r1 - r0;
+    const int e0 = lu_ptr[r0], nnz = lu_ptr[r1] - e0;
+    T* x = reinterpret_cast<T*>(smem_raw);
+    T* val = x + nr;
+    unsigned short* col = reinterpret_cast<unsigned short*>(val + nnz);
+    unsigned short* rp = col + nnz;
+    unsigned short* dg = rp + nr + 1;
+    for (int q = threadIdx.x; q < nnz; q += blockDim.x) {
+        val[q] = lu[e0 + q];
+        col[q] = lu_col[e0 + q];
+    }
+    for (int i = threadIdx.x; i <= nr; i += blockDim.x) rp[i] = (unsigned short)(lu_ptr[r0 + i] - e0);
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+        dg[i] = (unsigned short)(lu_diag[r0 + i] - e0);
+        x[i] = (T)r[r0 + i];
+    }
+    __syncthreads();
+    for (int l = blk_lvl[b] + 1; l < blk_lvl[b + 1]; ++l) {
+        for (int q = lvl_ptr[l] + threadIdx.x; q < lvl_ptr[l + 1]; q += blockDim.x) {
+            int li = lvl_rows[q] - r0;
+            T acc = x[li];
+            for (int p = rp[li]; p < dg[li]; ++p) acc -= val[p] * x[col[p]];
+            x[li] = acc;
+        }
+        __syncthreads();
+    }
+    for (int l = blk_ulvl[b]; l < blk_ulvl[b + 1]; ++l) {
+        for (int q = ulvl_ptr[l] + threadIdx.x; q < ulvl_ptr[l + 1]; q += blockDim.x) {
+            int li = ulvl_rows[q] - r0;
+            int d = dg[li];
+            T acc = x[li];
+            for (int p = d + 1; p < rp[li + 1]; ++p) acc -= val[p] * x[col[p]];
+            x[li] = acc * val[d];
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) z[r0 + i] = (double)x[i];
 }
 
 // ------------------------------------------------------------------ host set-up
@@ -282,6 +348,25 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
     P->nb = nb;
     P->maxb = maxb;
     P->nlevels_max = nlmax;
+    {
+        size_t need64 = 0, need32 = 0;
+        bool fits16 = true;
+        for (int b = 0; b < nb; ++b) {
+            size_t nr = bstart[b + 1] - bstart[b];
+            size_t nz = lu_ptr[bstart[b + 1]] - lu_ptr[bstart[b]];
+            if (nz >= 65535 || nr + 1 >= 65535) fits16 = false;
+            need64 = std::max(need64, nr * 8 + nz * 8 + nz * 2 + (nr + 1) * 2 + nr * 2);
+            need32 = std::max(need32, nr * 4 + nz * 4 + nz * 2 + (nr + 1) * 2 + nr * 2);
+        }
+        P->smem_stage[0] = (fits16 && need64 <= kMaxDynSmem) ? need64 : 0;
+        P->smem_stage[1] = (fits16 && need32 <= kMaxDynSmem) ? need32 : 0;
+        if (P->smem_stage[0])
+            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)P->smem_stage[0]));
+        if (P->smem_stage[1])
+            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)P->smem_stage[1]));
+    }
     cudaStream_t s = c->stream;
     P->col.upload(P->h_col, s);
     P->rowof.upload(rowof, s);
@@ -316,7 +401,7 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     cudaStream_t s = c->stream;
     const int N = c->N;
     c->tm.begin(TM_FD_JAC, s);
-    k_shift<<<grid_for(N, 256), 256, 0, s>>>(N, y, yp, ewt, h, std::sqrt(DBL_EPSILON), P->shift.p);
+    fvm_launch(c, k_shift, grid_for(N, 256), 256, 0, s, N, y, yp, ewt, h, std::sqrt(DBL_EPSILON), P->shift.p);
     for (int col = 0; col < P->ncol; ++col) {
         Perturb pt;
         pt.mode = 2;
@@ -327,7 +412,7 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
         launch_residual(c, y, yp, pt, nullptr, P->Fc.p);
         int cnt = P->h_cptr[col + 1] - P->h_cptr[col];
         if (cnt > 0)
-            k_fd_scatter<<<grid_for(cnt, 256), 256, 0, s>>>(cnt, P->cnnz.p + P->h_cptr[col], P->rowof.p,
+            fvm_launch(c, k_fd_scatter, grid_for(cnt, 256), 256, 0, s, cnt, P->cnnz.p + P->h_cptr[col], P->rowof.p,
                                                             P->col.p, P->Fc.p, F0, P->shift.p, P->J.p);
     }
     c->tm.end(TM_FD_JAC, s);
@@ -336,12 +421,12 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     c->tm.begin(TM_ILU_FACTOR, s);
     if (precision) {
         P->lu32.alloc(nlu);
-        k_ilu_factor<float><<<P->nb, 128, 0, s>>>(P->bstart.p, P->lu_ptr.p, P->lu_src.p, P->lu_diag.p, P->lu_col.p,
+        fvm_launch(c, k_ilu_factor<float>, P->nb, 128, 0, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p, P->lu_diag.p, P->lu_col.p,
                                                   P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->J.p, P->lu32.p,
                                                   P->status.p);
     } else {
         P->lu64.alloc(nlu);
-        k_ilu_factor<double><<<P->nb, 128, 0, s>>>(P->bstart.p, P->lu_ptr.p, P->lu_src.p, P->lu_diag.p, P->lu_col.p,
+        fvm_launch(c, k_ilu_factor<double>, P->nb, 128, 0, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p, P->lu_diag.p, P->lu_col.p,
                                                    P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->J.p, P->lu64.p,
                                                    P->status.p);
     }
@@ -367,14 +452,24 @@ void psolve_dev(fvm_ctx* c, const double* r, double* z) {
         fvm_ctx* c;
         ~EndTimer() { c->tm.end(TM_ILU_APPLY, c->stream); }
     } end_timer{c};
-    if (P->factored) {
+    if (P->smem_stage[P->factored]) {
+        size_t sm = P->smem_stage[P->factored];
+        if (P->factored)
+            fvm_launch(c, k_ilu_apply_smem<float>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p,
+                                                          P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p,
+                                                          P->ulvl_rows.p, P->blk_ulvl.p, P->lu32.p, r, z);
+        else
+            fvm_launch(c, k_ilu_apply_smem<double>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p,
+                                                           P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p,
+                                                           P->ulvl_rows.p, P->blk_ulvl.p, P->lu64.p, r, z);
+    } else if (P->factored) {
         size_t sm = sizeof(float) * P->maxb;
-        k_ilu_apply<float><<<P->nb, 128, sm, s>>>(P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
+        fvm_launch(c, k_ilu_apply<float>, P->nb, 128, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
                                                  P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p, P->ulvl_rows.p,
                                                  P->blk_ulvl.p, P->lu32.p, r, z);
     } else {
         size_t sm = sizeof(double) * P->maxb;
-        k_ilu_apply<double><<<P->nb, 128, sm, s>>>(P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
+        fvm_launch(c, k_ilu_apply<double>, P->nb, 128, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
                                                   P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p, P->ulvl_rows.p,
                                                   P->blk_ulvl.p, P->lu64.p, r, z);
     }

@@ -31,8 +31,10 @@ static __device__ __forceinline__ double block_sum(double v) {
 }
 
 // every block calls this after writing partial[blockIdx.x * nv + v]; the
-// last block to arrive writes out[v] = sum_b partial[b * nv + v] in block
-// order and re-arms the counter
+// last block to arrive writes out[v] = sum_b partial[b * nv + v] and
+// re-arms the counter.  One warp per value: lane l sums blocks l, l+32, ...
+// in order, then a fixed shuffle tree combines the lanes, so the result
+// does not depend on which block finished last.
 static __device__ __forceinline__ void last_block_reduce(double* partial, int nv,
                                                          unsigned* counter, double* out) {
     __shared__ bool last;
@@ -45,10 +47,13 @@ static __device__ __forceinline__ void last_block_reduce(double* partial, int nv
     __syncthreads();
     if (!last) return;
     __threadfence();
-    for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const volatile double* vp = partial;
+    for (int v = warp; v < nv; v += nw) {
         double s = 0.0;
-        for (int b = 0; b < (int)gridDim.x; ++b) s += ((volatile double*)partial)[(size_t)b * nv + v];
-        out[v] = s;
+        for (int b = lane; b < (int)gridDim.x; b += 32) s += vp[(size_t)b * nv + v];
+        s = warp_sum(s);
+        if (lane == 0) out[v] = s;
     }
     __syncthreads();
     if (threadIdx.x == 0) *counter = 0u;

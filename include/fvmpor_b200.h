@@ -156,13 +156,15 @@ int fvm_precond_info(fvm_ctx* ctx, int* nnz, int* ncolours, int* nblocks,
  * convention +J).  Any pointer may be NULL. */
 int fvm_precond_jacobian(fvm_ctx* ctx, int* rowptr, int* col, double* val);
 
-/* Right-preconditioned restarted GMRES(m) on J x = b in the WRMS norm
- * weighted by ewt, zero initial guess, until ||b - J x||_wrms <= tol.
- * Algorithm of decomp/gmres.c:26-201 with arnoldi :412-511 and the Givens
- * least squares of decomp/linalg_dense.c:128-173.  precision 1 keeps the
- * Krylov basis in FP32; the Hessenberg, Givens and stopping test stay FP64.
- * Returns 0 on convergence, 1 (recoverable) otherwise; *iters gets the
- * number of Arnoldi steps. */
+/* Preconditioned restarted GMRES(m) on J x = b, zero initial guess, left
+ * preconditioned and scaled by D = diag(ewt) as IDAS SPGMR runs it inside
+ * Newton (ida_integrator.h:248-254): stops when ||D P^-1 (b - J x)||_wrms
+ * <= tol.  Arnoldi, Givens least squares and restarts follow
+ * decomp/gmres.c:26-201, :412-511 and decomp/linalg_dense.c:128-173.
+ * J*v is the difference quotient (fvm_jv) with sigma = 1/||v||_wrms.
+ * precision 1 keeps the Krylov basis in FP32; the Hessenberg, Givens and
+ * stopping test stay FP64.  Needs fvm_psetup first.  Returns 0 on
+ * convergence, 1 (recoverable) otherwise; *iters gets the Arnoldi steps. */
 int fvm_gmres(fvm_ctx* ctx, double t, double cj, const double* y,
               const double* yp, const double* F0, const double* ewt,
               const double* b, double* x, int m, int max_restarts,
@@ -183,6 +185,11 @@ double fvm_dot(fvm_ctx* ctx, const double* x, const double* y);
 #define FVM_PROF_NCAT 7
 int fvm_profile(fvm_ctx* ctx, int enable);
 int fvm_profile_read(fvm_ctx* ctx, double* ms, long* counts);
+
+/* Running totals since fvm_create: kernels launched by the library on this
+ * context and residual evaluations (the Physics::calls() counter,
+ * fvmpor.h:206).  Either pointer may be NULL. */
+int fvm_counters(fvm_ctx* ctx, long* launches, long* residuals);
 
 /* ------------------------------------------------------------------ */
 /* Integrator: variable-order BDF + Newton-Krylov driving the above.     */

@@ -29,7 +29,8 @@
 //   Jacobian   preconditioner_dss.cpp:21-142 (pattern, distance-2
 //              colouring), :284-373 (shift and per-colour residuals)
 //   ILU(0)     decomp/ILU.c:12-115, :133-223
-//   GMRES      decomp/gmres.c:26-201, :412-511 (modified Gram-Schmidt)
+//   GMRES      decomp/gmres.c:26-201, :412-511 (modified Gram-Schmidt), left
+//              preconditioned and ewt-scaled as IDAS SPGMR runs it
 // The BDF controller is the shared template of the product
 // (fvmpor_b200/csrc/bdf_controller.hpp), so oracle and GPU integrations
 // differ only in the kernels.
@@ -781,8 +782,9 @@ void Oracle::psolve(const double* r, double* z) const {
     }
 }
 
-// right-preconditioned restarted GMRES with modified Gram-Schmidt, scaled
-// by the error weights, zero initial guess
+// restarted GMRES with modified Gram-Schmidt (decomp/gmres.c:412-511), left
+// preconditioned and scaled by the error weights as IDAS SPGMR runs it
+// inside Newton: minimises ||D P^-1 (b - J x)||, zero initial guess
 int Oracle::gmres(double cj, const double* y, const double* yp, const double* F0,
                   const double* ewt, const double* b, double* x, int m, int max_restarts,
                   double tol, int* iters, double* rn, long* njv, long* nps) {
@@ -807,10 +809,12 @@ int Oracle::gmres(double cj, const double* y, const double* yp, const double* F0
     std::vector<double> xv(N, 0.0);
     for (int cycle = 0; cycle <= max_restarts; ++cycle) {
         if (have_x) jtimes(xv, Jz);
+        for (int i = 0; i < N; ++i) t[i] = have_x ? b[i] - Jz[i] : b[i];
+        psolve(t.data(), z.data());
+        (*nps)++;
         double beta = 0.0;
         for (int i = 0; i < N; ++i) {
-            double r = have_x ? b[i] - Jz[i] : b[i];
-            V[0][i] = ewt[i] * r;
+            V[0][i] = ewt[i] * z[i];
             beta += V[0][i] * V[0][i];
         }
         beta = std::sqrt(beta);
@@ -824,10 +828,10 @@ int Oracle::gmres(double cj, const double* y, const double* yp, const double* F0
         bool conv = false;
         for (; j < m; ++j) {
             for (int i = 0; i < N; ++i) t[i] = V[j][i] / ewt[i];
-            psolve(t.data(), z.data());
+            jtimes(t, Jz);
+            psolve(Jz.data(), z.data());
             (*nps)++;
-            jtimes(z, Jz);
-            for (int i = 0; i < N; ++i) w[i] = ewt[i] * Jz[i];
+            for (int i = 0; i < N; ++i) w[i] = ewt[i] * z[i];
             std::vector<double> hcol(j + 2);
             for (int l = 0; l <= j; ++l) {   // modified Gram-Schmidt (gmres.c:412-511)
                 double s = 0.0;
@@ -866,10 +870,7 @@ int Oracle::gmres(double cj, const double* y, const double* yp, const double* F0
         std::fill(t.begin(), t.end(), 0.0);
         for (int l = 0; l < j; ++l)
             for (int i = 0; i < N; ++i) t[i] += yv[l] * V[l][i];
-        for (int i = 0; i < N; ++i) t[i] /= ewt[i];
-        psolve(t.data(), z.data());
-        (*nps)++;
-        for (int i = 0; i < N; ++i) xv[i] += z[i];
+        for (int i = 0; i < N; ++i) xv[i] += t[i] / ewt[i];
         have_x = true;
         if (conv) {
             std::copy(xv.begin(), xv.end(), x);
@@ -1104,6 +1105,8 @@ int orc_integrate(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, doub
     bo.hmax = opts->hmax;
     fvmb::BdfController<CpuOps> ctl(ops, bo);
     long nre0 = o->n_res;
+    std::fill(o->w_front.begin(), o->w_front.end(), 0.5);   // averaged weights before step 1
+    std::fill(o->w_back.begin(), o->w_back.end(), 0.5);
     // y'0 = F(t0, y0, 0) / ahh on free rows (fvmpor_ODE_impl.cpp:45-57)
     std::vector<double> zero(N, 0.0), F(N);
     o->residual(t0, y0, zero.data(), F.data());
