@@ -141,6 +141,14 @@ def _declare(L):
     L.fvm_profile.argtypes = [_P, _I]
     L.fvm_profile_read.argtypes = [_P, _P, _P]
     L.fvm_counters.argtypes = [_P, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+    L.fvm_mlp_nparams.restype = _I
+    L.fvm_mlp_set_params.argtypes = [_P, _P]
+    L.fvm_mlp_get_params.argtypes = [_P, _P]
+    L.fvm_mlp_forward.argtypes = [_P, _P, _I, _P]
+    L.fvm_mlp_grad.argtypes = [_P, _P, _P, _I, _P, C.POINTER(C.c_float)]
+    L.fvm_mlp_train.argtypes = [_P, _P, _P, _I, _I, _I, C.c_float, _P]
+    L.fvm_integrate_record.argtypes = [_P, C.POINTER(Opts), _D, _D, _P, _P, C.POINTER(Stats), _P, _P, C.c_long,
+                                       _I, C.POINTER(C.c_long)]
 
 
 PROFILE_CATEGORIES = ("node", "element", "gather", "ilu_apply", "gram_schmidt", "ilu_factor", "fd_jacobian")
@@ -364,6 +372,62 @@ class Integrator:
         if r < 0:
             raise _err("fvm_integrate_host", r)
         return r, st.as_dict()
+
+    def integrate_record(self, t0, t_end, y0, y_end, X, Y, stride=64):
+        """integrate while recording (features, target) pairs of every
+        stride-th node per accepted step into the float32 CUDA tensors X
+        [cap, 8] and Y [cap]; returns (rc, stats, count)"""
+        import torch
+
+        assert X.is_cuda and X.dtype == torch.float32 and Y.is_cuda and Y.dtype == torch.float32
+        st = Stats()
+        cnt = C.c_long()
+        r = lib().fvm_integrate_record(self.ph._c, C.byref(self.opts), t0, t_end, _ptr(y0), _ptr(y_end),
+                                       C.byref(st), C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()),
+                                       Y.numel(), stride, C.byref(cnt))
+        if r < 0:
+            raise _err("fvm_integrate_record", r)
+        return r, st.as_dict(), cnt.value
+
+
+class Predictor:
+    """Per-node MLP that proposes the Newton initial iterate (BF16 weights,
+    FP32 accumulation on the tcgen05 tensor cores; fvm_mlp_*)."""
+
+    def __init__(self, physics: Physics):
+        self.ph = physics
+        self.n = lib().fvm_mlp_nparams()
+
+    def set_params(self, P):
+        P = np.ascontiguousarray(P, np.float32)
+        assert P.size == self.n
+        _check(lib().fvm_mlp_set_params(self.ph._c, P.ctypes.data), "fvm_mlp_set_params")
+
+    def get_params(self):
+        P = np.zeros(self.n, np.float32)
+        _check(lib().fvm_mlp_get_params(self.ph._c, P.ctypes.data), "fvm_mlp_get_params")
+        return P
+
+    def forward(self, X, out):
+        r = lib().fvm_mlp_forward(self.ph._c, C.c_void_p(X.data_ptr()), X.shape[0], C.c_void_p(out.data_ptr()))
+        _check(r, "fvm_mlp_forward")
+        return r
+
+    def grad(self, X, Y):
+        """full-batch gradient of mean((mlp(X) - Y)^2) and the loss"""
+        g = np.zeros(self.n - 16, np.float32)   # trainable part (feature scalers excluded)
+        loss = C.c_float()
+        r = lib().fvm_mlp_grad(self.ph._c, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), Y.numel(),
+                               g.ctypes.data, C.byref(loss))
+        _check(r, "fvm_mlp_grad")
+        return g, loss.value, r
+
+    def train(self, X, Y, epochs=5, batch=0, lr=1e-3):
+        hist = np.zeros(epochs, np.float32)
+        r = lib().fvm_mlp_train(self.ph._c, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), Y.numel(), epochs,
+                                batch, lr, hist.ctypes.data)
+        _check(r, "fvm_mlp_train")
+        return r, hist
 
 
 @dataclass

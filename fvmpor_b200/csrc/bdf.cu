@@ -151,8 +151,12 @@ struct DeviceOps {
     DevBuf<double> partial, res;
     DevBuf<unsigned> counter;
     double* host = nullptr;
-    double tcur = 0.0;
-    Predictor* pred = nullptr;
+    double tcur = 0.0, hcur = 0.0;
+    Predictor* pred = nullptr;     // learned Newton iterate (optional)
+    Recorder* rec = nullptr;       // training-set recorder (optional)
+    DevBuf<double> ypred, yppred, hprev;
+    DevBuf<float> feat;
+    bool f_fresh = false;          // F already holds F(t, y, y')
 
     DeviceOps(fvm_ctx* ctx, const fvm_opts& opts) : c(ctx), o(opts), N(ctx->N) {
         for (int j = 0; j < kNPhi; ++j) { phi[j].alloc(N); phi[j].zero(c->stream); }
@@ -189,15 +193,37 @@ struct DeviceOps {
         for (int j = 0; j < kNPhi; ++j) cf.v[j] = f[j];
         fvm_launch(c, k_phi_scale, g(), 256, 0, c->stream, N, j0, j1, ptrs(), cf);
     }
-    void predict(int k, const double* gamma) {
+    void predict(int k, const double* gamma, double h) {
         Coef7 gm;
         for (int j = 0; j < kNPhi; ++j) gm.v[j] = gamma[j];
         fvm_launch(c, k_predict, g(), 256, 0, c->stream, N, k, ptrs(), gm, y.p, yp.p, e.p);
+        f_fresh = false;
+        hcur = h;
+        if (pred || rec) {
+            // keep the BDF predictor and the learned-iterate features
+            FVM_CUDA(cudaMemcpyAsync(ypred.p, y.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+            FVM_CUDA(cudaMemcpyAsync(yppred.p, yp.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+            predictor_features(c, phi[0].p, hprev.p, ypred.p, h, feat.p);
+        }
     }
     double wrms_y() { return std::sqrt(reduce_sumsq(c, y.p, ewt.p) / N); }
     void residual() {
+        if (f_fresh) {   // the learned-iterate check already evaluated it
+            f_fresh = false;
+            return;
+        }
         Perturb none;
         launch_residual(c, y.p, yp.p, none, nullptr, F.p);
+    }
+    void enable_learning(Predictor* p, Recorder* r) {
+        pred = p;
+        rec = r;
+        if (pred || rec) {
+            ypred.alloc(N);
+            yppred.alloc(N);
+            hprev.alloc(N);
+            feat.alloc((size_t)N * 8);
+        }
     }
     int psetup(double cj, double h) {
         psetup_dev(c, cj, h, y.p, yp.p, F.p, ewt.p, o.precision);
@@ -223,11 +249,21 @@ struct DeviceOps {
         for (int q = 0; q < 4; ++q) out[q] = std::sqrt(host[q] / N);
     }
     void phi_update(int k, int set_kp2) {
+        if (pred || rec) {
+            // the accepted corrector y against the predictor (training
+            // target), then h_{n-1} <- h_n before phi_0 advances
+            if (rec) recorder_push(c, rec, feat.p, y.p, ypred.p, phi[0].p, o.rtol, o.atol);
+            FVM_CUDA(cudaMemcpyAsync(hprev.p, phi[0].p, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+        }
         fvm_launch(c, k_phi_update, g(), 256, 0, c->stream, N, k, set_kp2, ptrs(), e.p);
     }
-    bool newton_guess(double tnew, double cj) {
+    bool newton_guess(double tnew, double h, double cj) {
+        (void)tnew;
         if (!pred) return false;
-        return predictor_apply(c, pred, tnew, cj, phi[0].p, phi[1].p, y.p, yp.p, e.p, ewt.p, F.p);
+        bool kept = predictor_apply(c, pred, o.rtol, o.atol, h, cj, phi[0].p, hprev.p, ypred.p, yppred.p, y.p,
+                                    yp.p, e.p, F.p);
+        f_fresh = true;   // F holds the residual of whichever iterate was kept
+        return kept;
     }
 
     // y0 -> phi_0, y'0 from the initial residual, phi_1 = h y'0
@@ -246,21 +282,24 @@ struct DeviceOps {
         double h = bdf_first_step(t0, tout, ypn, o.h0, o.hmax);
         FVM_CUDA(cudaMemcpyAsync(phi[0].p, y.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
         fvm_launch(c, k_scale_vec, g(), 256, 0, s, N, h, yp.p, phi[1].p);
+        if (hprev.p) FVM_CUDA(cudaMemcpyAsync(hprev.p, y.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
         return h;
     }
 };
 
 int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, const double* y0,
-                  double* y_end, fvm_stats* stats) {
+                  double* y_end, fvm_stats* stats, Recorder* rec = nullptr) {
     const fvm_opts& o = *opts;
     if (o.max_order < 1 || o.max_order > 5) throw Error("integrate: max_order must be 1..5");
     if (!(o.rtol > 0) || !(o.atol > 0)) throw Error("integrate: tolerances must be positive");
     if (!(t_end > t0)) throw Error("integrate: t_end must exceed t0");
     DeviceOps ops(c, o);
+    Predictor* pred = nullptr;
     if (o.use_predictor) {
-        ops.pred = predictor_of(c);
-        if (!ops.pred) throw Error("integrate: use_predictor set but no trained predictor loaded");
+        pred = predictor_of(c);
+        if (!pred) throw Error("integrate: use_predictor set but no trained predictor loaded");
     }
+    ops.enable_learning(pred, rec);
     BdfOptions bo;
     bo.rtol = o.rtol;
     bo.atol = o.atol;
@@ -320,6 +359,31 @@ extern "C" int fvm_integrate(fvm_ctx* c, const fvm_opts* opts, double t0, double
         int rc = integrate_dev(c, opts, t0, t_end, y0, y_end, stats);
         FVM_CUDA(cudaGetLastError());
         if (rc < 0) set_error("fvm_integrate: step failure code " + std::to_string(rc));
+        return rc;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+extern "C" int fvm_integrate_record(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end,
+                                    const double* y0, double* y_end, fvm_stats* stats, float* X, float* Y,
+                                    long capacity, int stride, long* count) {
+    try {
+        if (!c || !opts || !y0 || !y_end || !X || !Y || !count || capacity <= 0 || stride <= 0)
+            throw Error("fvm_integrate_record: bad argument");
+        Recorder r;
+        r.X = X;
+        r.Y = Y;
+        r.cap = capacity;
+        r.stride = stride;
+        int rc = integrate_dev(c, opts, t0, t_end, y0, y_end, stats, &r);
+        *count = r.count;
+        FVM_CUDA(cudaGetLastError());
+        if (rc < 0) set_error("fvm_integrate_record: step failure code " + std::to_string(rc));
         return rc;
     } catch (const Error& ex) {
         set_error(ex.what());

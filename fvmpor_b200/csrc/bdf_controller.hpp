@@ -24,7 +24,7 @@
 //   void   ewt_from_phi0(double rtol, double atol);
 //   void   begin_step();                     // freeze upwinding at (phi_0, y')
 //   void   phi_scale(int j0, int j1, const double* f);   // phi_j *= f[j]
-//   void   predict(int k, const double* gamma);          // y, y' ; e = 0
+//   void   predict(int k, const double* gamma, double h); // y, y' ; e = 0
 //   double wrms_y();
 //   void   residual();                       // F = F(t, y, y')
 //   int    psetup(double cj, double h);      // 0 ok, else zero pivot
@@ -35,7 +35,8 @@
 //                                            // returns ||x||_wrms
 //   void   err_norms(int k, double out[4]);  // see below
 //   void   phi_update(int k, int set_kp2);
-//   void   newton_guess(double cj);          // optional learned iterate
+//   bool   newton_guess(double t, double h, double cj); // learned iterate
+//                                            // kept (true) or BDF predictor
 #pragma once
 
 #include <algorithm>
@@ -121,9 +122,9 @@ template <class Ops> struct BdfController {
             double ck = std::max(std::fabs(alpha[k] + alphas - alpha0), alpha[k]);
             if (k >= ns) ops.phi_scale(ns, k, beta);
             double tnew = t + h;
-            ops.predict(k, gamma);
+            ops.predict(k, gamma, h);
             double pnorm = ops.wrms_y();
-            if (o.use_guess && ops.newton_guess(tnew, cj)) st.npred++;
+            if (o.use_guess && ops.newton_guess(tnew, h, cj)) st.npred++;
             bool converged = false, fresh_p = false;
             // refresh the preconditioner on the first step, when cj has moved
             // by more than a factor of two since the last factorisation, every
@@ -133,7 +134,7 @@ template <class Ops> struct BdfController {
             for (int attempt = 0; attempt < 2 && !converged; ++attempt) {
                 if (attempt == 1) {
                     if (fresh_p) break;
-                    ops.predict(k, gamma);   // retry from the predictor with a fresh factor
+                    ops.predict(k, gamma, h);   // retry from the predictor with a fresh factor
                     need_p = true;
                 }
                 ops.set_time(tnew);

@@ -534,6 +534,33 @@ static void build(fvm_ctx* c, const fvm_mesh* m, const fvm_physics* ph, int flag
         }
     }
     c->h_node_type.assign(ntype.begin(), ntype.end());
+    {
+        // static learned-predictor inputs: mean ln K of the incident
+        // elements, elevation, and the area of the node's CV faces
+        std::vector<float> sf((size_t)3 * N, 0.0f);
+        std::vector<double> lnk(N, 0.0), asum(N, 0.0);
+        std::vector<int> cnt(N, 0);
+        for (int e = 0; e < T; ++e) {
+            double lk = std::log(std::max(eK3[e], 1e-300));
+            for (int k = 0; k < npe; ++k) {
+                int i = m->elem_nodes[(size_t)e * npe + k];
+                lnk[i] += lk;
+                cnt[i]++;
+            }
+            for (int f = 0; f < nfe; ++f) {
+                int a = m->elem_nodes[(size_t)e * npe + (dim == 3 ? tet_edge_a(f) : tri_edge_a(f))];
+                int b = m->elem_nodes[(size_t)e * npe + (dim == 3 ? tet_edge_b(f) : tri_edge_b(f))];
+                asum[a] += area[(size_t)nfe * e + f];
+                asum[b] += area[(size_t)nfe * e + f];
+            }
+        }
+        for (int i = 0; i < N; ++i) {
+            sf[i] = (float)(lnk[i] / std::max(cnt[i], 1));
+            sf[(size_t)N + i] = (float)c->h_vert[i];
+            sf[(size_t)2 * N + i] = (float)asum[i];
+        }
+        c->statf.upload(sf, s);
+    }
     c->h_hD = hD;
 
     // ---- upload
@@ -595,6 +622,7 @@ using namespace fvmb;
 
 void fvmb_destroy_ilu(fvmb::BlockILU* p);
 void fvmb_destroy_krylov(fvmb::Krylov* p);
+void fvmb_destroy_predictor(fvmb::Predictor* p);
 
 extern "C" const char* fvm_last_error(void) { return g_last_error.c_str(); }
 
@@ -616,6 +644,7 @@ extern "C" void fvm_destroy(fvm_ctx* c) {
     cudaStreamSynchronize(c->stream);
     fvmb_destroy_ilu(c->ilu);
     fvmb_destroy_krylov(c->kry);
+    fvmb_destroy_predictor(c->pred);
     cudaStream_t s = c->stream;
     delete c;
     if (s) cudaStreamDestroy(s);

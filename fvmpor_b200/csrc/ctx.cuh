@@ -110,6 +110,7 @@ struct Perturb {
 
 struct BlockILU;   // precond.cu
 struct Krylov;     // linalg.cu
+struct Predictor;  // predictor.cu
 
 } // namespace fvmb
 
@@ -161,9 +162,12 @@ struct fvm_ctx {
     fvmb::DevBuf<int4> epos;         // [T] slot of each element node (4th = 0 in 2D)
     fvmb::DevBuf<double> faceq;      // [T*nfe] averaged-weight face fluxes
     fvmb::DevBuf<double> tmpN[4];    // scratch vectors
+    fvmb::DevBuf<float> statf;       // [3][N] static node features: mean ln K, elevation,
+                                     // CV surface area (learned predictor inputs)
 
     fvmb::BlockILU* ilu = nullptr;
     fvmb::Krylov* kry = nullptr;
+    fvmb::Predictor* pred = nullptr;
 
     long n_residuals = 0;
     long launches = 0;               // kernels launched on this context

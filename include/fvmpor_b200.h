@@ -238,6 +238,39 @@ int fvm_integrate(fvm_ctx* ctx, const fvm_opts* opts, double t0,
                   fvm_stats* stats);
 
 /* ------------------------------------------------------------------ */
+/* Learned Newton initial iterate (no counterpart in the reference:     */
+/* IDAS always starts Newton from its BDF predictor).  A per-node MLP    */
+/* 8 -> 64 -> 64 -> 64 -> 1 (GELU), BF16 weights, FP32 accumulation on   */
+/* tcgen05 tensor cores, proposes y_pred + (rtol|h|+atol) * MLP(x) with  */
+/* x = (h_n, h_n - h_{n-1}, y_pred - h_n, log10 dt, ln K, z, CV area, 0);*/
+/* the integrator keeps it only when its residual norm is below the BDF  */
+/* predictor's (opts.use_predictor = 1).                                 */
+/* ------------------------------------------------------------------ */
+int fvm_mlp_nparams(void);   /* packed FP32 parameters: W1 b1 W2 b2 W3 b3
+                                w4 b4, then 8 feature means, 8 scales */
+int fvm_mlp_set_params(fvm_ctx* ctx, const float* params_host);
+int fvm_mlp_get_params(fvm_ctx* ctx, float* params_host);
+/* out[i] = MLP(X[i]) for n rows of raw features X[n][8] (device).      */
+int fvm_mlp_forward(fvm_ctx* ctx, const float* X, int n, float* out);
+/* Full-batch gradient of mean((MLP(X) - Y)^2) over the trainable
+ * parameters (host buffer of fvm_mlp_nparams() - 16) and the loss.      */
+int fvm_mlp_grad(fvm_ctx* ctx, const float* X, const float* Y, int n,
+                 float* grad_host, float* loss);
+/* Adam on (X, Y) in consecutive mini-batches of `batch` rows (0 = 148 x
+ * 256); loss_history_host gets the mean loss of each epoch.             */
+int fvm_mlp_train(fvm_ctx* ctx, const float* X, const float* Y, int n,
+                  int epochs, int batch, float lr, float* loss_history_host);
+/* fvm_integrate that also records training pairs: the features of every
+ * stride-th node (offset rotating per step) at the BDF predictor and the
+ * target (y_{n+1} - y_pred) / (rtol |h_n| + atol) of each accepted step,
+ * into device buffers X[capacity][8], Y[capacity]; *count gets the rows
+ * written. */
+int fvm_integrate_record(fvm_ctx* ctx, const fvm_opts* opts, double t0,
+                         double t_end, const double* y0, double* y_end,
+                         fvm_stats* stats, float* X, float* Y, long capacity,
+                         int stride, long* count);
+
+/* ------------------------------------------------------------------ */
 /* Synthetic problem generators (host).  The reference reads gmsh-made   */
 /* .pmesh files (meshing/genMesh.sh, decomp/split.c:459-500); these      */
 /* build the benchmark meshes directly.  Arrays are malloc'd by the      */

@@ -911,7 +911,7 @@ struct CpuOps {
         for (int j = j0; j <= j1; ++j)
             for (int i = 0; i < N; ++i) phi[j][i] *= f[j];
     }
-    void predict(int k, const double* gamma) {
+    void predict(int k, const double* gamma, double) {
         for (int i = 0; i < N; ++i) {
             double s = phi[0][i], sp = 0.0;
             for (int j = 1; j <= k; ++j) { s += phi[j][i]; sp += gamma[j] * phi[j][i]; }
@@ -949,7 +949,7 @@ struct CpuOps {
             for (int j = k - 1; j >= 0; --j) phi[j][i] += phi[j + 1][i];
         }
     }
-    bool newton_guess(double, double) { return false; }
+    bool newton_guess(double, double, double) { return false; }
 };
 
 } // namespace orc
