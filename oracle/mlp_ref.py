@@ -49,7 +49,9 @@ def gelu_grad(x):
 
 
 def unpack(P):
-    P = np.asarray(P, np.float32)
+    P = np.asarray(P)
+    if P.dtype != np.float64:
+        P = P.astype(np.float32)
     return dict(
         W1=P[OFF_W1:OFF_B1].reshape(H, IN), b1=P[OFF_B1:OFF_W2], W2=P[OFF_W2:OFF_B2].reshape(H, H),
         b2=P[OFF_B2:OFF_W3], W3=P[OFF_W3:OFF_B3].reshape(H, H), b3=P[OFF_B3:OFF_W4], w4=P[OFF_W4:OFF_B4],
@@ -80,12 +82,13 @@ def forward(P, X, keep=False, exact=False):
     p = {k: np.asarray(v, dt) for k, v in unpack(P).items()}
     x = r((np.asarray(X, dt) - p["mu"]) / p["sd"])
     W1, W2, W3 = r(p["W1"]), r(p["W2"]), r(p["W3"])
+    act = _gelu64 if exact else gelu
     z1 = x @ W1.T + p["b1"]
-    a1 = r(gelu(z1).astype(dt) if exact else gelu(z1))
+    a1 = r(act(z1))
     z2 = a1 @ W2.T + p["b2"]
-    a2 = r(gelu(z2).astype(dt) if exact else gelu(z2))
+    a2 = r(act(z2))
     z3 = a2 @ W3.T + p["b3"]
-    h3 = (0.5 * z3 * (1.0 + _erf(z3 / math.sqrt(2.0)))) if exact else gelu(z3)
+    h3 = act(z3)
     out = h3 @ p["w4"] + p["b4"]
     if keep:
         return out, dict(x=x, z1=z1, a1=a1, z2=z2, a2=a2, z3=z3, h3=h3, W2=W2, W3=W3, p=p)
@@ -119,6 +122,11 @@ def grad(P, X, Y, exact=False):
     g[OFF_B1:OFF_W2] = dz1.sum(0)
     g[OFF_W1:OFF_B1] = (dz1b.T @ c["x"]).ravel()
     return g, float(np.mean(np.asarray(e, np.float64) ** 2))
+
+
+def _gelu64(x):
+    x = np.asarray(x, np.float64)
+    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
 
 
 def _gelu_grad64(x):

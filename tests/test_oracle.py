@@ -267,3 +267,37 @@ def test_oracle_integration_short_horizon():
     assert np.all(yend[top] == 0.0)
     below = (np.abs(a["coords"][:, 1] - 4.75) < 0.01) & (np.abs(a["coords"][:, 0] - 5.0) < 0.6)
     assert np.all(yend[below] > y0[below])
+
+
+# ---------------------------------------------------------------- MLP oracle
+def test_mlp_oracle_gradient_matches_finite_differences():
+    from oracle import mlp_ref
+
+    rng = np.random.default_rng(0)
+    P = mlp_ref.init_params(2, rng.normal(0, 1, 8).astype(np.float32), (rng.random(8) + 0.5).astype(np.float32))
+    X = rng.normal(0, 1, (40, 8))
+    Y = rng.normal(0, 1, 40)
+    g, _ = mlp_ref.grad(P, X, Y, exact=True)
+    P64 = P.astype(np.float64)
+    for j in list(rng.choice(mlp_ref.N_TRAIN, 25, replace=False)) + [mlp_ref.OFF_B4]:
+        h = 1e-6
+        Pp, Pm = P64.copy(), P64.copy()
+        Pp[j] += h
+        Pm[j] -= h
+        lp = np.mean((mlp_ref.forward(Pp, X, exact=True) - Y) ** 2)
+        lm = np.mean((mlp_ref.forward(Pm, X, exact=True) - Y) ** 2)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[j]) <= 1e-6 * max(1.0, abs(fd)), (j, fd, g[j])
+
+
+def test_mlp_oracle_bf16_rounding():
+    from oracle import mlp_ref
+
+    # bf16 keeps 7 fraction bits: the spacing above 1.0 is 2^-7
+    x = np.array([1.0, 1.00390625, 1.0048828125, 1.01171875, -3.14159], np.float32)
+    r = mlp_ref.bf16(x)
+    assert r[0] == 1.0
+    assert r[1] == 1.0            # exactly halfway: ties to the even neighbour
+    assert r[2] == 1.0078125      # above halfway rounds up
+    assert r[3] == 1.015625       # halfway between 1.0078125 (odd) and 1.015625 (even)
+    assert abs(r[4] + 3.140625) < 1e-6
