@@ -186,6 +186,25 @@ double fvm_dot(fvm_ctx* ctx, const double* x, const double* y);
 int fvm_profile(fvm_ctx* ctx, int enable);
 int fvm_profile_read(fvm_ctx* ctx, double* ms, long* counts);
 
+/* WRMS norm sqrt(mean((x*ewt)^2)) of n values, like fvm_wrms, but without
+ * any device allocation and without a context: for callers that cannot
+ * call cudaMalloc (a host integrator that owns all device memory through its
+ * own pool and calls the norm inside its step loop, where an allocation
+ * would stall the device or is forbidden).  No counterpart in the
+ * reference.  The reduction scratch is a static 32 KiB __device__ array
+ * that every GPU loading the library keeps until exit, which bounds n to
+ * fvm_wrms_noalloc_max_n() = 8,388,608; larger n is rejected (status < 0,
+ * message in fvm_last_error()).  The first call on a device looks the
+ * array's address up with cudaGetSymbolAddress, so make that first call
+ * before any stream capture.  x, ewt (may be NULL = 1) and result are
+ * device pointers; the work is queued on `stream` (a cudaStream_t, NULL for
+ * the legacy default stream) and *result is valid once that stream reaches
+ * it.  All calls share the one scratch array: calls that overlap on the GPU
+ * (on different streams) race and must be serialised by the caller. */
+long fvm_wrms_noalloc_max_n(void);
+int fvm_wrms_noalloc(const double* x, const double* ewt, long n,
+                     double* result, void* stream);
+
 /* Running totals since fvm_create: kernels launched by the library on this
  * context and residual evaluations (the Physics::calls() counter,
  * fvmpor.h:206).  Either pointer may be NULL. */
