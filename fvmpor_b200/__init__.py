@@ -111,6 +111,11 @@ _D = C.c_double
 _I = C.c_int
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("n", C.c_int), ("best", C.c_int), ("variant", C.c_int * 16), ("chunk", C.c_int * 16),
+                ("us", C.c_double * 16)]
+
+
 def _declare(L):
     L.fvm_create.restype = _P
     L.fvm_create.argtypes = [C.POINTER(Mesh), C.POINTER(PhysicsDesc), _I]
@@ -141,6 +146,10 @@ def _declare(L):
     L.fvm_profile.argtypes = [_P, _I]
     L.fvm_profile_read.argtypes = [_P, _P, _P]
     L.fvm_counters.argtypes = [_P, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+    L.fvm_autotune.argtypes = [_P, C.POINTER(TuneResult)]
+    L.fvm_set_element_pass.argtypes = [_P, _I, _I]
+    L.fvm_element_pass.argtypes = [_P, C.POINTER(_I), C.POINTER(_I)]
+    L.fvm_set_precond_blocks.argtypes = [_P, _I]
     L.fvm_mlp_nparams.restype = _I
     L.fvm_mlp_set_params.argtypes = [_P, _P]
     L.fvm_mlp_get_params.argtypes = [_P, _P]
@@ -244,7 +253,9 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
-FLAG_RECOMPUTE_GEOMETRY = 1
+FLAG_RECOMPUTE_GEOMETRY = 1   # element pass rebuilds the face geometry (3D default)
+FLAG_AUTOTUNE = 2             # pick the element-pass variant and chunk size at creation
+FLAG_STORED_GEOMETRY = 4      # element pass streams stored face coefficients
 
 
 class Physics:
@@ -293,6 +304,21 @@ class Physics:
     def profile(self, enable: bool):
         _check(lib().fvm_profile(self._c, 1 if enable else 0), "fvm_profile")
 
+    def autotune(self):
+        """time every element-pass candidate on this mesh, keep the fastest;
+        returns [(variant, chunk, us)] and the index kept"""
+        r = TuneResult()
+        _check(lib().fvm_autotune(self._c, C.byref(r)), "fvm_autotune")
+        return [(r.variant[i], r.chunk[i], r.us[i]) for i in range(r.n)], r.best
+
+    def set_element_pass(self, variant, chunk):
+        _check(lib().fvm_set_element_pass(self._c, variant, chunk), "fvm_set_element_pass")
+
+    def element_pass(self):
+        v, ch = _I(), _I()
+        _check(lib().fvm_element_pass(self._c, C.byref(v), C.byref(ch)), "fvm_element_pass")
+        return v.value, ch.value
+
     def counters(self):
         a, b = C.c_long(), C.c_long()
         _check(lib().fvm_counters(self._c, C.byref(a), C.byref(b)), "fvm_counters")
@@ -317,6 +343,10 @@ class Preconditioner:
 
     def apply(self, r, z):
         _check(lib().fvm_psolve(self.ph._c, _ptr(r), _ptr(z)), "fvm_psolve")
+
+    def set_blocks_per_sm(self, per_sm):
+        """block-ILU blocks per SM on large meshes (drops the current factor)"""
+        _check(lib().fvm_set_precond_blocks(self.ph._c, per_sm), "fvm_set_precond_blocks")
 
     def info(self):
         a, b, c, d = _I(), _I(), _I(), _I()
@@ -394,9 +424,29 @@ class Predictor:
     """Per-node MLP that proposes the Newton initial iterate (BF16 weights,
     FP32 accumulation on the tcgen05 tensor cores; fvm_mlp_*)."""
 
+    # parameter vector layout (fvm_mlp_set_params): W1[64x8] b1[64]
+    # W2[64x64] b2[64] W3[64x64] b3[64] w4[64] b4 | feature mean[8], std[8]
+    IN, H = 8, 64
+
     def __init__(self, physics: Physics):
         self.ph = physics
         self.n = lib().fvm_mlp_nparams()
+
+    def init(self, X, seed=0):
+        """the untrained network: normal(0, 1/fan_in) weights, zero biases,
+        and feature scalers from the mean / std of the columns of X (a CUDA
+        float32 tensor [n, 8] of recorded features)"""
+        IN, H = self.IN, self.H
+        mu = X.mean(0).double().cpu().numpy()
+        sd = X.std(0).double().cpu().numpy() + 1e-6
+        rng = np.random.default_rng(seed)
+        parts = [rng.normal(0, 1 / np.sqrt(IN), H * IN), np.zeros(H),
+                 rng.normal(0, 1 / np.sqrt(H), H * H), np.zeros(H),
+                 rng.normal(0, 1 / np.sqrt(H), H * H), np.zeros(H),
+                 rng.normal(0, 1 / np.sqrt(H), H), np.zeros(1), mu, sd]
+        P = np.concatenate(parts).astype(np.float32)
+        assert P.size == self.n
+        self.set_params(P)
 
     def set_params(self, P):
         P = np.ascontiguousarray(P, np.float32)

@@ -17,6 +17,7 @@
 // bitwise reproducible run to run and independent of the launch shape; no
 // floating-point atomics are used anywhere.
 #include "ctx.cuh"
+#include "tc05.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -30,13 +31,25 @@ static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 
 constexpr int kBlock = 256;
+constexpr int kDefaultChunk = 512;   // elements per chunk of the element pass
 
 // ------------------------------------------------------------------ kernels
+// Besides the node arrays, the node pass writes the head and (single zone)
+// krw of every node into each element chunk that holds the node, at the
+// chunk-major copy positions cpos[part_ptr[i] .. part_ptr[i+1]), so the
+// element pass streams its chunk's node data contiguously.
+struct NodeCopies {
+    const int* part_ptr = nullptr;   // [N+1]
+    const int* cpos = nullptr;       // [P] chunk-major position of each copy
+    double* ch_h = nullptr;          // [P]
+    double* ch_krw = nullptr;        // [P] (single zone)
+};
+
 __global__ void k_node(int N, const double* __restrict__ y, const double* __restrict__ yp,
                        Perturb pt, const ZoneDev* __restrict__ zones, int nz,
                        const int* __restrict__ nz_ptr, const int* __restrict__ nz_zone,
                        const double* __restrict__ nz_w, double rho0, double* __restrict__ krw,
-                       double* __restrict__ hstar, double* __restrict__ stor) {
+                       double* __restrict__ hstar, double* __restrict__ stor, NodeCopies cp) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     double h = y[i], hp = yp[i];
@@ -55,13 +68,20 @@ __global__ void k_node(int N, const double* __restrict__ y, const double* __rest
         hstar[i] = h;
     }
     double phi = 0.0, dsw = 0.0;
+    const int c0 = cp.part_ptr[i], c1 = cp.part_ptr[i + 1];
     if (nz == 1) {
         double Sw, d, k;
         van_genuchten(h, zones[0], Sw, d, k);
         krw[i] = k;
         phi = zones[0].phi * nz_w[i];
         dsw = d * nz_w[i];
+        for (int q = c0; q < c1; ++q) {
+            const int cm = cp.cpos[q];
+            cp.ch_h[cm] = h;
+            cp.ch_krw[cm] = k;
+        }
     } else {
+        for (int q = c0; q < c1; ++q) cp.ch_h[cp.cpos[q]] = h;
         for (int p = nz_ptr[i]; p < nz_ptr[i + 1]; ++p) {
             int z = nz_zone[p];
             double w = nz_w[p];
@@ -77,143 +97,228 @@ __global__ void k_node(int N, const double* __restrict__ y, const double* __rest
     stor[i] = hp * ahh;
 }
 
-// krw at a face: upwind node (0/1) or the averaged weights 0.5/0.5 the
-// reference uses before the first step (fvmpor.h:594-595, 919-924)
-__device__ __forceinline__ double face_krw(unsigned u, double ka, double kb) {
-    return u == 0 ? ka : (u == 1 ? kb : ka * 0.5 + kb * 0.5);
+
+// Element pass: persistent CTAs walk the element chunks (CE consecutive
+// elements each, chunk c = blockIdx.x, blockIdx.x + gridDim.x, ...) through
+// a two-stage TMA pipeline.  While the CTA computes chunk i from one shared
+// stage, one thread has already issued the 1D bulk copies (cp.async.bulk,
+// completion counted on that stage's mbarrier) that bring chunk i+1 into the
+// other stage: the chunk's distinct nodes -- head, krw and, for the
+// rebuilt-geometry variant, coordinates, from the chunk-major copies the
+// node pass wrote -- and its element records (local corner ids, upwind
+// flags, conductivity) and node-ordered corner lists.  Every array is padded
+// per chunk to 16-byte multiples, so each copy is one aligned transfer.
+// Each element then reads its corners from shared memory through 16-bit
+// local ids and leaves its dim+1 corner partials
+//   sum over its faces of -/+ rho0 krw_up (sum_k C_fk h_k + G_f)
+// (shape-gradient SpMVs + process_fluxes, fvmpor.h:682-759,
+// fvmpor_ODE_impl.cpp:75-80) in shared memory (corner-major, so the writes
+// of a warp hit distinct banks).  Every chunk node sums its corners in
+// ascending element order and writes ONE partial, chunk-major; the gather
+// adds a node's partials in ascending chunk order, so the residual is
+// bitwise reproducible and independent of the launch shape, without
+// floating-point atomics.
+//   VAR 0: stored coefficients C_fk, G_f (any simplex), streamed from global
+//   VAR 1: tetrahedra, fluxes rebuilt from the vertices (tet_face_fluxes)
+struct ElemArgs {
+    int T, N, CE, nch, kiso, estride;
+    int nnmax;                    // largest padded node segment of a chunk
+    const int2* ch_seg;           // [nchunk] (padded start, node count) of each chunk
+    const int* ch_node;           // [P] global node ids, ascending per chunk (several zones)
+    const ushort4* elocal;        // [estride] chunk-local corner ids
+    const unsigned short* ch_lptr;// [P] corner-list offsets, at the chunk's node segment
+    const unsigned short* ch_lc;  // [estride*npe] corner lists (k*CE + el), per chunk
+    const double* coef;           // VAR 0
+    const double* ch_xyz;         // VAR 1: [3][P] chunk-major coordinates
+    const double* eK;             // VAR 1: [estride] (kiso) or [3][estride]
+    const int* ezone;
+    const double* krw;            // [nz][N] (several zones)
+    const double* ch_h;           // [P] chunk-major head (written by the node pass)
+    const double* ch_krw;         // [P] chunk-major krw (single zone)
+    const unsigned char* upw;     // [8*estride]
+    double rho0;
+    double* part;                 // [P] chunk-major partials
+    int* err;                     // 5 = a pipeline wait gave up
+    size_t P;
+};
+
+constexpr int kElemThreads = 256;
+
+__host__ __device__ __forceinline__ int pad8(int n) { return (n + 7) & ~7; }
+
+// byte offsets inside one pipeline stage (host and device agree)
+struct StageLayout {
+    size_t h, krw, xyz, eloc, upw, ek, lc, lp, bytes;
+    __host__ __device__ StageLayout(int CE, int npe, int nnmax, bool mz, bool rc, bool kiso) {
+        const size_t nd = (size_t)nnmax * 8;
+        h = 0;
+        krw = h + nd;
+        xyz = krw + (mz ? 0 : nd);
+        eloc = xyz + (rc ? 3 * nd : 0);
+        upw = eloc + (size_t)CE * 8;
+        ek = upw + (size_t)CE * 8;
+        lc = ek + (rc ? (size_t)CE * 8 * (kiso ? 1 : 3) : 0);
+        lp = lc + (size_t)CE * npe * 2;
+        bytes = (lp + (size_t)nnmax * 2 + 127) & ~(size_t)127;
+    }
+};
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     tc05::smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(tc05::smem_u32(bar))
+                 : "memory");
 }
 
-// stored-coefficient element pass, tetrahedra
-template <bool MULTIZONE>
-__global__ void __launch_bounds__(256) k_elem_tet(int T, int N, const int4* __restrict__ en,
-                                                   const double* __restrict__ coef,
-                                                   const int* __restrict__ ezone,
-                                                   const double* __restrict__ krw,
-                                                   const double* __restrict__ h,
-                                                   const unsigned char* __restrict__ upw,
-                                                   double rho0, const int4* __restrict__ epos,
-                                                   double* __restrict__ slots) {
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= T) return;
-    int4 nd = en[e];
-    double hv[4] = {h[nd.x], h[nd.y], h[nd.z], h[nd.w]};
-    size_t zo = MULTIZONE ? (size_t)ezone[e] * N : 0;
-    double kr[4] = {krw[zo + nd.x], krw[zo + nd.y], krw[zo + nd.z], krw[zo + nd.w]};
-    uint2 uw = *reinterpret_cast<const uint2*>(upw + (size_t)8 * e);
-    double c[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-        const double* cf = coef + (size_t)(f * 5) * T + e;
-        double q = cf[0] * hv[0];
-        q += cf[(size_t)T] * hv[1];
-        q += cf[(size_t)2 * T] * hv[2];
-        q += cf[(size_t)3 * T] * hv[3];
-        q += cf[(size_t)4 * T];
-        int a = tet_edge_a(f), b = tet_edge_b(f);
-        unsigned u = ((f < 4 ? uw.x >> (8 * f) : uw.y >> (8 * (f - 4)))) & 0xffu;
-        double flux = rho0 * (q * face_krw(u, kr[a], kr[b]));
-        c[a] -= flux;
-        c[b] += flux;
+template <int NPE, bool VAR1, bool MZ>
+__device__ __forceinline__ void elem_issue(const ElemArgs& a, const StageLayout& L, unsigned char* st,
+                                           int4* meta, uint64_t* bar, int c) {
+    const int2 sg = a.ch_seg[c];
+    const int e0 = c * a.CE;
+    const int ne = min(a.CE, a.T - e0);
+    const int nnp = pad8(sg.y + 1), nep = pad8(ne);
+    *meta = make_int4(sg.x, sg.y, e0, ne);
+    uint32_t bytes = (uint32_t)nnp * 8 * (1 + (MZ ? 0 : 1) + (VAR1 ? 3 : 0)) + (uint32_t)nep * 16 +
+                     (VAR1 ? (uint32_t)nep * 8 * (a.kiso ? 1 : 3) : 0) + (uint32_t)nep * NPE * 2 + (uint32_t)nnp * 2;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc05::smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    bulk_g2s(st + L.h, a.ch_h + sg.x, nnp * 8, bar);
+    if (!MZ) bulk_g2s(st + L.krw, a.ch_krw + sg.x, nnp * 8, bar);
+    if (VAR1)
+        for (int d = 0; d < 3; ++d) bulk_g2s(st + L.xyz + (size_t)d * a.nnmax * 8, a.ch_xyz + d * a.P + sg.x, nnp * 8, bar);
+    bulk_g2s(st + L.eloc, a.elocal + e0, nep * 8, bar);
+    bulk_g2s(st + L.upw, a.upw + (size_t)8 * e0, nep * 8, bar);
+    if (VAR1) {
+        const int nk = a.kiso ? 1 : 3;
+        for (int d = 0; d < nk; ++d)
+            bulk_g2s(st + L.ek + (size_t)d * a.CE * 8, a.eK + (size_t)d * a.estride + e0, nep * 8, bar);
     }
-    int4 ps = epos[e];
-    slots[ps.x] = c[0];
-    slots[ps.y] = c[1];
-    slots[ps.z] = c[2];
-    slots[ps.w] = c[3];
+    bulk_g2s(st + L.lc, a.ch_lc + (size_t)e0 * NPE, nep * NPE * 2, bar);
+    bulk_g2s(st + L.lp, a.ch_lptr + sg.x, nnp * 2, bar);
 }
 
-// recompute-geometry element pass, tetrahedra: the face coefficients are
-// rebuilt from the (L2-resident) node coordinates instead of streamed
-template <bool MULTIZONE>
-__global__ void __launch_bounds__(256) k_elem_tet_rc(int T, int N, const int4* __restrict__ en,
-                                                      const double* __restrict__ xyz,
-                                                      const double* __restrict__ eK,
-                                                      const int* __restrict__ ezone,
-                                                      const double* __restrict__ krw,
-                                                      const double* __restrict__ h,
-                                                      const unsigned char* __restrict__ upw,
-                                                      double rho0, const int4* __restrict__ epos,
-                                                      double* __restrict__ slots) {
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= T) return;
-    int4 nd = en[e];
-    int ids[4] = {nd.x, nd.y, nd.z, nd.w};
-    double X[4][3];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        X[k][0] = xyz[ids[k]];
-        X[k][1] = xyz[(size_t)N + ids[k]];
-        X[k][2] = xyz[(size_t)2 * N + ids[k]];
+template <int NPE, int NFE, int VAR, bool MZ, int EPT>
+__global__ void __launch_bounds__(kElemThreads) k_elem_chunk(ElemArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_e[];
+    const StageLayout L(a.CE, NPE, a.nnmax, MZ, VAR == 1, a.kiso != 0);
+    double* cc = reinterpret_cast<double*>(smem_e + 2 * L.bytes);               // [NPE][CE]
+    int4* meta = reinterpret_cast<int4*>(cc + (size_t)NPE * a.CE);                // [2]
+    uint64_t* full = reinterpret_cast<uint64_t*>(meta + 2);                      // [2]
+    if ((int)blockIdx.x >= a.nch) return;
+    if (threadIdx.x == 0) {
+        tc05::mbar_init(&full[0], 1);
+        tc05::mbar_init(&full[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        elem_issue<NPE, VAR == 1, MZ>(a, L, smem_e, &meta[0], &full[0], blockIdx.x);
     }
-    double C[6][4], G[6], A[6], vol;
-    tet_coefficients(X[0], X[1], X[2], X[3], eK[e], eK[(size_t)T + e], eK[(size_t)2 * T + e], C, G, A, &vol);
-    double hv[4] = {h[nd.x], h[nd.y], h[nd.z], h[nd.w]};
-    size_t zo = MULTIZONE ? (size_t)ezone[e] * N : 0;
-    double kr[4] = {krw[zo + nd.x], krw[zo + nd.y], krw[zo + nd.z], krw[zo + nd.w]};
-    uint2 uw = *reinterpret_cast<const uint2*>(upw + (size_t)8 * e);
-    double c[4] = {0.0, 0.0, 0.0, 0.0};
+    __syncthreads();
+    int i = 0;
+    for (int c = blockIdx.x; c < a.nch; c += gridDim.x, ++i) {
+        const int s = i & 1;
+        const int cn = c + gridDim.x;
+        if (threadIdx.x == 0 && cn < a.nch) {
+            // the other stage was released by the barrier that ended the
+            // previous chunk; order those generic reads before the copies
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            elem_issue<NPE, VAR == 1, MZ>(a, L, smem_e + (s ^ 1) * L.bytes, &meta[s ^ 1], &full[s ^ 1], cn);
+        }
+        const bool ok = tc05::mbar_wait(&full[s], (uint32_t)((i >> 1) & 1));
+        if (!__syncthreads_and(ok ? 1 : 0)) {
+            // a chunk never arrived: report it, let the copies already issued
+            // land (bounded) and leave
+            if (threadIdx.x == 0) {
+                atomicExch(a.err, 5);
+                tc05::mbar_wait(&full[s], (uint32_t)((i >> 1) & 1));
+                if (cn < a.nch) tc05::mbar_wait(&full[s ^ 1], (uint32_t)(((i + 1) >> 1) & 1));
+            }
+            __syncthreads();
+            return;
+        }
+        const int4 md = meta[s];
+        const int j0 = md.x, nn = md.y, e0 = md.z, ne = md.w;
+        const unsigned char* st = smem_e + s * L.bytes;
+        const double* sh = reinterpret_cast<const double*>(st + L.h);
+        const double* skr = reinterpret_cast<const double*>(st + L.krw);
+        const double* sx = reinterpret_cast<const double*>(st + L.xyz);
+        const ushort4* sel = reinterpret_cast<const ushort4*>(st + L.eloc);
+        const uint2* sup = reinterpret_cast<const uint2*>(st + L.upw);
+        const double* sk = reinterpret_cast<const double*>(st + L.ek);
+        const unsigned short* slc = reinterpret_cast<const unsigned short*>(st + L.lc);
+        const unsigned short* slp = reinterpret_cast<const unsigned short*>(st + L.lp);
 #pragma unroll
-    for (int f = 0; f < 6; ++f) {
-        double q = C[f][0] * hv[0];
-        q += C[f][1] * hv[1];
-        q += C[f][2] * hv[2];
-        q += C[f][3] * hv[3];
-        q += G[f];
-        int a = tet_edge_a(f), b = tet_edge_b(f);
-        unsigned u = ((f < 4 ? uw.x >> (8 * f) : uw.y >> (8 * (f - 4)))) & 0xffu;
-        double flux = rho0 * (q * face_krw(u, kr[a], kr[b]));
-        c[a] -= flux;
-        c[b] += flux;
+        for (int t = 0; t < EPT; ++t) {
+            const int el = threadIdx.x + t * kElemThreads;
+            if (el >= ne) continue;
+            const int e = e0 + el;
+            const ushort4 lq = sel[el];
+            const int li[4] = {lq.x, lq.y, lq.z, lq.w};
+            double hv[NPE], kr[NPE];
+            const size_t zo = MZ ? (size_t)a.ezone[e] * a.N : 0;
+#pragma unroll
+            for (int k = 0; k < NPE; ++k) {
+                hv[k] = sh[li[k]];
+                kr[k] = MZ ? a.krw[zo + a.ch_node[j0 + li[k]]] : skr[li[k]];
+            }
+            double q[NFE];
+            if (VAR == 0) {
+#pragma unroll
+                for (int f = 0; f < NFE; ++f) {
+                    const double* cf = a.coef + (size_t)(f * (NPE + 1)) * a.T + e;
+                    double sacc = cf[0] * hv[0];
+#pragma unroll
+                    for (int k = 1; k < NPE; ++k) sacc += cf[(size_t)k * a.T] * hv[k];
+                    q[f] = sacc + cf[(size_t)NPE * a.T];
+                }
+            } else {
+                double X[4][3];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    X[k][0] = sx[li[k]];
+                    X[k][1] = sx[a.nnmax + li[k]];
+                    X[k][2] = sx[2 * a.nnmax + li[k]];
+                }
+                const double K0 = sk[el];
+                const double K1 = a.kiso ? K0 : sk[a.CE + el];
+                const double K2 = a.kiso ? K0 : sk[2 * a.CE + el];
+                double qq[6];
+                tet_face_fluxes(X[0], X[1], X[2], X[3], K0, K1, K2, hv[0], hv[1], hv[2], hv[3 % NPE], qq);
+#pragma unroll
+                for (int f = 0; f < NFE; ++f) q[f] = qq[f];
+            }
+            const uint2 uw = sup[el];
+            double cacc[NPE];
+#pragma unroll
+            for (int k = 0; k < NPE; ++k) cacc[k] = 0.0;
+#pragma unroll
+            for (int f = 0; f < NFE; ++f) {
+                const int fa = NPE == 4 ? tet_edge_a(f) : tri_edge_a(f);
+                const int fb = NPE == 4 ? tet_edge_b(f) : tri_edge_b(f);
+                const unsigned u = (f < 4 ? uw.x >> (8 * f) : uw.y >> (8 * (f - 4))) & 0xffu;
+                const double flux = a.rho0 * (q[f] * face_krw(u, kr[fa], kr[fb]));
+                cacc[fa] -= flux;
+                cacc[fb] += flux;
+            }
+#pragma unroll
+            for (int k = 0; k < NPE; ++k) cc[k * a.CE + el] = cacc[k];
+        }
+        __syncthreads();
+        // one partial per chunk node, corners in ascending element order
+        for (int j = threadIdx.x; j < nn; j += kElemThreads) {
+            const int p0 = slp[j], p1 = slp[j + 1];
+            double sacc = 0.0;
+            for (int p = p0; p < p1; ++p) sacc += cc[slc[p]];
+            a.part[j0 + j] = sacc;
+        }
+        __syncthreads();
     }
-    int4 ps = epos[e];
-    slots[ps.x] = c[0];
-    slots[ps.y] = c[1];
-    slots[ps.z] = c[2];
-    slots[ps.w] = c[3];
 }
 
-template <bool MULTIZONE>
-__global__ void __launch_bounds__(256) k_elem_tri(int T, int N, const int4* __restrict__ en,
-                                                   const double* __restrict__ coef,
-                                                   const int* __restrict__ ezone,
-                                                   const double* __restrict__ krw,
-                                                   const double* __restrict__ h,
-                                                   const unsigned char* __restrict__ upw,
-                                                   double rho0, const int4* __restrict__ epos,
-                                                   double* __restrict__ slots) {
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= T) return;
-    int4 nd = en[e];
-    double hv[3] = {h[nd.x], h[nd.y], h[nd.z]};
-    size_t zo = MULTIZONE ? (size_t)ezone[e] * N : 0;
-    double kr[3] = {krw[zo + nd.x], krw[zo + nd.y], krw[zo + nd.z]};
-    unsigned uw = *reinterpret_cast<const unsigned*>(upw + (size_t)8 * e);
-    double c[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int f = 0; f < 3; ++f) {
-        const double* cf = coef + (size_t)(f * 4) * T + e;
-        double q = cf[0] * hv[0];
-        q += cf[(size_t)T] * hv[1];
-        q += cf[(size_t)2 * T] * hv[2];
-        q += cf[(size_t)3 * T];
-        int a = tri_edge_a(f), b = tri_edge_b(f);
-        unsigned u = (uw >> (8 * f)) & 0xffu;
-        double flux = rho0 * (q * face_krw(u, kr[a], kr[b]));
-        c[a] -= flux;
-        c[b] += flux;
-    }
-    int4 ps = epos[e];
-    slots[ps.x] = c[0];
-    slots[ps.y] = c[1];
-    slots[ps.z] = c[2];
-}
-
-// node gather: the element pass left node i's partials in the contiguous
-// slot range [inc_ptr[i], inc_ptr[i+1]) in ascending element order; sum
-// them in that order.  F0 != nullptr turns the result into
-// (F - F0) * inv_sigma.
-__global__ void k_gather(int N, const int* __restrict__ inc_ptr,
-                         const double* __restrict__ slots, const double* __restrict__ invV,
+// node gather: the element pass left node i's partials, one per chunk that
+// touches the node, at the chunk-major positions cpos[part_ptr[i] ..
+// part_ptr[i+1]) in ascending chunk order; sum them in that order.
+// F0 != nullptr turns the result into (F - F0) * inv_sigma.
+__global__ void k_gather(int N, const int* __restrict__ part_ptr, const int* __restrict__ cpos,
+                         const double* __restrict__ part, const double* __restrict__ invV,
                          const double* __restrict__ bterm, const double* __restrict__ hD,
                          const unsigned char* __restrict__ ntype, const double* __restrict__ h,
                          const double* __restrict__ stor, const double* __restrict__ F0,
@@ -226,8 +331,8 @@ __global__ void k_gather(int N, const int* __restrict__ inc_ptr,
         r = hD[i] - h[i];
     } else {
         double s = 0.0;
-        int p1 = inc_ptr[i + 1];
-        for (int p = inc_ptr[i]; p < p1; ++p) s += slots[p];
+        int p1 = part_ptr[i + 1];
+        for (int p = part_ptr[i]; p < p1; ++p) s += part[cpos[p]];
         r = s * invV[i];
         r = r + bterm[i];
         r = r - stor[i];
@@ -292,6 +397,167 @@ __global__ void k_edge_upwind(int E, int nfe, const int* __restrict__ edge_ptr,
 }
 
 // ------------------------------------------------------------------ drivers
+static NodeCopies node_copies(fvm_ctx* c) {
+    NodeCopies cp;
+    cp.part_ptr = c->part_ptr.p;
+    cp.cpos = c->ch_cpos.p;
+    cp.ch_h = c->ch_h.p;
+    cp.ch_krw = c->ch_krw.p;
+    return cp;
+}
+
+// elements per thread of a chunk CTA (powers of two up to 8)
+static int chunk_ept(int CE) {
+    int t = (CE + kElemThreads - 1) / kElemThreads;
+    return t <= 1 ? 1 : t <= 2 ? 2 : t <= 4 ? 4 : 8;
+}
+
+// dispatch on the run-time shape: f is called with the kernel instance
+template <class F> static void with_elem_kernel(const fvm_ctx* c, F&& f) {
+    const bool mz = c->nz > 1;
+    const int ept = chunk_ept(c->chunk_e);
+    auto by_ept = [&](auto k1, auto k2, auto k4, auto k8) {
+        if (ept == 1) f(k1);
+        else if (ept == 2) f(k2);
+        else if (ept == 4) f(k4);
+        else f(k8);
+    };
+#define FVM_EPT(NPE, NFE, V, M) k_elem_chunk<NPE, NFE, V, M, 1>, k_elem_chunk<NPE, NFE, V, M, 2>, \
+                                k_elem_chunk<NPE, NFE, V, M, 4>, k_elem_chunk<NPE, NFE, V, M, 8>
+    if (c->dim == 3) {
+        if (c->recompute) mz ? by_ept(FVM_EPT(4, 6, 1, true)) : by_ept(FVM_EPT(4, 6, 1, false));
+        else mz ? by_ept(FVM_EPT(4, 6, 0, true)) : by_ept(FVM_EPT(4, 6, 0, false));
+    } else {
+        mz ? by_ept(FVM_EPT(3, 3, 0, true)) : by_ept(FVM_EPT(3, 3, 0, false));
+    }
+#undef FVM_EPT
+}
+
+// shared bytes of one element-pass CTA: two pipeline stages, the corner
+// partials, the stage descriptors and the two mbarriers
+static size_t chunk_smem_bytes(const fvm_ctx* c, int CE, int nnmax) {
+    const StageLayout L(CE, c->npe, nnmax, c->nz > 1, c->recompute, c->kiso);
+    return 2 * L.bytes + sizeof(double) * (size_t)CE * c->npe + 2 * sizeof(int4) + 2 * sizeof(uint64_t);
+}
+
+static void set_chunk_attrs(fvm_ctx* c) {
+    with_elem_kernel(c, [&](auto k) {
+        FVM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->chunk_smem));
+    });
+}
+
+static void launch_elem(fvm_ctx* c, const double* h) {
+    ElemArgs a;
+    (void)h;   // the node pass left the head in the chunk-major copies
+    a.T = c->T; a.N = c->N; a.CE = c->chunk_e; a.nch = c->nchunk; a.kiso = c->kiso ? 1 : 0;
+    a.estride = c->estride; a.nnmax = c->chunk_maxnn;
+    a.ch_seg = c->ch_seg.p; a.ch_node = c->ch_node.p;
+    a.elocal = c->elocal.p; a.ch_lptr = c->ch_lptr.p; a.ch_lc = c->ch_lc.p;
+    a.coef = c->coef.p; a.ch_xyz = c->ch_xyz.p; a.eK = c->eK.p; a.ezone = c->ezone.p;
+    a.krw = c->krw.p; a.ch_h = c->ch_h.p; a.ch_krw = c->ch_krw.p; a.upw = c->upw.p; a.rho0 = c->rho0;
+    a.part = c->part.p; a.err = c->elem_err.p; a.P = c->ch_node.n;
+    with_elem_kernel(c, [&](auto k) { fvm_launch(c, k, c->chunk_grid, kElemThreads, c->chunk_smem, c->stream, a); });
+}
+
+// Chunk the elements (consecutive ids, CE per chunk) and build the tables
+// of the chunked element pass: the distinct nodes of every chunk, the
+// 16-bit local corner ids, the node-ordered corner lists, and the node-major
+// layout of the per-(node, chunk) partials that the gather sums.
+static void build_chunks(fvm_ctx* c, int CE) {
+    const int T = c->T, N = c->N, npe = c->npe;
+    if (CE < 32 || CE > 8 * kElemThreads) throw Error("chunk size out of range (32..2048 elements)");
+    if (CE % 8) throw Error("chunk size must be a multiple of 8");
+    const int nch = (T + CE - 1) / CE;
+    const size_t ES = (size_t)c->estride;
+    const std::vector<int>& en = c->h_elem_nodes;
+    // chunk c's nodes occupy the padded segment [seg.x, seg.x + pad8(nn + 1))
+    std::vector<int2> seg(nch);
+    std::vector<int> ch_node;
+    ch_node.reserve((size_t)T);
+    std::vector<ushort4> elocal(ES, make_ushort4(0, 0, 0, 0));
+    std::vector<unsigned short> lptr, lc(ES * npe, 0);
+    lptr.reserve((size_t)T + 8 * nch);
+    std::vector<int> stamp(N, -1), lid(N, 0), pcount(N, 0), nodes, cnt;
+    int maxnn = 0;
+    for (int ch = 0; ch < nch; ++ch) {
+        const int e0 = ch * CE, e1 = std::min(T, e0 + CE);
+        nodes.clear();
+        for (int e = e0; e < e1; ++e)
+            for (int k = 0; k < npe; ++k) {
+                int g = en[(size_t)e * npe + k];
+                if (stamp[g] != ch) { stamp[g] = ch; nodes.push_back(g); }
+            }
+        std::sort(nodes.begin(), nodes.end());
+        const int nn = (int)nodes.size();
+        const int nnp = pad8(nn + 1);
+        maxnn = std::max(maxnn, nnp);
+        seg[ch] = make_int2((int)ch_node.size(), nn);
+        for (int j = 0; j < nn; ++j) { lid[nodes[j]] = j; pcount[nodes[j]]++; }
+        cnt.assign(nn + 1, 0);
+        for (int e = e0; e < e1; ++e) {
+            unsigned short l[4] = {0, 0, 0, 0};
+            for (int k = 0; k < npe; ++k) {
+                l[k] = (unsigned short)lid[en[(size_t)e * npe + k]];
+                cnt[l[k] + 1]++;
+            }
+            elocal[e] = make_ushort4(l[0], l[1], l[2], l[3]);
+        }
+        for (int j = 0; j < nn; ++j) cnt[j + 1] += cnt[j];
+        for (int j = 0; j <= nn; ++j) lptr.push_back((unsigned short)cnt[j]);
+        lptr.resize(lptr.size() + (nnp - nn - 1), 0);
+        for (int e = e0; e < e1; ++e)
+            for (int k = 0; k < npe; ++k) {
+                int j = lid[en[(size_t)e * npe + k]];
+                lc[(size_t)e0 * npe + cnt[j]++] = (unsigned short)(k * CE + (e - e0));
+            }
+        ch_node.insert(ch_node.end(), nodes.begin(), nodes.end());
+        ch_node.resize(ch_node.size() + (nnp - nn), nodes.empty() ? 0 : nodes.back());
+    }
+    std::vector<int> part_ptr(N + 1, 0);
+    for (int i = 0; i < N; ++i) part_ptr[i + 1] = part_ptr[i] + pcount[i];
+    // node-major copy slot q -> chunk-major position (ascending chunk per node)
+    std::vector<int> cpos(part_ptr[N]), seen(N, 0);
+    for (int ch = 0; ch < nch; ++ch)
+        for (int j = 0; j < seg[ch].y; ++j) {
+            const int p = seg[ch].x + j;
+            const int g = ch_node[p];
+            cpos[part_ptr[g] + seen[g]++] = p;
+        }
+    cudaStream_t s = c->stream;
+    c->chunk_e = CE;
+    c->nchunk = nch;
+    c->chunk_maxnn = maxnn;
+    c->ch_seg.upload(seg, s);
+    c->ch_node.upload(ch_node, s);
+    c->ch_cpos.upload(cpos, s);
+    const size_t P = ch_node.size();
+    if (c->dim == 3) {
+        std::vector<double> cx(3 * P);
+        for (size_t p = 0; p < P; ++p)
+            for (int d = 0; d < 3; ++d) cx[(size_t)d * P + p] = c->h_xyz[(size_t)d * N + ch_node[p]];
+        c->ch_xyz.upload(cx, s);
+    }
+    c->ch_h.alloc(P);
+    c->ch_krw.alloc(P);
+    c->elocal.upload(elocal, s);
+    c->ch_lptr.upload(lptr, s);
+    c->ch_lc.upload(lc, s);
+    c->part_ptr.upload(part_ptr, s);
+    c->part.alloc(ch_node.size());
+    c->chunk_smem = chunk_smem_bytes(c, CE, maxnn);
+    if (c->chunk_smem > 227 * 1024) throw Error("chunk does not fit in shared memory");
+    set_chunk_attrs(c);
+    // persistent grid: as many CTAs as fit on the device at once
+    int per_sm = 0, nsm = 0;
+    with_elem_kernel(c, [&](auto k) {
+        FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kElemThreads, c->chunk_smem));
+    });
+    FVM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    if (per_sm < 1) throw Error("element pass: chunk does not fit on an SM");
+    c->chunk_grid = std::min(nch, per_sm * nsm);
+    FVM_CUDA(cudaStreamSynchronize(s));
+}
+
 void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Perturb& pt,
                      const double* F0, double* out) {
     cudaStream_t s = c->stream;
@@ -299,33 +565,15 @@ void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Pertur
     c->tm.begin(TM_NODE, s);
     fvm_launch(c, k_node, grid_for(c->N, kBlock), kBlock, 0, s, c->N, y, yp, pt, c->zones.p, c->nz, c->nz_ptr.p,
                                                       c->nz_zone.p, c->nz_w.p, c->rho0, c->krw.p,
-                                                      c->hstar.p, c->stor.p);
+                                                      c->hstar.p, c->stor.p, node_copies(c));
     c->tm.end(TM_NODE, s);
-    int gb = grid_for(c->T, kBlock);
     c->tm.begin(TM_ELEM, s);
-    if (c->dim == 3) {
-        if (c->recompute) {
-            if (c->nz > 1)
-                fvm_launch(c, k_elem_tet_rc<true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->xyz.p, c->eK.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
-            else
-                fvm_launch(c, k_elem_tet_rc<false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->xyz.p, c->eK.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
-        } else {
-            if (c->nz > 1)
-                fvm_launch(c, k_elem_tet<true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
-            else
-                fvm_launch(c, k_elem_tet<false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
-        }
-    } else {
-        if (c->nz > 1)
-            fvm_launch(c, k_elem_tri<true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
-        else
-            fvm_launch(c, k_elem_tri<false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, h, c->upw.p, c->rho0, c->epos.p, c->slots.p);
-    }
+    launch_elem(c, h);
     c->tm.end(TM_ELEM, s);
     double inv_sigma = 0.0;
     if (F0 && !pt.sigma_dev) inv_sigma = 1.0 / pt.sigma;
     c->tm.begin(TM_GATHER, s);
-    fvm_launch(c, k_gather, grid_for(c->N, kBlock), kBlock, 0, s, c->N, c->inc_ptr.p, c->slots.p,
+    fvm_launch(c, k_gather, grid_for(c->N, kBlock), kBlock, 0, s, c->N, c->part_ptr.p, c->ch_cpos.p, c->part.p,
                                                         c->invV.p, c->bterm.p, c->hD.p, c->ntype.p,
                                                         h, c->stor.p, F0, inv_sigma,
                                                         F0 ? pt.sigma_dev : nullptr, out);
@@ -338,7 +586,7 @@ void launch_begin_step(fvm_ctx* c, const double* y, const double* yp) {
     Perturb none;
     fvm_launch(c, k_node, grid_for(c->N, kBlock), kBlock, 0, s, c->N, y, yp, none, c->zones.p, c->nz, c->nz_ptr.p,
                                                       c->nz_zone.p, c->nz_w.p, c->rho0, c->krw.p,
-                                                      c->hstar.p, c->stor.p);
+                                                      c->hstar.p, c->stor.p, node_copies(c));
     int gb = grid_for(c->T, kBlock);
     if (c->dim == 3) {
         if (c->nz > 1) fvm_launch(c, k_faceq<4, 6, true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
@@ -355,6 +603,85 @@ void reset_upwind(fvm_ctx* c) {
     FVM_CUDA(cudaMemsetAsync(c->upw.p, 2, c->upw.n, c->stream));
 }
 
+// head from the hydrostatic/Dirichlet rules of set_initial_conditions
+// (vs.h:8-32)
+static std::vector<double> initial_head_host(const fvm_ctx* c, double water_table) {
+    std::vector<double> h(c->N);
+    for (int i = 0; i < c->N; ++i) h[i] = c->h_node_type[i] ? c->h_hD[i] : water_table - c->h_vert[i];
+    return h;
+}
+
+// ------------------------------------------------------------------ autotuner
+// Times the element pass for every (variant, chunk size) candidate on the
+// context's own mesh and keeps the fastest.  Each candidate runs on the
+// hydrostatic initial head; every timed launch follows a write of a buffer
+// larger than the L2 cache, so no candidate profits from data left there by
+// the previous launch.  CUDA events on the context stream, median of the
+// timed launches.
+static void autotune(fvm_ctx* c, fvm_tune_result* out) {
+    const int chunks[] = {256, 512, 1024, 2048};
+    const int nvar = c->dim == 3 ? 2 : 1;
+    cudaStream_t s = c->stream;
+    std::vector<double> y0 = initial_head_host(c, 0.0);
+    DevBuf<double> y, yp, flush;
+    y.alloc(c->N);
+    yp.alloc(c->N);
+    yp.zero(s);
+    FVM_CUDA(cudaMemcpyAsync(y.p, y0.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice, s));
+    const size_t flush_n = (size_t)192 << 20;   // 192 MiB > 126 MB L2
+    flush.alloc(flush_n / sizeof(double));
+    Perturb none;
+    cudaEvent_t e0, e1;
+    FVM_CUDA(cudaEventCreate(&e0));
+    FVM_CUDA(cudaEventCreate(&e1));
+    const bool rc0 = c->recompute;
+    const int ce0 = c->chunk_e;
+    double best = 1e300;
+    int best_var = rc0 ? 1 : 0, best_ce = ce0, n = 0, best_i = -1;
+    for (int v = 0; v < nvar; ++v)
+        for (int ce : chunks) {
+            c->recompute = v == 1;
+            try {
+                build_chunks(c, ce);
+            } catch (const Error&) {
+                continue;   // does not fit in shared memory
+            }
+            // chunk-major node copies of this partition
+            fvm_launch(c, k_node, grid_for(c->N, kBlock), kBlock, 0, s, c->N, y.p, yp.p, none, c->zones.p, c->nz,
+                       c->nz_ptr.p, c->nz_zone.p, c->nz_w.p, c->rho0, c->krw.p, c->hstar.p, c->stor.p,
+                       node_copies(c));
+            for (int w = 0; w < 2; ++w) launch_elem(c, y.p);
+            std::vector<float> t;
+            for (int k = 0; k < 7; ++k) {
+                FVM_CUDA(cudaMemsetAsync(flush.p, k, flush_n, s));
+                FVM_CUDA(cudaEventRecord(e0, s));
+                launch_elem(c, y.p);
+                FVM_CUDA(cudaEventRecord(e1, s));
+                FVM_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.0f;
+                FVM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                t.push_back(ms);
+            }
+            std::sort(t.begin(), t.end());
+            double us = 1e3 * t[t.size() / 2];
+            if (out && n < FVM_TUNE_MAX) {
+                out->variant[n] = v;
+                out->chunk[n] = ce;
+                out->us[n] = us;
+            }
+            if (us < best) { best = us; best_var = v; best_ce = ce; best_i = n; }
+            ++n;
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->recompute = best_var == 1;
+    build_chunks(c, best_ce);
+    if (out) {
+        out->n = std::min(n, FVM_TUNE_MAX);
+        out->best = best_i;
+    }
+}
+
 // ------------------------------------------------------------------ set-up
 static void build(fvm_ctx* c, const fvm_mesh* m, const fvm_physics* ph, int flags) {
     if (!m || !ph) throw Error("fvm_create: null argument");
@@ -367,8 +694,12 @@ static void build(fvm_ctx* c, const fvm_mesh* m, const fvm_physics* ph, int flag
     const int npe = dim + 1, nfe = dim == 2 ? 3 : 6;
     if ((long)T * nfe >= (1l << 31) - 1) throw Error("fvm_create: mesh too large");
     c->dim = dim; c->N = N; c->T = T; c->npe = npe; c->nfe = nfe;
+    c->estride = pad8(T) + 8;   // per-element arrays padded for whole 16-byte chunk copies
     c->nz = ph->n_zones; c->rho0 = ph->rho0;
-    c->recompute = (flags & FVM_FLAG_RECOMPUTE_GEOMETRY) && dim == 3;
+    // 3D default: rebuild the face geometry from the vertices (FP64 ALU
+    // instead of 240 B of streamed coefficients per element)
+    c->recompute = dim == 3 && !(flags & FVM_FLAG_STORED_GEOMETRY);
+    if (flags & FVM_FLAG_RECOMPUTE_GEOMETRY) c->recompute = dim == 3;
     FVM_CUDA(cudaGetDevice(&c->device));
     FVM_CUDA(cudaStreamCreate(&c->stream));   // blocking: orders after the legacy default stream
     cudaStream_t s = c->stream;
@@ -565,12 +896,22 @@ static void build(fvm_ctx* c, const fvm_mesh* m, const fvm_physics* ph, int flag
 
     // ---- upload
     c->enodes.upload(en, s);
-    if (c->recompute) {
+    if (dim == 3) {
+        // vertices and conductivities for the rebuilt-geometry element pass;
+        // one K per element when every element is isotropic
         std::vector<double> xyz((size_t)3 * N);
         for (int i = 0; i < N; ++i)
             for (int d = 0; d < 3; ++d) xyz[(size_t)d * N + i] = m->coords[3 * (size_t)i + d];
         c->xyz.upload(xyz, s);
-        c->eK.upload(eK3, s);
+        c->h_xyz = xyz;
+        c->kiso = true;
+        for (int e = 0; e < T && c->kiso; ++e)
+            c->kiso = eK3[e] == eK3[(size_t)T + e] && eK3[e] == eK3[(size_t)2 * T + e];
+        const size_t ES = (size_t)c->estride;
+        std::vector<double> ek((c->kiso ? 1 : 3) * ES, 0.0);
+        for (int d = 0; d < (c->kiso ? 1 : 3); ++d)
+            for (int e = 0; e < T; ++e) ek[(size_t)d * ES + e] = eK3[(size_t)d * T + e];
+        c->eK.upload(ek, s);
     }
     c->coef.upload(coef, s);
     if (c->nz > 1) c->ezone.upload(std::vector<int>(m->elem_zone, m->elem_zone + T), s);
@@ -581,18 +922,6 @@ static void build(fvm_ctx* c, const fvm_mesh* m, const fvm_physics* ph, int flag
     c->nz_ptr.upload(nz_ptr, s);
     c->nz_zone.upload(nz_zone, s);
     c->nz_w.upload(nz_w, s);
-    c->inc_ptr.upload(inc_ptr, s);
-    c->inc.upload(inc, s);
-    {
-        // slot of (e, k) in the node-ordered partial array: the inverse of inc
-        std::vector<int4> epos(T, make_int4(0, 0, 0, 0));
-        for (size_t p = 0; p < inc.size(); ++p) {
-            int e = inc[p] / npe, k = inc[p] % npe;
-            int* q = reinterpret_cast<int*>(&epos[e]);
-            q[k] = (int)p;
-        }
-        c->epos.upload(epos, s);
-    }
     std::vector<ZoneDev> zd(ph->n_zones);
     for (int z = 0; z < ph->n_zones; ++z) {
         const fvm_zone& Z = ph->zones[z];
@@ -605,15 +934,17 @@ static void build(fvm_ctx* c, const fvm_mesh* m, const fvm_physics* ph, int flag
     c->edge_w.upload(edge_w, s);
     c->flip.upload(flip, s);
     // averaged weights until the first begin_step (fvmpor.h:594-595)
-    c->upw.upload(std::vector<unsigned char>((size_t)8 * T, 2), s);
+    c->upw.upload(std::vector<unsigned char>((size_t)8 * c->estride, 2), s);
     c->krw.alloc((size_t)c->nz * N);
     c->krw.zero(s);
     c->hstar.alloc(N);
     c->stor.alloc(N);
-    c->slots.alloc((size_t)T * npe);
     c->faceq.alloc((size_t)T * nfe);
     for (auto& b : c->tmpN) b.alloc(N);
-    FVM_CUDA(cudaStreamSynchronize(s));
+    c->elem_err.alloc(1);
+    c->elem_err.zero(s);
+    build_chunks(c, kDefaultChunk);
+    if (flags & FVM_FLAG_AUTOTUNE) autotune(c, nullptr);
 }
 
 } // namespace fvmb
@@ -667,8 +998,7 @@ extern "C" int fvm_n_nodes(const fvm_ctx* c) { return c ? c->N : 0; }
 extern "C" int fvm_initial_head(fvm_ctx* c, double water_table, double* y) {
     FVM_API_BEGIN
     if (!c || !y) throw Error("fvm_initial_head: null argument");
-    std::vector<double> h(c->N);
-    for (int i = 0; i < c->N; ++i) h[i] = c->h_node_type[i] ? c->h_hD[i] : water_table - c->h_vert[i];
+    std::vector<double> h = initial_head_host(c, water_table);
     FVM_CUDA(cudaMemcpyAsync(y, h.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
     FVM_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
@@ -712,6 +1042,44 @@ extern "C" int fvm_jv(fvm_ctx* c, double t, double cj, const double* y, const do
     launch_residual(c, y, yp, pt, F0, Jv);
     FVM_CUDA(cudaGetLastError());
     FVM_CUDA(cudaStreamSynchronize(c->stream));
+    return 0;
+    FVM_API_END
+}
+
+extern "C" int fvm_autotune(fvm_ctx* c, fvm_tune_result* out) {
+    FVM_API_BEGIN
+    if (!c) throw Error("fvm_autotune: null context");
+    if (out) std::memset(out, 0, sizeof(*out));
+    autotune(c, out);
+    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    return 0;
+    FVM_API_END
+}
+
+extern "C" int fvm_set_element_pass(fvm_ctx* c, int variant, int chunk) {
+    FVM_API_BEGIN
+    if (!c) throw Error("fvm_set_element_pass: null context");
+    if (variant != 0 && variant != 1) throw Error("fvm_set_element_pass: variant must be 0 or 1");
+    if (variant == 1 && c->dim != 3) throw Error("fvm_set_element_pass: rebuilt geometry is a 3D variant");
+    const bool old_rc = c->recompute;
+    const int old_ce = c->chunk_e;
+    c->recompute = variant == 1;
+    try {
+        build_chunks(c, chunk);
+    } catch (...) {
+        c->recompute = old_rc;
+        build_chunks(c, old_ce);
+        throw;
+    }
+    return 0;
+    FVM_API_END
+}
+
+extern "C" int fvm_element_pass(const fvm_ctx* c, int* variant, int* chunk) {
+    FVM_API_BEGIN
+    if (!c) throw Error("fvm_element_pass: null context");
+    if (variant) *variant = c->recompute ? 1 : 0;
+    if (chunk) *chunk = c->chunk_e;
     return 0;
     FVM_API_END
 }

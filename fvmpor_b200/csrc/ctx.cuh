@@ -93,6 +93,12 @@ FVM_HD void van_genuchten(double h, const ZoneDev& z, double& Sw, double& dSw, d
     krw = k;
 }
 
+// krw at a face: upwind node (0/1) or the averaged weights 0.5/0.5 the
+// reference uses before the first step (fvmpor.h:594-595, 919-924)
+FVM_HD double face_krw(unsigned u, double ka, double kb) {
+    return u == 0 ? ka : (u == 1 ? kb : ka * 0.5 + kb * 0.5);
+}
+
 // ---------------------------------------------------------------------------
 // Perturbation applied by the node pass before the residual:
 //   mode 0: none (plain residual)
@@ -129,13 +135,14 @@ struct fvm_ctx {
     std::vector<int> h_node_type;    // 0 free, 1 Dirichlet
     std::vector<double> h_vert;      // elevation of each node
     std::vector<double> h_hD;        // Dirichlet head (valid where type 1)
+    std::vector<double> h_xyz;       // [3][N] coordinates (3D)
 
     // element data
     fvmb::DevBuf<int4> enodes;        // [T] node ids (4th = -1 for triangles)
     fvmb::DevBuf<double> coef;        // [(f*(npe+1)+k)*T + e]
     fvmb::DevBuf<int> ezone;          // [T], only when nz > 1
-    fvmb::DevBuf<double> eK;          // [3][T] conductivities (recompute variant)
-    fvmb::DevBuf<double> xyz;         // [3][N] coordinates (recompute variant)
+    fvmb::DevBuf<double> eK;          // [T] (kiso) or [3][T] conductivities (3D)
+    fvmb::DevBuf<double> xyz;         // [3][N] coordinates (3D)
     fvmb::DevBuf<unsigned char> upw;  // [T*8] upwind flag per face: 1 = node b
     fvmb::DevBuf<unsigned char> flip; // [T] bit f set when node a of face f is
                                       // the global back node of its edge
@@ -147,7 +154,6 @@ struct fvm_ctx {
     fvmb::DevBuf<unsigned char> ntype;
     fvmb::DevBuf<int> nz_ptr, nz_zone;  // zones touching each node (CSR)
     fvmb::DevBuf<double> nz_w;          // SCV volume fraction per node-zone
-    fvmb::DevBuf<int> inc_ptr, inc;     // node -> (e*npe + k), ascending e
     fvmb::DevBuf<fvmb::ZoneDev> zones;
 
     // edges (for the frozen upwind directions)
@@ -158,13 +164,29 @@ struct fvm_ctx {
     fvmb::DevBuf<double> krw;        // [nz][N]
     fvmb::DevBuf<double> hstar;      // perturbed head
     fvmb::DevBuf<double> stor;       // ahh * y'
-    fvmb::DevBuf<double> slots;      // [T*npe] element partials in node order
-    fvmb::DevBuf<int4> epos;         // [T] slot of each element node (4th = 0 in 2D)
+    // chunked element pass: CE consecutive elements per CTA
+    int chunk_e = 0, nchunk = 0, chunk_maxnn = 0;
+    size_t chunk_smem = 0;
+    bool kiso = false;                    // eK holds one K per element
+    int chunk_grid = 0;                   // persistent CTAs of the element pass
+    int estride = 0;                      // padded element count of the per-element arrays
+    fvmb::DevBuf<int2> ch_seg;            // [nchunk] (padded start, count) of each chunk's nodes
+    fvmb::DevBuf<int> elem_err;           // element-pass pipeline status
+    fvmb::DevBuf<int> ch_node;            // [P] distinct nodes per chunk, ascending
+    fvmb::DevBuf<int> ch_cpos;            // [P] node-major copy slot -> chunk-major position
+    fvmb::DevBuf<double> ch_xyz;          // [3][P] chunk-major coordinates (3D)
+    fvmb::DevBuf<double> ch_h, ch_krw;    // [P] chunk-major head / krw (node pass output)
+    fvmb::DevBuf<ushort4> elocal;         // [T] chunk-local corner ids
+    fvmb::DevBuf<unsigned short> ch_lptr; // [P + nchunk] corner-list offsets
+    fvmb::DevBuf<unsigned short> ch_lc;   // [T*npe] node-ordered corner lists
+    fvmb::DevBuf<int> part_ptr;           // [N+1] node -> its chunk copies (node-major slots)
+    fvmb::DevBuf<double> part;            // [P] per-(chunk, node) partials, chunk-major
     fvmb::DevBuf<double> faceq;      // [T*nfe] averaged-weight face fluxes
     fvmb::DevBuf<double> tmpN[4];    // scratch vectors
     fvmb::DevBuf<float> statf;       // [3][N] static node features: mean ln K, elevation,
                                      // CV surface area (learned predictor inputs)
 
+    int ilu_per_sm = 1;              // block-ILU blocks per SM on large meshes
     fvmb::BlockILU* ilu = nullptr;
     fvmb::Krylov* kry = nullptr;
     fvmb::Predictor* pred = nullptr;

@@ -18,6 +18,9 @@ struct Krylov {
     DevBuf<unsigned> counter;
     DevBuf<double> res;       // reduction results
     DevBuf<double> sigma;
+    DevBuf<unsigned> bar;     // grid barrier of the fused orthogonalisation
+    DevBuf<int> err;          // 3 = a grid barrier timed out
+    int coop_grid = 0;        // blocks of the cooperative launch, 0 = three-pass path
     double* host = nullptr;   // pinned
 };
 

@@ -158,6 +158,141 @@ __global__ void k_cgs_pass3(int N, int nv, B* __restrict__ U, size_t ld,
     last_block_reduce(partial, 1, counter, out);
 }
 
+// ---- fused Arnoldi orthogonalisation (one cooperative launch per step)
+// Grid barrier of a cooperative launch: arrival counter plus generation
+// word.  The wait is bounded; if it runs out the kernel records error 3 and
+// every block leaves at its next barrier.
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, int* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vg = gen;
+        const unsigned g = *vg;
+        __threadfence();
+        if (atomicAdd(count, 1u) == gridDim.x - 1) {
+            *count = 0u;
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            long it = 0;
+            while (*vg == g) {
+                if (++it > (1l << 26)) { atomicExch(err, 3); break; }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int*)err == 0;
+}
+
+// out[v] = sum over blocks b (ascending, lane-strided, fixed shuffle tree) of
+// partial[b * nv + v] -- the order of last_block_reduce, so every block gets
+// the same bits; written to shared memory
+__device__ __forceinline__ void block_reduce_all(const double* partial, int nv, int nblk, double* out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const volatile double* vp = partial;
+    for (int v = warp; v < nv; v += nw) {
+        double s = 0.0;
+        for (int b = lane; b < nblk; b += 32) s += vp[(size_t)b * nv + v];
+        s = warp_sum(s);
+        if (lane == 0) out[v] = s;
+    }
+    __syncthreads();
+}
+
+// CGS2 step of Arnoldi for basis vector nv (three reductions, two grid
+// barriers between them plus one after the norm), followed by the next
+// Krylov direction t = s_nv U_nv / ewt and its difference-quotient increment
+// sigma = 1 / ||t||_wrms:
+//   W = ewt Jv; a = U^T W; W -= U diag(s^2) a; b = U^T W; W -= U diag(s^2) b;
+//   U_nv = W; s_nv = 1 / ||U_nv||.
+// res receives a (m+2 slots), b (m+2 slots) and ||U_nv||^2, as the three
+// separate passes wrote them.
+template <class B>
+__global__ void __launch_bounds__(kRedThreads) k_arnoldi_cgs2(int N, int nv, int mslot, B* __restrict__ U, size_t ld,
+                                                              double* __restrict__ scale,
+                                                              const double* __restrict__ Jv,
+                                                              const double* __restrict__ ewt,
+                                                              double* __restrict__ W, double* partial,
+                                                              unsigned* bar, int* err, double* res,
+                                                              double* __restrict__ t_next, double* sigma_next) {
+    __shared__ double coef[64];
+    __shared__ double red[32];
+    const int nblk = gridDim.x;
+    const int chunk = (N + nblk - 1) / nblk;
+    const int k0 = blockIdx.x * chunk, k1 = min(N, k0 + chunk);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    double* pa = partial;
+    double* pb = partial + (size_t)nblk * 64;
+    double* pc = partial + (size_t)nblk * 128;
+    // pass 1
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) W[k] = ewt[k] * Jv[k];
+    __syncthreads();
+    for (int i = warp; i < nv; i += nw) {
+        const B* Ui = U + ld * i;
+        double sacc = 0.0;
+        for (int k = k0 + lane; k < k1; k += 32) sacc += ldb(Ui, k) * W[k];
+        sacc = warp_sum(sacc);
+        if (lane == 0) pa[(size_t)blockIdx.x * nv + i] = sacc;
+    }
+    if (!grid_barrier(bar, bar + 1, err)) return;
+    block_reduce_all(pa, nv, nblk, coef);
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) res[i] = coef[i];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = coef[i] * scale[i] * scale[i];
+    __syncthreads();
+    // pass 2
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        double acc = 0.0;
+        for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
+        W[k] = W[k] - acc;
+    }
+    __syncthreads();
+    for (int i = warp; i < nv; i += nw) {
+        const B* Ui = U + ld * i;
+        double sacc = 0.0;
+        for (int k = k0 + lane; k < k1; k += 32) sacc += ldb(Ui, k) * W[k];
+        sacc = warp_sum(sacc);
+        if (lane == 0) pb[(size_t)blockIdx.x * nv + i] = sacc;
+    }
+    if (!grid_barrier(bar, bar + 1, err)) return;
+    block_reduce_all(pb, nv, nblk, coef);
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) res[mslot + i] = coef[i];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = coef[i] * scale[i] * scale[i];
+    __syncthreads();
+    // pass 3: new basis vector and its norm
+    B* Un = U + ld * nv;
+    double sq = 0.0;
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        double acc = 0.0;
+        for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
+        const B st = (B)(W[k] - acc);
+        Un[k] = st;
+        const double d = (double)st;
+        sq += d * d;
+    }
+    sq = warp_sum(sq);
+    if (lane == 0) red[warp] = sq;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double tt = threadIdx.x < nw ? red[threadIdx.x] : 0.0;
+        tt = warp_sum(tt);
+        if (threadIdx.x == 0) pc[blockIdx.x] = tt;
+    }
+    if (!grid_barrier(bar, bar + 1, err)) return;
+    block_reduce_all(pc, 1, nblk, coef);
+    const double nrm2 = coef[0];
+    const double sn = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        res[2 * mslot] = nrm2;
+        scale[nv] = sn;
+        // ||t||_wrms^2 = sum_k (s U_k)^2 / N
+        const double tw = sn * sn * nrm2 / (double)N;
+        *sigma_next = tw > 0.0 ? 1.0 / sqrt(tw) : 1.0;
+    }
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) t_next[k] = sn * ldb(Un, k) / ewt[k];
+}
+
 __global__ void k_set_scale(const double* nrm2, double* scale, int idx) {
     double n = sqrt(nrm2[0]);
     scale[idx] = n > 0.0 ? 1.0 / n : 0.0;
@@ -239,9 +374,25 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
     K->t.alloc(c->N);
     K->z.alloc(c->N);
     K->Jv.alloc(c->N);
-    K->partial.alloc((size_t)kRedBlocks * (m + 2));
+    K->partial.alloc((size_t)kRedBlocks * std::max(m + 2, 3 * 64));
     K->counter.alloc(1);
     K->counter.zero(c->stream);
+    K->bar.alloc(2);
+    K->bar.zero(c->stream);
+    K->err.alloc(1);
+    K->err.zero(c->stream);
+    {
+        // the fused orthogonalisation needs every block resident at once
+        int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+        FVM_CUDA(cudaGetDevice(&dev));
+        FVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        FVM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        if (precision)
+            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<float>, kRedThreads, 0));
+        else
+            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<double>, kRedThreads, 0));
+        K->coop_grid = (coop && per_sm > 0 && m + 1 <= 64) ? std::min(kRedBlocks, per_sm * nsm) : 0;
+    }
     K->res.alloc(3 * (m + 2) + 8);
     K->sigma.alloc(1);
     // results of the three passes plus the m+1 basis scales
@@ -274,11 +425,15 @@ double reduce_dot(fvm_ctx* c, const double* x, const double* y) {
     return K->host[0];
 }
 
-// J*v into out, sigma = 1/||v||_wrms computed on the device
+// J*v into out, sigma = 1/||v||_wrms computed on the device (or already in
+// K->sigma when have_sigma)
 static void jv_dev(fvm_ctx* c, Krylov* K, double cj, const double* y, const double* yp,
-                   const double* F0, const double* v, const double* ewt, double* out) {
-    fvm_launch(c, k_sumsq, kRedBlocks, kRedThreads, 0, c->stream, c->N, v, ewt, K->partial.p, K->counter.p, K->res.p);
-    fvm_launch(c, k_sigma_from_sumsq, 1, 1, 0, c->stream, K->res.p, c->N, K->sigma.p);
+                   const double* F0, const double* v, const double* ewt, double* out, bool have_sigma = false) {
+    if (!have_sigma) {
+        fvm_launch(c, k_sumsq, kRedBlocks, kRedThreads, 0, c->stream, c->N, v, ewt, K->partial.p, K->counter.p,
+                   K->res.p);
+        fvm_launch(c, k_sigma_from_sumsq, 1, 1, 0, c->stream, K->res.p, c->N, K->sigma.p);
+    }
     Perturb pt;
     pt.mode = 1;
     pt.cj = cj;
@@ -327,9 +482,13 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         int j = 0;
         bool conv = false;
         for (; j < m; ++j) {
-            // w = D P^-1 J D^-1 V_j (left preconditioning, scaled by D = ewt)
-            fvm_launch(c, k_unscale<B>, grid_for(N, 256), 256, 0, s, N, U + ld * j, K->scale.p, j, ewt, K->t.p);
-            jv_dev(c, K, cj, y, yp, F0, K->t.p, ewt, K->Jv.p);
+            // w = D P^-1 J D^-1 V_j (left preconditioning, scaled by D = ewt);
+            // the fused orthogonalisation of step j-1 already left the
+            // direction in K->t and its increment in K->sigma
+            const bool fused_in = j > 0 && K->coop_grid > 0;
+            if (!fused_in)
+                fvm_launch(c, k_unscale<B>, grid_for(N, 256), 256, 0, s, N, U + ld * j, K->scale.p, j, ewt, K->t.p);
+            jv_dev(c, K, cj, y, yp, F0, K->t.p, ewt, K->Jv.p, fused_in);
             if (cnt) cnt->njv++;
             psolve_dev(c, K->Jv.p, K->z.p);
             if (cnt) cnt->nps++;
@@ -338,14 +497,44 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
             double* rb = K->res.p + (m + 2);
             double* rn = K->res.p + 2 * (m + 2);
             c->tm.begin(TM_CGS, s);
-            fvm_launch(c, k_cgs_pass1<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->z.p, ewt, K->W.p, K->partial.p, K->counter.p, ra);
-            fvm_launch(c, k_cgs_pass2<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->scale.p, ra, K->W.p, K->partial.p, K->counter.p, rb);
-            fvm_launch(c, k_cgs_pass3<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->scale.p, rb, K->W.p, K->partial.p, K->counter.p, rn);
-            fvm_launch(c, k_set_scale, 1, 1, 0, s, rn, K->scale.p, nv);
+            if (K->coop_grid > 0) {
+                int Ni = N, nvi = nv, ms = m + 2;
+                B* Ub = U;
+                size_t ldv = ld;
+                double* scp = K->scale.p;
+                const double* jvp = K->z.p;
+                const double* ew = ewt;
+                double* Wp = K->W.p;
+                double* pp = K->partial.p;
+                unsigned* bp = K->bar.p;
+                int* ep = K->err.p;
+                double* rp = K->res.p;
+                double* tp = K->t.p;
+                double* sgp = K->sigma.p;
+                void* args[] = {&Ni, &nvi, &ms, &Ub, &ldv, &scp, &jvp, &ew, &Wp, &pp, &bp, &ep, &rp, &tp, &sgp};
+                FVM_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi_cgs2<B>, dim3(K->coop_grid),
+                                                     dim3(kRedThreads), args, 0, s));
+                c->launches++;
+            } else {
+                fvm_launch(c, k_cgs_pass1<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->z.p, ewt, K->W.p, K->partial.p, K->counter.p, ra);
+                fvm_launch(c, k_cgs_pass2<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->scale.p, ra, K->W.p, K->partial.p, K->counter.p, rb);
+                fvm_launch(c, k_cgs_pass3<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->scale.p, rb, K->W.p, K->partial.p, K->counter.p, rn);
+                fvm_launch(c, k_set_scale, 1, 1, 0, s, rn, K->scale.p, nv);
+            }
             c->tm.end(TM_CGS, s);
             FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, s));
             FVM_CUDA(cudaMemcpyAsync(K->host + 3 * (m + 2), K->scale.p, sizeof(double) * (nv), cudaMemcpyDeviceToHost, s));
+            int* herr = reinterpret_cast<int*>(K->host + 4 * (m + 2) + 7);
+            if (K->coop_grid > 0) FVM_CUDA(cudaMemcpyAsync(herr, K->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
             FVM_CUDA(cudaStreamSynchronize(s));
+            if (K->coop_grid > 0 && *herr != 0) {
+                // a grid barrier gave up: the step's numbers are not valid
+                K->err.zero(s);
+                K->bar.zero(s);
+                *iters = total;
+                *res_norm = rnorm;
+                return 2;
+            }
             const double* ha = K->host;
             const double* hb = K->host + (m + 2);
             const double* hsc = K->host + 3 * (m + 2);

@@ -27,6 +27,7 @@
 // (decomp/ILU.c:133-223).
 #include "ctx.cuh"
 #include "krylov.cuh"
+#include "tc05.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -37,11 +38,15 @@ namespace fvmb {
 struct BlockILU {
     bool built = false;
     int nnz = 0, ncol = 0;
-    std::vector<int> h_rowptr, h_col, h_cptr, h_colour;
+    std::vector<int> h_rowptr, h_col, h_colour;
     DevBuf<int> rowof, col;
     DevBuf<double> J;
-    DevBuf<int> colour, cnnz;
-    DevBuf<double> shift, Fc;
+    DevBuf<double> shift;
+    // element-wise finite-difference Jacobian
+    DevBuf<int> fd_epos;      // [T*npe*npe] slot of (element, perturbed node, corner)
+    DevBuf<int> fd_jptr;      // [nnz+1] slots of each nonzero
+    DevBuf<double> fd_slots;  // [T*npe*npe]
+    DevBuf<double> krwb, krwp, dstor;
     int nb = 0, maxb = 0;
     DevBuf<int> bstart, lu_ptr, lu_src, lu_diag;
     DevBuf<unsigned short> lu_col;
@@ -53,10 +58,14 @@ struct BlockILU {
     int* h_status = nullptr;  // pinned
     int nlevels_max = 0;
     size_t smem_stage[2] = {0, 0};   // staged apply: shared bytes for FP64 / FP32, 0 = not possible
+    int lanes = 4;                   // row entries prefetched per thread in the staged sweeps
 };
 
 // largest dynamic shared-memory carve-out a CTA may request on sm_100
 constexpr size_t kMaxDynSmem = 227 * 1024;
+// threads of a staged triangular-solve CTA: levels hold a few dozen rows,
+// so a small CTA keeps the per-level barrier cheap
+constexpr int kIluThreads = 128;
 
 // ------------------------------------------------------------------ kernels
 __global__ void k_shift(int N, const double* __restrict__ y, const double* __restrict__ yp,
@@ -68,15 +77,157 @@ __global__ void k_shift(int N, const double* __restrict__ y, const double* __res
     shift[j] = eps * fmax(a, fmax(b, w));
 }
 
-__global__ void k_fd_scatter(int count, const int* __restrict__ list, const int* __restrict__ rowof,
-                             const int* __restrict__ col, const double* __restrict__ Fc,
-                             const double* __restrict__ F0, const double* __restrict__ shift,
-                             double* __restrict__ J) {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= count) return;
-    int p = list[q];
-    int i = rowof[p], j = col[p];
-    J[p] = (Fc[i] - F0[i]) / shift[j];
+// ---- finite-difference Jacobian, one element at a time
+// Column j of the reference's coloured difference quotient is
+// (F(y + d_j e_j, y' + cj d_j e_j) - F(y, y')) / d_j (preconditioner_dss.cpp:
+// 284-373): the distance-2 colouring makes every row see at most one
+// perturbed node per colour, so the coloured evaluation equals these
+// single-column quotients.  With the upwind directions frozen, perturbing
+// node m changes only the elements that contain m, and only through h_m and
+// krw(h_m): each element forms the change of its corner partials for each of
+// its nodes in turn,
+//   dflux_f = rho0 (q_f (krw'_f - krw_f) + d_m C_fm krw'_f),
+// which is the same quotient written without the cancellation of two full
+// residuals.  The changes land in fixed slots (nonzero-major, ascending
+// element) and one pass per nonzero sums them, adds the storage term on the
+// diagonal and writes the Dirichlet rows: npe + 2 kernels per set-up instead
+// of one residual evaluation per colour.
+
+// per node: krw at h and h + d (every zone touching the node) and the change
+// of the storage term y' ahh(h) on the diagonal
+__global__ void k_fd_node(int N, const double* __restrict__ y, const double* __restrict__ yp, double cj,
+                          const double* __restrict__ shift, const ZoneDev* __restrict__ zones, int nz,
+                          const int* __restrict__ nz_ptr, const int* __restrict__ nz_zone,
+                          const double* __restrict__ nz_w, double rho0, double* __restrict__ krwb,
+                          double* __restrict__ krwp, double* __restrict__ dstor) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double h = y[i], d = shift[i];
+    const double hp = h + d;
+    double phi = 0.0, dsw = 0.0, dswp = 0.0;
+    const int p0 = nz == 1 ? i : nz_ptr[i], p1 = nz == 1 ? i + 1 : nz_ptr[i + 1];
+    for (int p = p0; p < p1; ++p) {
+        const int z = nz == 1 ? 0 : nz_zone[p];
+        const double w = nz_w[p];
+        double Sw, ds, k, dsp, kp;
+        van_genuchten(h, zones[z], Sw, ds, k);
+        van_genuchten(hp, zones[z], Sw, dsp, kp);
+        krwb[(size_t)z * N + i] = k;
+        krwp[(size_t)z * N + i] = kp;
+        phi += zones[z].phi * w;
+        dsw += ds * w;
+        dswp += dsp * w;
+    }
+    const double ahh = (phi * dsw) * rho0, ahhp = (phi * dswp) * rho0;
+    dstor[i] = (yp[i] + cj * d) * ahhp - yp[i] * ahh;
+}
+
+// per element: the npe x npe changes of its corner partials, one column
+// (perturbed node m) at a time, divided by d_m, into their slots
+template <int NPE, int NFE, bool RC, bool MZ>
+__global__ void __launch_bounds__(256) k_fd_elem(int T, int N, const int4* __restrict__ en,
+                                                 const double* __restrict__ coef, const double* __restrict__ xyz,
+                                                 const double* __restrict__ eK, int kiso, int estride,
+                                                 const int* __restrict__ ezone, const double* __restrict__ y,
+                                                 const double* __restrict__ shift, const double* __restrict__ krwb,
+                                                 const double* __restrict__ krwp,
+                                                 const unsigned char* __restrict__ upw, double rho0,
+                                                 const int* __restrict__ epos, double* __restrict__ slots) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= T) return;
+    const int4 nd = en[e];
+    const int g[4] = {nd.x, nd.y, nd.z, nd.w};
+    const size_t zo = MZ ? (size_t)ezone[e] * N : 0;
+    double hv[NPE], dl[NPE], kr[NPE], kp[NPE];
+#pragma unroll
+    for (int k = 0; k < NPE; ++k) {
+        hv[k] = y[g[k]];
+        dl[k] = shift[g[k]];
+        kr[k] = krwb[zo + g[k]];
+        kp[k] = krwp[zo + g[k]];
+    }
+    double C[NFE][NPE], G[NFE];
+    if (RC) {
+        double X[4][3];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            X[k][0] = xyz[g[k]];
+            X[k][1] = xyz[(size_t)N + g[k]];
+            X[k][2] = xyz[(size_t)2 * N + g[k]];
+        }
+        double Kx, Ky, Kz;
+        if (kiso) Kx = Ky = Kz = eK[e];
+        else { Kx = eK[e]; Ky = eK[(size_t)estride + e]; Kz = eK[(size_t)2 * estride + e]; }
+        double CC[6][4], GG[6];
+        tet_coefficients_fast(X[0], X[1], X[2], X[3], Kx, Ky, Kz, CC, GG);
+#pragma unroll
+        for (int f = 0; f < NFE; ++f) {
+#pragma unroll
+            for (int k = 0; k < NPE; ++k) C[f][k] = CC[f][k];
+            G[f] = GG[f];
+        }
+    } else {
+#pragma unroll
+        for (int f = 0; f < NFE; ++f) {
+#pragma unroll
+            for (int k = 0; k < NPE; ++k) C[f][k] = coef[(size_t)(f * (NPE + 1) + k) * T + e];
+            G[f] = coef[(size_t)(f * (NPE + 1) + NPE) * T + e];
+        }
+    }
+    const uint2 uw = *reinterpret_cast<const uint2*>(upw + (size_t)8 * e);
+    double q[NFE];
+    unsigned u[NFE];
+#pragma unroll
+    for (int f = 0; f < NFE; ++f) {
+        double s = C[f][0] * hv[0];
+#pragma unroll
+        for (int k = 1; k < NPE; ++k) s += C[f][k] * hv[k];
+        q[f] = s + G[f];
+        u[f] = (f < 4 ? uw.x >> (8 * f) : uw.y >> (8 * (f - 4))) & 0xffu;
+    }
+#pragma unroll
+    for (int m = 0; m < NPE; ++m) {
+        double dc[NPE];
+#pragma unroll
+        for (int k = 0; k < NPE; ++k) dc[k] = 0.0;
+#pragma unroll
+        for (int f = 0; f < NFE; ++f) {
+            const int a = NPE == 4 ? tet_edge_a(f) : tri_edge_a(f);
+            const int b = NPE == 4 ? tet_edge_b(f) : tri_edge_b(f);
+            const double kf = face_krw(u[f], kr[a], kr[b]);
+            const double kfp = face_krw(u[f], a == m ? kp[a] : kr[a], b == m ? kp[b] : kr[b]);
+            const double df = rho0 * (q[f] * (kfp - kf) + (dl[m] * C[f][m]) * kfp);
+            dc[a] -= df;
+            dc[b] += df;
+        }
+        const double inv = 1.0 / dl[m];
+#pragma unroll
+        for (int k = 0; k < NPE; ++k) slots[epos[(size_t)e * NPE * NPE + m * NPE + k]] = dc[k] * inv;
+    }
+}
+
+// per nonzero (i, j): J_ij = (1/V_i) sum of the slots - [i == j] dstor_i / d_i;
+// Dirichlet rows h_D - h differentiate to the quotient of that expression
+__global__ void k_fd_gather(int nnz, const int* __restrict__ rowof, const int* __restrict__ col,
+                            const int* __restrict__ jptr, const double* __restrict__ slots,
+                            const double* __restrict__ invV, const double* __restrict__ dstor,
+                            const unsigned char* __restrict__ ntype, const double* __restrict__ hD,
+                            const double* __restrict__ y, const double* __restrict__ shift,
+                            double* __restrict__ J) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nnz) return;
+    const int i = rowof[q], j = col[q];
+    double v;
+    if (ntype[i]) {
+        v = i == j ? ((hD[i] - (y[i] + shift[i])) - (hD[i] - y[i])) / shift[i] : 0.0;
+    } else {
+        double s = 0.0;
+        const int p1 = jptr[q + 1];
+        for (int p = jptr[q]; p < p1; ++p) s += slots[p];
+        v = s * invV[i];
+        if (i == j) v = v - dstor[i] / shift[i];
+    }
+    J[q] = v;
 }
 
 template <class T>
@@ -164,15 +315,120 @@ __global__ void __launch_bounds__(128) k_ilu_apply(const int* __restrict__ bstar
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) z[i] = (double)x[i - r0];
 }
 
-// Staged variant: the CTA first copies its block's factor (values, local
-// column indices, row pointers, pivot positions) and right-hand side into
-// shared memory with coalesced loads, then runs the level loops entirely in
-// shared memory, so each level costs a few shared-memory latencies and a
-// barrier instead of a dependent chain of L2/HBM loads.
-// Shared layout: x[T nrows] | val[T nnz] | col[u16 nnz] | rp[u16 nrows+1] |
-// dg[u16 nrows]
+// Staged variant: the CTA first brings its block's factor into shared
+// memory, then runs the level loops entirely there, so each level costs a
+// few shared-memory latencies and a barrier instead of a dependent chain of
+// L2/HBM loads.  The block's entries are one contiguous range of the factor
+// arrays; the copy window is that range widened to 8-entry (16-byte)
+// boundaries and moved by two 1D TMA bulk copies (cp.async.bulk, completion
+// counted on an mbarrier, bounded wait), while the threads fill the row
+// pointers, pivot positions, level lists and right-hand side alongside.
+// Shared layout: x[T nrows, 16-B padded] | val[T window] | col[u16 window] |
+// rp[u16 nrows+1] | dg[u16 nrows] | lrow[u16 nrows] | urow[u16 nrows] |
+// lptr[u16 nl+1] | uptr[u16 nu+1] | mbarrier (8-B aligned)
+struct IluWindow {
+    int base, wn;   // first entry of the copy window (multiple of 8), window length
+};
+__device__ __forceinline__ IluWindow ilu_window(int e0, int e1) {
+    IluWindow w;
+    w.base = e0 & ~7;
+    w.wn = ((e1 + 7) & ~7) - w.base;
+    return w;
+}
+__host__ __device__ __forceinline__ size_t round16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+// shared bytes of the staged kernels for one block (host and device agree);
+// nlev = nl + 1 + nu + 1 level offsets of the two sweeps
+__host__ __device__ __forceinline__ size_t ilu_stage_bytes(size_t nr, size_t wn, size_t nlev, size_t sz) {
+    return round16(round16(nr * sz) + wn * (sz + 2) + (4 * nr + 1 + nlev) * 2) + 16;
+}
+
 template <class T>
-__global__ void __launch_bounds__(256) k_ilu_apply_smem(const int* __restrict__ bstart,
+__device__ __forceinline__ void ilu_stage_bulk(T* val, unsigned short* col, const T* lu,
+                                               const unsigned short* lu_col, IluWindow w, uint64_t* bar) {
+    if (threadIdx.x == 0) {
+        uint32_t b = tc05::smem_u32(bar);
+        uint32_t bytes = (uint32_t)(w.wn * (sizeof(T) + sizeof(unsigned short)));
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes));
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         tc05::smem_u32(val)),
+                     "l"(lu + w.base), "r"((uint32_t)(w.wn * sizeof(T))), "r"(b)
+                     : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         tc05::smem_u32(col)),
+                     "l"(lu_col + w.base), "r"((uint32_t)(w.wn * sizeof(unsigned short))), "r"(b)
+                     : "memory");
+    }
+}
+
+// One triangular sweep over the levels [l0, nlv): rows of a level are
+// independent, one thread per row.  UPPER: x_i = (x_i - sum_{p>diag}) *
+// inverse pivot; else x_i = x_i - sum_{p<diag} (unit lower triangle).  A
+// thread's row of level l+1 -- its index, range, first KM entries and pivot,
+// none of which depend on x -- is fetched while level l is computed, so after
+// each barrier only the x loads (independent of each other) and the
+// accumulation remain on the critical path.
+template <class T, int KM, bool UPPER> struct IluRow {
+    int li, p0, p1;
+    T v[KM];
+    unsigned short c[KM];
+    T piv;
+};
+
+template <class T, int KM, bool UPPER>
+__device__ __forceinline__ void ilu_fetch(IluRow<T, KM, UPPER>& R, int l, int nlv, const T* val,
+                                          const unsigned short* col, const unsigned short* rp,
+                                          const unsigned short* dg, const unsigned short* rows,
+                                          const unsigned short* lptr) {
+    R.li = -1;
+    if (l >= nlv) return;
+    const int q = lptr[l] + threadIdx.x;
+    if (q >= lptr[l + 1]) return;
+    R.li = rows[q];
+    const int d = dg[R.li];
+    R.p0 = UPPER ? d + 1 : rp[R.li];
+    R.p1 = UPPER ? rp[R.li + 1] : d;
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+        const int p = R.p0 + k < R.p1 ? R.p0 + k : 0;   // unused slots read entry 0
+        R.v[k] = val[p];
+        R.c[k] = col[p];
+    }
+    R.piv = UPPER ? val[d] : (T)1;
+}
+
+template <class T, int KM, bool UPPER>
+__device__ __forceinline__ void ilu_sweep(T* x, const T* val, const unsigned short* col, const unsigned short* rp,
+                                          const unsigned short* dg, const unsigned short* rows,
+                                          const unsigned short* lptr, int l0, int nlv) {
+    IluRow<T, KM, UPPER> cur, nxt;
+    ilu_fetch(cur, l0, nlv, val, col, rp, dg, rows, lptr);
+    for (int l = l0; l < nlv; ++l) {
+        ilu_fetch(nxt, l + 1, nlv, val, col, rp, dg, rows, lptr);
+        if (cur.li >= 0) {
+            T acc = (T)0;
+#pragma unroll
+            for (int k = 0; k < KM; ++k)
+                if (cur.p0 + k < cur.p1) acc += cur.v[k] * x[cur.c[k]];
+            for (int p = cur.p0 + KM; p < cur.p1; ++p) acc += val[p] * x[col[p]];
+            x[cur.li] = UPPER ? (x[cur.li] - acc) * cur.piv : x[cur.li] - acc;
+        }
+        // rows of a level wider than the CTA
+        for (int q = lptr[l] + threadIdx.x + blockDim.x; q < lptr[l + 1]; q += blockDim.x) {
+            const int li = rows[q];
+            const int d = dg[li];
+            const int p0 = UPPER ? d + 1 : rp[li], p1 = UPPER ? rp[li + 1] : d;
+            T acc = (T)0;
+            for (int p = p0; p < p1; ++p) acc += val[p] * x[col[p]];
+            x[li] = UPPER ? (x[li] - acc) * val[d] : x[li] - acc;
+        }
+        __syncthreads();
+        cur = nxt;
+    }
+}
+
+template <class T, int KM>
+__global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __restrict__ bstart,
                                                         const int* __restrict__ lu_ptr,
                                                         const int* __restrict__ lu_diag,
                                                         const unsigned short* __restrict__ lu_col,
@@ -184,46 +440,118 @@ __global__ void __launch_bounds__(256) k_ilu_apply_smem(const int* __restrict__ 
                                                         const int* __restrict__ blk_ulvl,
                                                         const T* __restrict__ lu,
                                                         const double* __restrict__ r,
-                                                        double* __restrict__ z) {
+                                                        double* __restrict__ z, int* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int b = blockIdx.x;
     const int r0 = bstart[b], r1 = bstart[b + 1], nr = r1 - r0;
-    const int e0 = lu_ptr[r0], nnz = lu_ptr[r1] - e0;
+    const IluWindow w = ilu_window(lu_ptr[r0], lu_ptr[r1]);
+    const int la = blk_lvl[b], nl = blk_lvl[b + 1] - la;
+    const int ua = blk_ulvl[b], nu = blk_ulvl[b + 1] - ua;
     T* x = reinterpret_cast<T*>(smem_raw);
-    T* val = x + nr;
-    unsigned short* col = reinterpret_cast<unsigned short*>(val + nnz);
-    unsigned short* rp = col + nnz;
+    T* val = reinterpret_cast<T*>(smem_raw + round16(sizeof(T) * nr));
+    unsigned short* col = reinterpret_cast<unsigned short*>(val + w.wn);
+    unsigned short* rp = col + w.wn;
     unsigned short* dg = rp + nr + 1;
-    for (int q = threadIdx.x; q < nnz; q += blockDim.x) {
-        val[q] = lu[e0 + q];
-        col[q] = lu_col[e0 + q];
-    }
-    for (int i = threadIdx.x; i <= nr; i += blockDim.x) rp[i] = (unsigned short)(lu_ptr[r0 + i] - e0);
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
-        dg[i] = (unsigned short)(lu_diag[r0 + i] - e0);
-        x[i] = (T)r[r0 + i];
+    unsigned short* lrow = dg + nr;
+    unsigned short* urow = lrow + nr;
+    unsigned short* lptr = urow + nr;
+    unsigned short* uptr = lptr + nl + 1;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + ilu_stage_bytes(nr, w.wn, nl + nu + 2, sizeof(T)) - 16);
+    if (threadIdx.x == 0) {
+        tc05::mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;");
     }
     __syncthreads();
-    for (int l = blk_lvl[b] + 1; l < blk_lvl[b + 1]; ++l) {
-        for (int q = lvl_ptr[l] + threadIdx.x; q < lvl_ptr[l + 1]; q += blockDim.x) {
-            int li = lvl_rows[q] - r0;
-            T acc = x[li];
-            for (int p = rp[li]; p < dg[li]; ++p) acc -= val[p] * x[col[p]];
-            x[li] = acc;
-        }
-        __syncthreads();
+    ilu_stage_bulk(val, col, lu, lu_col, w, bar);
+    // a block's rows appear once in each level-ordered list, at [r0, r1)
+    for (int i = threadIdx.x; i <= nr; i += blockDim.x) rp[i] = (unsigned short)(lu_ptr[r0 + i] - w.base);
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+        dg[i] = (unsigned short)(lu_diag[r0 + i] - w.base);
+        x[i] = (T)r[r0 + i];
+        lrow[i] = (unsigned short)(lvl_rows[r0 + i] - r0);
+        urow[i] = (unsigned short)(ulvl_rows[r0 + i] - r0);
     }
-    for (int l = blk_ulvl[b]; l < blk_ulvl[b + 1]; ++l) {
-        for (int q = ulvl_ptr[l] + threadIdx.x; q < ulvl_ptr[l + 1]; q += blockDim.x) {
-            int li = ulvl_rows[q] - r0;
-            int d = dg[li];
-            T acc = x[li];
-            for (int p = d + 1; p < rp[li + 1]; ++p) acc -= val[p] * x[col[p]];
-            x[li] = acc * val[d];
-        }
-        __syncthreads();
+    for (int l = threadIdx.x; l <= nl; l += blockDim.x) lptr[l] = (unsigned short)(lvl_ptr[la + l] - r0);
+    for (int l = threadIdx.x; l <= nu; l += blockDim.x) uptr[l] = (unsigned short)(ulvl_ptr[ua + l] - r0);
+    bool ok = tc05::mbar_wait(bar, 0);
+    if (!ok) ok = tc05::mbar_wait(bar, 0);   // copies in flight get a second bounded chance
+    if (!__syncthreads_and(ok ? 1 : 0)) {
+        // the factor never arrived: report it and pass the vector through
+        // unpreconditioned instead of reading unfilled shared memory
+        if (threadIdx.x == 0) atomicExch(err, 2);
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) z[r0 + i] = r[r0 + i];
+        return;
     }
+    // level 0 of the lower sweep has no off-diagonal entries
+    ilu_sweep<T, KM, false>(x, val, col, rp, dg, lrow, lptr, 1, nl);
+    ilu_sweep<T, KM, true>(x, val, col, rp, dg, urow, uptr, 0, nu);
     for (int i = threadIdx.x; i < nr; i += blockDim.x) z[r0 + i] = (double)x[i];
+}
+
+// Shared-memory factorisation: gather the block's Jacobian entries into the
+// same copy window the apply uses, eliminate level by level in shared
+// memory (IKJ, pivots inverted after their row), write the block back.
+template <class T>
+__global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__ bstart,
+                                                         const int* __restrict__ lu_ptr,
+                                                         const int* __restrict__ lu_src,
+                                                         const int* __restrict__ lu_diag,
+                                                         const unsigned short* __restrict__ lu_col,
+                                                         const int* __restrict__ lvl_ptr,
+                                                         const int* __restrict__ lvl_rows,
+                                                         const int* __restrict__ blk_lvl,
+                                                         const double* __restrict__ J, T* __restrict__ lu,
+                                                         int* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int b = blockIdx.x;
+    const int r0 = bstart[b], r1 = bstart[b + 1], nr = r1 - r0;
+    const int e0 = lu_ptr[r0], e1 = lu_ptr[r1];
+    const IluWindow w = ilu_window(e0, e1);
+    T* val = reinterpret_cast<T*>(smem_raw + round16(sizeof(T) * nr));
+    unsigned short* col = reinterpret_cast<unsigned short*>(val + w.wn);
+    unsigned short* rp = col + w.wn;
+    unsigned short* dg = rp + nr + 1;
+    unsigned short* lrow = dg + nr;
+    unsigned short* lptr = lrow + 2 * nr;
+    const int la = blk_lvl[b], nl = blk_lvl[b + 1] - la;
+    const int lq0 = lvl_ptr[la];
+#pragma unroll 4
+    for (int p = e0 + threadIdx.x; p < e1; p += blockDim.x) {
+        val[p - w.base] = (T)J[lu_src[p]];
+        col[p - w.base] = lu_col[p];
+    }
+    for (int i = threadIdx.x; i <= nr; i += blockDim.x) rp[i] = (unsigned short)(lu_ptr[r0 + i] - w.base);
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+        dg[i] = (unsigned short)(lu_diag[r0 + i] - w.base);
+        lrow[i] = (unsigned short)(lvl_rows[lq0 + i] - r0);
+    }
+    for (int l = threadIdx.x; l <= nl; l += blockDim.x) lptr[l] = (unsigned short)(lvl_ptr[la + l] - lq0);
+    __syncthreads();
+    for (int l = 0; l < nl; ++l) {
+        for (int q = lptr[l] + threadIdx.x; q < lptr[l + 1]; q += blockDim.x) {
+            int li = lrow[q];
+            int s0 = rp[li], s1 = rp[li + 1], di = dg[li];
+            for (int kk = s0; kk < di; ++kk) {
+                int k = col[kk];
+                T lik = val[kk] * val[dg[k]];
+                val[kk] = lik;
+                int kpos = dg[k] + 1, kend = rp[k + 1];
+                for (int jj = kk + 1; jj < s1 && kpos < kend; ++jj) {
+                    int j = col[jj];
+                    while (kpos < kend && col[kpos] < j) ++kpos;
+                    if (kpos < kend && col[kpos] == j) val[jj] = val[jj] - lik * val[kpos];
+                }
+            }
+            T d = val[di];
+            if (d == (T)0 || !isfinite((double)d)) {
+                atomicExch(status, 1);
+                d = (T)1;
+            }
+            val[di] = (T)1 / d;
+        }
+        __syncthreads();
+    }
+    for (int p = e0 + threadIdx.x; p < e1; p += blockDim.x) lu[p] = val[p - w.base];
 }
 
 // ------------------------------------------------------------------ host set-up
@@ -276,23 +604,39 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
         P->h_colour[i] = cc;
     }
     P->ncol = maxc;
-    // nnz grouped by the colour of their column
-    P->h_cptr.assign(maxc + 1, 0);
-    for (int p = 0; p < P->nnz; ++p) P->h_cptr[P->h_colour[cl[p]] + 1]++;
-    for (int k = 0; k < maxc; ++k) P->h_cptr[k + 1] += P->h_cptr[k];
-    std::vector<int> cnnz(P->nnz), rowof(P->nnz);
-    {
-        std::vector<int> pos(P->h_cptr.begin(), P->h_cptr.end() - 1);
-        for (int i = 0; i < N; ++i)
-            for (int p = rp[i]; p < rp[i + 1]; ++p) {
-                rowof[p] = i;
-                cnnz[pos[P->h_colour[cl[p]]]++] = p;
+    std::vector<int> rowof(P->nnz);
+    for (int i = 0; i < N; ++i)
+        for (int p = rp[i]; p < rp[i + 1]; ++p) rowof[p] = i;
+    // element-wise difference quotients: slot of (element e, perturbed node
+    // m, corner k) -> nonzero (node of k, node of m); slots of one nonzero
+    // are contiguous and in ascending element order
+    const int npe2 = npe * npe;
+    std::vector<int> fd_q((size_t)T * npe2), fd_jptr(P->nnz + 1, 0), fd_epos((size_t)T * npe2);
+    for (int e = 0; e < T; ++e) {
+        const int* v = &c->h_elem_nodes[(size_t)e * npe];
+        for (int m = 0; m < npe; ++m)
+            for (int k = 0; k < npe; ++k) {
+                const int i = v[k], j = v[m];
+                const int* b = &cl[rp[i]];
+                const int* f = std::lower_bound(b, &cl[0] + rp[i + 1], j);
+                const int q = (int)(f - &cl[0]);
+                fd_q[(size_t)e * npe2 + m * npe + k] = q;
+                fd_jptr[q + 1]++;
             }
     }
-    // blocks of contiguous nodes; 148 SMs -> block counts in multiples of 148
+    for (int q = 0; q < P->nnz; ++q) fd_jptr[q + 1] += fd_jptr[q];
+    {
+        std::vector<int> fill(fd_jptr.begin(), fd_jptr.end() - 1);
+        for (size_t t = 0; t < fd_q.size(); ++t) fd_epos[t] = fill[fd_q[t]]++;
+    }
+    // blocks of contiguous nodes; on a large mesh a multiple of the SM count
+    // (c->ilu_per_sm blocks per SM: fewer, larger blocks precondition better,
+    // more, smaller ones have shorter level chains and share an SM)
+    int nsm = 148;
+    FVM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
     int target = 1500;
     int nb;
-    if (N >= 148 * 256) nb = 148 * std::max(1, (int)std::lround((double)N / (148.0 * target)));
+    if (N >= nsm * 256) nb = nsm * std::max(1, c->ilu_per_sm);
     else nb = std::max(1, (N + target - 1) / target);
     nb = std::min(nb, N);
     std::vector<int> bstart(nb + 1);
@@ -353,30 +697,54 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
         bool fits16 = true;
         for (int b = 0; b < nb; ++b) {
             size_t nr = bstart[b + 1] - bstart[b];
-            size_t nz = lu_ptr[bstart[b + 1]] - lu_ptr[bstart[b]];
-            if (nz >= 65535 || nr + 1 >= 65535) fits16 = false;
-            need64 = std::max(need64, nr * 8 + nz * 8 + nz * 2 + (nr + 1) * 2 + nr * 2);
-            need32 = std::max(need32, nr * 4 + nz * 4 + nz * 2 + (nr + 1) * 2 + nr * 2);
+            // the 16-byte aligned copy window of ilu_window()
+            size_t wn = (size_t)(((lu_ptr[bstart[b + 1]] + 7) & ~7) - (lu_ptr[bstart[b]] & ~7));
+            if (wn >= 65535 || nr + 1 >= 65535) fits16 = false;
+            size_t nlev = (size_t)(blk_lvl[b + 1] - blk_lvl[b]) + (size_t)(blk_ulvl[b + 1] - blk_ulvl[b]) + 2;
+            for (size_t sz : {(size_t)8, (size_t)4}) {
+                size_t need = ilu_stage_bytes(nr, wn, nlev, sz);
+                if (sz == 8) need64 = std::max(need64, need);
+                else need32 = std::max(need32, need);
+            }
         }
         P->smem_stage[0] = (fits16 && need64 <= kMaxDynSmem) ? need64 : 0;
         P->smem_stage[1] = (fits16 && need32 <= kMaxDynSmem) ? need32 : 0;
-        if (P->smem_stage[0])
-            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        // entries per row held in registers by the staged triangular sweeps:
+        // 8 covers the lower or upper part of a 3D row, 4 of a 2D row
+        P->lanes = (double)lu_ptr[N] / N > 9.0 ? 8 : 4;
+        if (P->smem_stage[0]) {
+            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)P->smem_stage[0]));
-        if (P->smem_stage[1])
-            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)P->smem_stage[0]));
+            FVM_CUDA(cudaFuncSetAttribute(k_ilu_factor_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)P->smem_stage[0]));
+        }
+        if (P->smem_stage[1]) {
+            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)P->smem_stage[1]));
+            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)P->smem_stage[1]));
+            FVM_CUDA(cudaFuncSetAttribute(k_ilu_factor_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)P->smem_stage[1]));
+        }
     }
     cudaStream_t s = c->stream;
     P->col.upload(P->h_col, s);
     P->rowof.upload(rowof, s);
     P->J.alloc(P->nnz);
-    P->colour.upload(P->h_colour, s);
-    P->cnnz.upload(cnnz, s);
     P->shift.alloc(N);
-    P->Fc.alloc(N);
+    P->fd_epos.upload(fd_epos, s);
+    P->fd_jptr.upload(fd_jptr, s);
+    P->fd_slots.alloc(fd_epos.size());
+    P->krwb.alloc((size_t)c->nz * N);
+    P->krwp.alloc((size_t)c->nz * N);
+    P->dstor.alloc(N);
     P->bstart.upload(bstart, s);
     P->lu_ptr.upload(lu_ptr, s);
+    // 8 padding entries so every block's widened copy window stays inside
+    lu_src.resize(lu_src.size() + 8, 0);
+    lu_col.resize(lu_col.size() + 8, 0);
     P->lu_src.upload(lu_src, s);
     P->lu_diag.upload(lu_diag, s);
     P->lu_col.upload(lu_col, s);
@@ -401,25 +769,45 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     cudaStream_t s = c->stream;
     const int N = c->N;
     c->tm.begin(TM_FD_JAC, s);
+    (void)F0;   // the element-wise quotients difference each element's own partials
     fvm_launch(c, k_shift, grid_for(N, 256), 256, 0, s, N, y, yp, ewt, h, std::sqrt(DBL_EPSILON), P->shift.p);
-    for (int col = 0; col < P->ncol; ++col) {
-        Perturb pt;
-        pt.mode = 2;
-        pt.cj = cj;
-        pt.shift = P->shift.p;
-        pt.colour = P->colour.p;
-        pt.c = col;
-        launch_residual(c, y, yp, pt, nullptr, P->Fc.p);
-        int cnt = P->h_cptr[col + 1] - P->h_cptr[col];
-        if (cnt > 0)
-            fvm_launch(c, k_fd_scatter, grid_for(cnt, 256), 256, 0, s, cnt, P->cnnz.p + P->h_cptr[col], P->rowof.p,
-                                                            P->col.p, P->Fc.p, F0, P->shift.p, P->J.p);
+    fvm_launch(c, k_fd_node, grid_for(N, 256), 256, 0, s, N, y, yp, cj, P->shift.p, c->zones.p, c->nz, c->nz_ptr.p,
+               c->nz_zone.p, c->nz_w.p, c->rho0, P->krwb.p, P->krwp.p, P->dstor.p);
+    {
+        const int gb = grid_for(c->T, 256);
+        const bool mz = c->nz > 1;
+        auto go = [&](auto kern) {
+            fvm_launch(c, kern, gb, 256, 0, s, c->T, N, c->enodes.p, c->coef.p, c->xyz.p, c->eK.p, c->kiso ? 1 : 0,
+                       c->estride, c->ezone.p, y, P->shift.p, P->krwb.p, P->krwp.p, c->upw.p, c->rho0, P->fd_epos.p,
+                       P->fd_slots.p);
+        };
+        if (c->dim == 3) {
+            if (c->recompute) mz ? go(k_fd_elem<4, 6, true, true>) : go(k_fd_elem<4, 6, true, false>);
+            else mz ? go(k_fd_elem<4, 6, false, true>) : go(k_fd_elem<4, 6, false, false>);
+        } else {
+            mz ? go(k_fd_elem<3, 3, false, true>) : go(k_fd_elem<3, 3, false, false>);
+        }
     }
+    fvm_launch(c, k_fd_gather, grid_for(P->nnz, 256), 256, 0, s, P->nnz, P->rowof.p, P->col.p, P->fd_jptr.p,
+               P->fd_slots.p, c->invV.p, P->dstor.p, c->ntype.p, c->hD.p, y, P->shift.p, P->J.p);
     c->tm.end(TM_FD_JAC, s);
     FVM_CUDA(cudaMemsetAsync(P->status.p, 0, sizeof(int), s));
     size_t nlu = P->lu_src.n;
     c->tm.begin(TM_ILU_FACTOR, s);
-    if (precision) {
+    if (P->smem_stage[precision]) {
+        size_t sm = P->smem_stage[precision];
+        if (precision) {
+            P->lu32.alloc(nlu);
+            fvm_launch(c, k_ilu_factor_smem<float>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p,
+                       P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->J.p, P->lu32.p,
+                       P->status.p);
+        } else {
+            P->lu64.alloc(nlu);
+            fvm_launch(c, k_ilu_factor_smem<double>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p,
+                       P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->J.p, P->lu64.p,
+                       P->status.p);
+        }
+    } else if (precision) {
         P->lu32.alloc(nlu);
         fvm_launch(c, k_ilu_factor<float>, P->nb, 128, 0, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p, P->lu_diag.p, P->lu_col.p,
                                                   P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->J.p, P->lu32.p,
@@ -454,14 +842,18 @@ void psolve_dev(fvm_ctx* c, const double* r, double* z) {
     } end_timer{c};
     if (P->smem_stage[P->factored]) {
         size_t sm = P->smem_stage[P->factored];
-        if (P->factored)
-            fvm_launch(c, k_ilu_apply_smem<float>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p,
-                                                          P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p,
-                                                          P->ulvl_rows.p, P->blk_ulvl.p, P->lu32.p, r, z);
-        else
-            fvm_launch(c, k_ilu_apply_smem<double>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p,
-                                                           P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p,
-                                                           P->ulvl_rows.p, P->blk_ulvl.p, P->lu64.p, r, z);
+        auto go = [&](auto kern, const auto* lu) {
+            fvm_launch(c, kern, P->nb, kIluThreads, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p,
+                       P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p, P->ulvl_rows.p, P->blk_ulvl.p, lu,
+                       r, z, P->status.p);
+        };
+        if (P->factored) {
+            if (P->lanes == 8) go(k_ilu_apply_smem<float, 8>, P->lu32.p);
+            else go(k_ilu_apply_smem<float, 4>, P->lu32.p);
+        } else {
+            if (P->lanes == 8) go(k_ilu_apply_smem<double, 8>, P->lu64.p);
+            else go(k_ilu_apply_smem<double, 4>, P->lu64.p);
+        }
     } else if (P->factored) {
         size_t sm = sizeof(float) * P->maxb;
         fvm_launch(c, k_ilu_apply<float>, P->nb, 128, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
@@ -509,6 +901,26 @@ extern "C" int fvm_psolve(fvm_ctx* c, const double* r, double* z) {
         psolve_dev(c, r, z);
         FVM_CUDA(cudaGetLastError());
         FVM_CUDA(cudaStreamSynchronize(c->stream));
+        return 0;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+extern "C" int fvm_set_precond_blocks(fvm_ctx* c, int per_sm) {
+    try {
+        if (!c) throw Error("fvm_set_precond_blocks: null context");
+        if (per_sm < 1 || per_sm > 16) throw Error("fvm_set_precond_blocks: blocks per SM must be in [1, 16]");
+        FVM_CUDA(cudaStreamSynchronize(c->stream));
+        c->ilu_per_sm = per_sm;
+        if (c->ilu) {
+            fvmb_destroy_ilu(c->ilu);
+            c->ilu = nullptr;
+        }
         return 0;
     } catch (const Error& ex) {
         set_error(ex.what());

@@ -522,14 +522,41 @@ __global__ void k_apply_guess(int N, const float* __restrict__ out, const double
     ypg[i] = yppred[i] + cj * d;
 }
 
-__global__ void k_take_guess(int N, const double* __restrict__ yg, const double* __restrict__ ypg,
-                             const double* __restrict__ ypred, double* __restrict__ y, double* __restrict__ yp,
-                             double* __restrict__ e) {
+// y = y_pred + a (y_guess - y_pred), y' likewise; e = y - y_pred
+__global__ void k_take_guess(int N, double a, const double* __restrict__ yg, const double* __restrict__ ypg,
+                             const double* __restrict__ ypred, const double* __restrict__ yppred,
+                             double* __restrict__ y, double* __restrict__ yp, double* __restrict__ e) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    y[i] = yg[i];
-    yp[i] = ypg[i];
-    e[i] = yg[i] - ypred[i];
+    const double d = a == 1.0 ? yg[i] - ypred[i] : a * (yg[i] - ypred[i]);
+    y[i] = a == 1.0 ? yg[i] : ypred[i] + d;
+    yp[i] = a == 1.0 ? ypg[i] : yppred[i] + a * (ypg[i] - yppred[i]);
+    e[i] = d;
+}
+
+// out = (F0.F0, F0.F1, F1.F1), fixed-order reduction
+__global__ void k_dot3(int N, const double* __restrict__ F0, const double* __restrict__ F1, double* partial,
+                       unsigned* counter, double* out) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        const double a = F0[k], b = F1[k];
+        s0 += a * a;
+        s1 += a * b;
+        s2 += b * b;
+    }
+    __shared__ double red[3][32];
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (lane == 0) { red[0][w] = s0; red[1][w] = s1; red[2][w] = s2; }
+    __syncthreads();
+    if (w < 3) {
+        double t = lane < nw ? red[w][lane] : 0.0;
+        t = warp_sum(t);
+        if (lane == 0) partial[(size_t)blockIdx.x * 3 + w] = t;
+    }
+    last_block_reduce(partial, 3, counter, out);
 }
 
 __global__ void k_record(int N, int stride, int offset, const float* __restrict__ Xall,
@@ -605,14 +632,29 @@ bool predictor_apply(fvm_ctx* c, Predictor* p, double rtol, double atol, double 
     Perturb none;
     launch_residual(c, p->yg.p, p->ypg.p, none, nullptr, p->Fg.p);
     launch_residual(c, ypred, yppred, none, nullptr, F);
-    double r_guess = reduce_sumsq(c, p->Fg.p, nullptr);
-    double r_pred = reduce_sumsq(c, F, nullptr);
-    if (std::isfinite(r_guess) && r_guess < r_pred) {
-        fvm_launch(c, k_take_guess, grid_for(N, 256), 256, 0, c->stream, N, p->yg.p, p->ypg.p, ypred, y, yp, e);
-        FVM_CUDA(cudaMemcpyAsync(F, p->Fg.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
-        return true;
-    }
-    return false;
+    // The residual is close to linear over one Newton correction, so along
+    // y(a) = y_pred + a (y_guess - y_pred) its squared norm is the quadratic
+    // through F0 = F(y_pred) and F1 = F(y_guess):
+    //   |F(a)|^2 ~ A + 2a (B - A) + a^2 (A - 2B + C),  A = F0.F0, B = F0.F1, C = F1.F1.
+    // Take its minimiser on [0, 1]; keep the BDF predictor when the learned
+    // direction does not lower the residual.
+    Krylov* K = krylov_get(c, c->kry ? c->kry->m : 1, c->kry ? c->kry->precision : 0);
+    fvm_launch(c, k_dot3, kRedBlocks, kRedThreads, 0, c->stream, N, F, p->Fg.p, K->partial.p, K->counter.p,
+               K->res.p);
+    FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    const double A = K->host[0], B = K->host[1], Cc = K->host[2];
+    const double curv = A - 2.0 * B + Cc;   // |F1 - F0|^2
+    if (!std::isfinite(A) || !std::isfinite(Cc) || !(curv > 0.0)) return false;
+    double a = (A - B) / curv;
+    a = std::min(1.0, a);
+    const double pred = A + 2.0 * a * (B - A) + a * a * curv;
+    if (!(a > 0.05) || !(pred < 0.98 * A)) return false;
+    fvm_launch(c, k_take_guess, grid_for(N, 256), 256, 0, c->stream, N, a, p->yg.p, p->ypg.p, ypred, yppred, y, yp,
+               e);
+    if (a == 1.0) FVM_CUDA(cudaMemcpyAsync(F, p->Fg.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+    else launch_residual(c, y, yp, none, nullptr, F);
+    return true;
 }
 
 void recorder_push(fvm_ctx* c, Recorder* r, const float* Xall, const double* y_new, const double* ypred,

@@ -39,9 +39,11 @@ void predictor_features(fvm_ctx* c, const double* h_n, const double* h_prev, con
 void predictor_forward(fvm_ctx* c, Predictor* p, const float* X, int n, float* out);
 
 // Replaces the Newton starting point (y, y', e) with the network's guess
-// y_pred + w * MLP when its residual norm is below the BDF predictor's.
-// ypred/yppred hold the BDF predictor; F receives the residual of the kept
-// iterate.  Returns true when the learned iterate was kept.
+// y_pred + a w MLP, a in (0, 1] the minimiser of the residual norm along
+// the learned direction (linearised from the residuals at both ends), when
+// that lowers the BDF predictor's residual.  ypred/yppred hold the BDF
+// predictor; F receives the residual of the kept iterate.  Returns true when
+// the learned iterate was kept.
 bool predictor_apply(fvm_ctx* c, Predictor* p, double rtol, double atol, double dt, double cj,
                      const double* h_n, const double* h_prev, const double* ypred,
                      const double* yppred, double* y, double* yp, double* e, double* F);

@@ -88,11 +88,27 @@ typedef struct {
     double rho0;             /* Constants::rho_0 (definitions.h:301-326)   */
 } fvm_physics;
 
-/* flags for fvm_create */
-#define FVM_FLAG_RECOMPUTE_GEOMETRY 1  /* face geometry rebuilt per launch
-                                          instead of streamed from HBM     */
-#define FVM_FLAG_AUTOTUNE           2  /* time both residual variants and
-                                          keep the faster one              */
+/* flags for fvm_create.  The element pass of the residual has two
+ * variants: stored face coefficients streamed from HBM (240 B per
+ * tetrahedron) or the face geometry rebuilt from the vertices on every
+ * launch (3D only, the 3D default). */
+#define FVM_FLAG_RECOMPUTE_GEOMETRY 1  /* rebuilt geometry (3D)            */
+#define FVM_FLAG_AUTOTUNE           2  /* time every element-pass variant
+                                          and chunk size on this mesh at
+                                          creation and keep the fastest    */
+#define FVM_FLAG_STORED_GEOMETRY    4  /* stored coefficients in 3D too    */
+
+/* Autotuner report: candidate i ran `variant[i]` (0 stored, 1 rebuilt
+ * geometry) with `chunk[i]` elements per CTA in `us[i]` microseconds (median
+ * element-pass time, L2 flushed before every launch); `best` indexes the
+ * candidate kept. */
+#define FVM_TUNE_MAX 16
+typedef struct {
+    int n, best;
+    int variant[FVM_TUNE_MAX];
+    int chunk[FVM_TUNE_MAX];
+    double us[FVM_TUNE_MAX];
+} fvm_tune_result;
 
 typedef struct fvm_ctx fvm_ctx;
 
@@ -204,6 +220,26 @@ int fvm_profile_read(fvm_ctx* ctx, double* ms, long* counts);
 long fvm_wrms_noalloc_max_n(void);
 int fvm_wrms_noalloc(const double* x, const double* ewt, long n,
                      double* result, void* stream);
+
+/* Element-pass tuning.  The residual's element pass runs over chunks of
+ * consecutive elements, one CTA per chunk, with the chunk's nodes staged in
+ * shared memory; the chunk size and the geometry variant (see the flags
+ * above) set its speed, not its result beyond rounding.  fvm_autotune times
+ * every candidate on this context's mesh and keeps the fastest (out may be
+ * NULL); fvm_set_element_pass selects one explicitly (chunk: 32..2048
+ * elements, bounded by shared memory); fvm_element_pass reports the
+ * current choice.  No counterpart in the reference, whose residual is a
+ * fixed sequence of cuSPARSE SpMVs (fvmpor.h:948-1124). */
+int fvm_autotune(fvm_ctx* ctx, fvm_tune_result* out);
+/* Block-ILU partition on large meshes: per_sm (1..16) blocks per SM.  Fewer,
+ * larger blocks couple more nodes inside the factor (fewer Krylov
+ * iterations); more, smaller ones shorten the level chains of the
+ * triangular solves and let several blocks share an SM.  Drops the current
+ * factor; the next fvm_psetup rebuilds the pattern.  The reference's
+ * preconditioner is one direct factorisation (preconditioner_dss.cpp:284-405). */
+int fvm_set_precond_blocks(fvm_ctx* ctx, int per_sm);
+int fvm_set_element_pass(fvm_ctx* ctx, int variant, int chunk);
+int fvm_element_pass(const fvm_ctx* ctx, int* variant, int* chunk);
 
 /* Running totals since fvm_create: kernels launched by the library on this
  * context and residual evaluations (the Physics::calls() counter,

@@ -54,10 +54,10 @@ def case(request):
     return request.param, PROBLEMS[request.param]()
 
 
-@pytest.mark.parametrize("flags", [0, fb.FLAG_RECOMPUTE_GEOMETRY])
+@pytest.mark.parametrize("flags", [fb.FLAG_STORED_GEOMETRY, fb.FLAG_RECOMPUTE_GEOMETRY])
 def test_residual_parity(case, flags, cuda):
     name, p = case
-    if flags and p.mesh.dim == 2:
+    if flags == fb.FLAG_RECOMPUTE_GEOMETRY and p.mesh.dim == 2:
         pytest.skip("geometry recompute is a 3D variant")
     ph = fb.Physics(p, flags)
     orc = Oracle(p)
@@ -68,6 +68,40 @@ def test_residual_parity(case, flags, cuda):
         ref = orc.residual(0.0, y, yp)
         err = np.abs(res.cpu().numpy() - ref) / row_scale(orc, p, y, yp)
         assert err.max() < 1e-11, (name, seed, err.max())
+
+
+def test_element_pass_chunks_and_autotune(case, cuda):
+    """every chunk size and geometry variant gives the oracle's residual;
+    each is bitwise reproducible run to run; the autotuner keeps one"""
+    name, p = case
+    ph = fb.Physics(p)
+    orc = Oracle(p)
+    y, yp = state(p, 4)
+    ref = orc.residual(0.0, y, yp)
+    scale = row_scale(orc, p, y, yp)
+    res = torch.empty(p.n_nodes, dtype=torch.float64, device=cuda)
+    variants = (0, 1) if p.mesh.dim == 3 else (0,)
+    for v in variants:
+        for ch in (64, 200, 512, 1024):
+            ph.set_element_pass(v, ch)
+            assert ph.element_pass() == (v, ch)
+            ph.residual(0.0, T(y, cuda), T(yp, cuda), res)
+            a = res.cpu().numpy()
+            ph.residual(0.0, T(y, cuda), T(yp, cuda), res)
+            assert np.array_equal(a, res.cpu().numpy()), (name, v, ch)
+            err = np.abs(a - ref) / scale
+            assert err.max() < 1e-11, (name, v, ch, err.max())
+    if p.mesh.dim == 2:
+        with pytest.raises(fb.FvmError):
+            ph.set_element_pass(1, 256)
+    with pytest.raises(fb.FvmError):
+        ph.set_element_pass(0, 40000)
+    table, best = ph.autotune()
+    assert len(table) >= 4 and 0 <= best < len(table)
+    assert ph.element_pass() == (table[best][0], table[best][1])
+    assert all(t[2] > 0 for t in table)
+    ph.residual(0.0, T(y, cuda), T(yp, cuda), res)
+    assert (np.abs(res.cpu().numpy() - ref) / scale).max() < 1e-11
 
 
 def test_initial_head_matches_rules(case, cuda):
@@ -191,6 +225,35 @@ def test_psolve_parity_on_identical_matrix(case, precision, cuda):
     tol = 1e-10 if precision == 0 else 2e-4
     err = np.abs(z.cpu().numpy() - ref).max() / np.abs(ref).max()
     assert err < tol, (name, precision, err)
+
+
+@pytest.mark.parametrize("per_sm", [1, 2, 4])
+def test_psolve_parity_blocks_per_sm(per_sm, cuda):
+    """large-mesh block partitions (a multiple of the SM count, per_sm
+    blocks per SM) against the oracle's ILU(0) on the same blocks"""
+    p = fb.make_problem("richards3d", nx=36, ny=36, nz=30, Lx=36.0, Ly=36.0, Lz=30.0)
+    ph = fb.Physics(p)
+    orc = Oracle(p)
+    y, yp = state(p, 6)
+    yt, ypt = T(y, cuda), T(yp, cuda)
+    ph.begin_step(0.0, yt, ypt)
+    F0 = torch.empty_like(yt)
+    ph.residual(0.0, yt, ypt, F0)
+    ewt = 1.0 / (1e-6 * np.abs(y) + 1e-6)
+    pc = fb.Preconditioner(ph)
+    pc.set_blocks_per_sm(per_sm)
+    assert pc.setup(0.0, 1e-2, 100.0, yt, ypt, F0, T(ewt, cuda), 0) == 0
+    _, _, val = pc.jacobian()
+    nb = pc.info()["nblocks"]
+    assert nb == per_sm * torch.cuda.get_device_properties(0).multi_processor_count
+    orc.psetup(0.0, 1e-2, 100.0, y, yp, F0.cpu().numpy(), ewt, nb)
+    assert factor_given(orc, val, nb) == 0
+    r = np.random.default_rng(8).standard_normal(p.n_nodes)
+    z = torch.empty_like(yt)
+    pc.apply(T(r, cuda), z)
+    ref = orc.psolve(r)
+    err = np.abs(z.cpu().numpy() - ref).max() / np.abs(ref).max()
+    assert err < 1e-10, (per_sm, err)
 
 
 @pytest.mark.parametrize("precision", [0, 1])
