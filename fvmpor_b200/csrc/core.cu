@@ -50,6 +50,7 @@ __global__ void k_node(int N, const double* __restrict__ y, const double* __rest
                        const int* __restrict__ nz_ptr, const int* __restrict__ nz_zone,
                        const double* __restrict__ nz_w, double rho0, double* __restrict__ krw,
                        double* __restrict__ hstar, double* __restrict__ stor, NodeCopies cp) {
+    if (pt.skip && *pt.skip) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     double h = y[i], hp = yp[i];
@@ -140,6 +141,7 @@ struct ElemArgs {
     double* part;                 // [P] chunk-major partials
     int* err;                     // 5 = a pipeline wait gave up
     size_t P;
+    const int* skip;              // skip the launch when *skip != 0
 };
 
 constexpr int kElemThreads = 256;
@@ -205,6 +207,7 @@ __global__ void __launch_bounds__(kElemThreads) k_elem_chunk(ElemArgs a) {
     int4* meta = reinterpret_cast<int4*>(cc + (size_t)NPE * a.CE);                // [2]
     uint64_t* full = reinterpret_cast<uint64_t*>(meta + 2);                      // [2]
     if ((int)blockIdx.x >= a.nch) return;
+    if (a.skip && *a.skip) return;
     if (threadIdx.x == 0) {
         tc05::mbar_init(&full[0], 1);
         tc05::mbar_init(&full[1], 1);
@@ -323,7 +326,8 @@ __global__ void k_gather(int N, const int* __restrict__ part_ptr, const int* __r
                          const unsigned char* __restrict__ ntype, const double* __restrict__ h,
                          const double* __restrict__ stor, const double* __restrict__ F0,
                          double inv_sigma, const double* __restrict__ sigma_dev,
-                         double* __restrict__ out) {
+                         double* __restrict__ out, const int* __restrict__ skip) {
+    if (skip && *skip) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     double r;
@@ -446,8 +450,9 @@ static void set_chunk_attrs(fvm_ctx* c) {
     });
 }
 
-static void launch_elem(fvm_ctx* c, const double* h) {
+static void launch_elem(fvm_ctx* c, const double* h, const int* skip = nullptr) {
     ElemArgs a;
+    a.skip = skip;
     (void)h;   // the node pass left the head in the chunk-major copies
     a.T = c->T; a.N = c->N; a.CE = c->chunk_e; a.nch = c->nchunk; a.kiso = c->kiso ? 1 : 0;
     a.estride = c->estride; a.nnmax = c->chunk_maxnn;
@@ -568,7 +573,7 @@ void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Pertur
                                                       c->hstar.p, c->stor.p, node_copies(c));
     c->tm.end(TM_NODE, s);
     c->tm.begin(TM_ELEM, s);
-    launch_elem(c, h);
+    launch_elem(c, h, pt.skip);
     c->tm.end(TM_ELEM, s);
     double inv_sigma = 0.0;
     if (F0 && !pt.sigma_dev) inv_sigma = 1.0 / pt.sigma;
@@ -576,7 +581,7 @@ void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Pertur
     fvm_launch(c, k_gather, grid_for(c->N, kBlock), kBlock, 0, s, c->N, c->part_ptr.p, c->ch_cpos.p, c->part.p,
                                                         c->invV.p, c->bterm.p, c->hD.p, c->ntype.p,
                                                         h, c->stor.p, F0, inv_sigma,
-                                                        F0 ? pt.sigma_dev : nullptr, out);
+                                                        F0 ? pt.sigma_dev : nullptr, out, pt.skip);
     c->tm.end(TM_GATHER, s);
     c->n_residuals++;
 }

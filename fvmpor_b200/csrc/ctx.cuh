@@ -112,6 +112,8 @@ struct Perturb {
     const double* shift = nullptr;   // mode 2: shift vector d
     const int* colour = nullptr;     // mode 2: colour of every node
     int c = 0;                       // mode 2: active colour
+    const int* skip = nullptr;       // when set and *skip != 0 the evaluation is skipped
+                                     // (a device-driven loop that has already finished)
 };
 
 struct BlockILU;   // precond.cu

@@ -7,6 +7,17 @@
 
 namespace fvmb {
 
+// state of a device-driven Arnoldi cycle (k_arnoldi_givens)
+struct ArnState {
+    int j;          // completed Arnoldi steps
+    int done;       // 0 running, 1 converged, 2 basis full, 3 breakdown
+    int m;
+    int pad;
+    double tol;     // stop when |g_j| / sqrt(N) <= tol
+    double sqrtN;
+    double rnorm;   // |g_j| / sqrt(N) after the last step
+};
+
 struct Krylov {
     int m = 0;
     int precision = 0;        // 0: FP64 basis, 1: FP32 basis
@@ -21,6 +32,8 @@ struct Krylov {
     DevBuf<unsigned> bar;     // grid barrier of the fused orthogonalisation
     DevBuf<int> err;          // 3 = a grid barrier timed out
     int coop_grid = 0;        // blocks of the cooperative launch, 0 = three-pass path
+    DevBuf<ArnState> st;      // device-driven Arnoldi state
+    DevBuf<double> ls;        // H [(m+1) x m], cs [m], sn [m], g [m+1]
     double* host = nullptr;   // pinned
 };
 
@@ -41,7 +54,7 @@ int gmres_dev(fvm_ctx* c, double cj, const double* y, const double* yp, const do
 // preconditioner (precond.cu)
 void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* yp,
                 const double* F0, const double* ewt, int precision);
-void psolve_dev(fvm_ctx* c, const double* r, double* z);
+void psolve_dev(fvm_ctx* c, const double* r, double* z, const int* skip = nullptr);
 bool ilu_ready(fvm_ctx* c);
 int ilu_status(fvm_ctx* c);   // 0 ok, 1 zero pivot in the last factorisation
 

@@ -199,98 +199,142 @@ __device__ __forceinline__ void block_reduce_all(const double* partial, int nv, 
     __syncthreads();
 }
 
-// CGS2 step of Arnoldi for basis vector nv (three reductions, two grid
-// barriers between them plus one after the norm), followed by the next
-// Krylov direction t = s_nv U_nv / ewt and its difference-quotient increment
-// sigma = 1 / ||t||_wrms:
-//   W = ewt Jv; a = U^T W; W -= U diag(s^2) a; b = U^T W; W -= U diag(s^2) b;
-//   U_nv = W; s_nv = 1 / ||U_nv||.
-// res receives a (m+2 slots), b (m+2 slots) and ||U_nv||^2, as the three
-// separate passes wrote them.
+constexpr int kCgsThreads = 512;
+
+// block-local dot products <U_i, W> over rows [k0, k1) for i < nv: the
+// warps split the (vector, row segment) pairs, the segments of a vector are
+// then summed in segment order.  Row nv of the output (when with_norm) is
+// sum W^2.  out[i] is valid in every thread after the call.
 template <class B>
-__global__ void __launch_bounds__(kRedThreads) k_arnoldi_cgs2(int N, int nv, int mslot, B* __restrict__ U, size_t ld,
+__device__ __forceinline__ void block_dots(const B* __restrict__ U, size_t ld, const double* __restrict__ W, int k0,
+                                           int k1, int nv, bool with_norm, double* seg_sums, double* out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int nvec = nv + (with_norm ? 1 : 0);
+    const int nseg = max(1, nw / nvec);
+    const int len = (k1 - k0 + nseg - 1) / nseg;
+    for (int idx = warp; idx < nvec * nseg; idx += nw) {
+        const int i = idx / nseg, sg = idx - i * nseg;
+        const int a = k0 + sg * len, b = min(k1, a + len);
+        double sacc = 0.0;
+        if (i < nv) {
+            const B* Ui = U + ld * i;
+            for (int k = a + lane; k < b; k += 32) sacc += ldb(Ui, k) * W[k];
+        } else {
+            for (int k = a + lane; k < b; k += 32) sacc += W[k] * W[k];
+        }
+        sacc = warp_sum(sacc);
+        if (lane == 0) seg_sums[idx] = sacc;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
+        double t = 0.0;
+        for (int sg = 0; sg < nseg; ++sg) t += seg_sums[i * nseg + sg];
+        out[i] = t;
+    }
+    __syncthreads();
+}
+
+// One Arnoldi step of the device-driven GMRES in one cooperative launch:
+// CGS2 orthogonalisation of the new direction against the basis, the new
+// basis vector and its scale, the next Krylov direction t = s_nv U_nv / ewt
+// with its difference-quotient increment sigma = 1 / ||t||_wrms, and (block
+// 0) the Hessenberg column, Givens rotations and stopping test
+// (linalg_dense.c:128-173):
+//   W = ewt Jv; a = U^T W;  W' = W - U diag(s^2) a;  b = U^T W';
+//   U_nv = W' - U diag(s^2) b;  ||U_nv||^2 = ||W'||^2 - sum_i (s_i b_i)^2.
+// The last line is Pythagoras on the re-orthogonalisation: b is a
+// rounding-level correction, so the norm needs no third reduction.  Two grid
+// barriers per step.  Every reduction is fixed-order (per-block partials in
+// block order), so results are bitwise reproducible.
+template <class B>
+__global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* st, B* __restrict__ U, size_t ld,
                                                               double* __restrict__ scale,
                                                               const double* __restrict__ Jv,
                                                               const double* __restrict__ ewt,
                                                               double* __restrict__ W, double* partial,
-                                                              unsigned* bar, int* err, double* res,
-                                                              double* __restrict__ t_next, double* sigma_next) {
-    __shared__ double coef[64];
-    __shared__ double red[32];
+                                                              unsigned* bar, int* err,
+                                                              double* __restrict__ t_next, double* sigma_next,
+                                                              double* __restrict__ H, double* __restrict__ cs,
+                                                              double* __restrict__ sn, double* __restrict__ g) {
+    __shared__ double ca[64], cb[64], seg[64];
+    if (st->done) return;            // the device-driven loop has finished
+    const int j = st->j, nv = j + 1, m = st->m;
     const int nblk = gridDim.x;
     const int chunk = (N + nblk - 1) / nblk;
     const int k0 = blockIdx.x * chunk, k1 = min(N, k0 + chunk);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     double* pa = partial;
     double* pb = partial + (size_t)nblk * 64;
-    double* pc = partial + (size_t)nblk * 128;
-    // pass 1
+    // pass 1: a = U^T W
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) W[k] = ewt[k] * Jv[k];
     __syncthreads();
-    for (int i = warp; i < nv; i += nw) {
-        const B* Ui = U + ld * i;
-        double sacc = 0.0;
-        for (int k = k0 + lane; k < k1; k += 32) sacc += ldb(Ui, k) * W[k];
-        sacc = warp_sum(sacc);
-        if (lane == 0) pa[(size_t)blockIdx.x * nv + i] = sacc;
-    }
+    block_dots(U, ld, W, k0, k1, nv, false, seg, ca);
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) pa[(size_t)blockIdx.x * nv + i] = ca[i];
     if (!grid_barrier(bar, bar + 1, err)) return;
-    block_reduce_all(pa, nv, nblk, coef);
-    if (blockIdx.x == 0)
-        for (int i = threadIdx.x; i < nv; i += blockDim.x) res[i] = coef[i];
-    for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = coef[i] * scale[i] * scale[i];
+    block_reduce_all(pa, nv, nblk, ca);
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) cb[i] = ca[i] * scale[i] * scale[i];
     __syncthreads();
-    // pass 2
+    // pass 2: W' = W - U diag(s^2) a; b = U^T W', ||W'||^2
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
         double acc = 0.0;
-        for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
+        for (int i = 0; i < nv; ++i) acc += cb[i] * ldb(U + ld * i, k);
         W[k] = W[k] - acc;
     }
     __syncthreads();
-    for (int i = warp; i < nv; i += nw) {
-        const B* Ui = U + ld * i;
-        double sacc = 0.0;
-        for (int k = k0 + lane; k < k1; k += 32) sacc += ldb(Ui, k) * W[k];
-        sacc = warp_sum(sacc);
-        if (lane == 0) pb[(size_t)blockIdx.x * nv + i] = sacc;
-    }
+    block_dots(U, ld, W, k0, k1, nv, true, seg, cb);
+    for (int i = threadIdx.x; i <= nv; i += blockDim.x) pb[(size_t)blockIdx.x * (nv + 1) + i] = cb[i];
     if (!grid_barrier(bar, bar + 1, err)) return;
-    block_reduce_all(pb, nv, nblk, coef);
-    if (blockIdx.x == 0)
-        for (int i = threadIdx.x; i < nv; i += blockDim.x) res[mslot + i] = coef[i];
-    for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = coef[i] * scale[i] * scale[i];
+    block_reduce_all(pb, nv + 1, nblk, cb);
+    double nrm2 = cb[nv];
+    for (int i = 0; i < nv; ++i) {
+        const double c = scale[i] * cb[i];
+        nrm2 -= c * c;
+    }
+    nrm2 = nrm2 > 0.0 ? nrm2 : 0.0;
+    const double snv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
+    __shared__ double coef[64];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = cb[i] * scale[i] * scale[i];
     __syncthreads();
-    // pass 3: new basis vector and its norm
+    // pass 3: the new basis vector and the next direction
     B* Un = U + ld * nv;
-    double sq = 0.0;
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
         double acc = 0.0;
         for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
-        const B st = (B)(W[k] - acc);
-        Un[k] = st;
-        const double d = (double)st;
-        sq += d * d;
+        const B u = (B)(W[k] - acc);
+        Un[k] = u;
+        t_next[k] = snv * (double)u / ewt[k];
     }
-    sq = warp_sum(sq);
-    if (lane == 0) red[warp] = sq;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        double tt = threadIdx.x < nw ? red[threadIdx.x] : 0.0;
-        tt = warp_sum(tt);
-        if (threadIdx.x == 0) pc[blockIdx.x] = tt;
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    scale[nv] = snv;
+    // ||t||_wrms^2 = sum_k (s U_k)^2 / N
+    const double tw = snv * snv * nrm2 / (double)N;
+    *sigma_next = tw > 0.0 ? 1.0 / sqrt(tw) : 1.0;
+    // Hessenberg column, rotations, least-squares residual
+    double hc[65];
+    for (int i = 0; i < nv; ++i) hc[i] = scale[i] * (ca[i] + cb[i]);
+    const double hn = sqrt(nrm2);
+    hc[nv] = hn;
+    if (!isfinite(hn) || !isfinite(hc[j])) {
+        st->done = 3;
+        return;
     }
-    if (!grid_barrier(bar, bar + 1, err)) return;
-    block_reduce_all(pc, 1, nblk, coef);
-    const double nrm2 = coef[0];
-    const double sn = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        res[2 * mslot] = nrm2;
-        scale[nv] = sn;
-        // ||t||_wrms^2 = sum_k (s U_k)^2 / N
-        const double tw = sn * sn * nrm2 / (double)N;
-        *sigma_next = tw > 0.0 ? 1.0 / sqrt(tw) : 1.0;
+    for (int i = 0; i < j; ++i) {
+        const double t0 = cs[i] * hc[i] + sn[i] * hc[i + 1];
+        const double t1 = -sn[i] * hc[i] + cs[i] * hc[i + 1];
+        hc[i] = t0;
+        hc[i + 1] = t1;
     }
-    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) t_next[k] = sn * ldb(Un, k) / ewt[k];
+    const double den = hypot(hc[j], hc[j + 1]);
+    if (den == 0.0) { cs[j] = 1.0; sn[j] = 0.0; }
+    else { cs[j] = hc[j] / den; sn[j] = hc[j + 1] / den; }
+    hc[j] = den;
+    g[j + 1] = -sn[j] * g[j];
+    g[j] = cs[j] * g[j];
+    for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hc[i];
+    const double rn = fabs(g[j + 1]) / st->sqrtN;
+    st->rnorm = rn;
+    st->j = j + 1;
+    if (rn <= st->tol || hn == 0.0) st->done = 1;
+    else if (j + 1 == m) st->done = 2;
 }
 
 __global__ void k_set_scale(const double* nrm2, double* scale, int idx) {
@@ -377,6 +421,8 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
     K->partial.alloc((size_t)kRedBlocks * std::max(m + 2, 3 * 64));
     K->counter.alloc(1);
     K->counter.zero(c->stream);
+    K->st.alloc(1);
+    K->ls.alloc((size_t)(m + 1) * m + 3 * (size_t)m + 1);
     K->bar.alloc(2);
     K->bar.zero(c->stream);
     K->err.alloc(1);
@@ -388,15 +434,17 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
         FVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         FVM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         if (precision)
-            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<float>, kRedThreads, 0));
+            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<float>, kCgsThreads, 0));
         else
-            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<double>, kRedThreads, 0));
-        K->coop_grid = (coop && per_sm > 0 && m + 1 <= 64) ? std::min(kRedBlocks, per_sm * nsm) : 0;
+            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<double>, kCgsThreads, 0));
+        // one block per SM: fewer arrivals at each grid barrier
+        K->coop_grid = (coop && per_sm > 0 && m + 1 <= 63) ? nsm : 0;
     }
     K->res.alloc(3 * (m + 2) + 8);
     K->sigma.alloc(1);
-    // results of the three passes plus the m+1 basis scales
-    FVM_CUDA(cudaMallocHost(&K->host, sizeof(double) * (4 * (m + 2) + 8)));
+    // results of the three passes, the m+1 basis scales, a status word and
+    // the device-driven Arnoldi state
+    FVM_CUDA(cudaMallocHost(&K->host, sizeof(double) * (4 * (m + 2) + 8) + sizeof(ArnState)));
     c->kry = K;
     return K;
 }
@@ -481,14 +529,92 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         g[0] = beta;
         int j = 0;
         bool conv = false;
-        for (; j < m; ++j) {
-            // w = D P^-1 J D^-1 V_j (left preconditioning, scaled by D = ewt);
-            // the fused orthogonalisation of step j-1 already left the
-            // direction in K->t and its increment in K->sigma
-            const bool fused_in = j > 0 && K->coop_grid > 0;
-            if (!fused_in)
-                fvm_launch(c, k_unscale<B>, grid_for(N, 256), 256, 0, s, N, U + ld * j, K->scale.p, j, ewt, K->t.p);
-            jv_dev(c, K, cj, y, yp, F0, K->t.p, ewt, K->Jv.p, fused_in);
+        if (K->coop_grid > 0) {
+            // Device-driven Arnoldi: each step is J*v, the preconditioner,
+            // the fused CGS2 and the Givens update, all reading the step
+            // index and the stop flag from device memory; steps are queued
+            // in batches and the host looks at the state once per batch.
+            // Steps queued after the stop are skipped by every kernel.
+            ArnState* hst = reinterpret_cast<ArnState*>(K->host + 4 * (m + 2) + 8);
+            *hst = ArnState{0, 0, m, 0, tol, sqrtN, rnorm};
+            FVM_CUDA(cudaMemcpyAsync(K->st.p, hst, sizeof(ArnState), cudaMemcpyHostToDevice, s));
+            double* H_d = K->ls.p;
+            double* cs_d = H_d + (size_t)(m + 1) * m;
+            double* sn_d = cs_d + m;
+            double* g_d = sn_d + m;
+            FVM_CUDA(cudaMemcpyAsync(g_d, g.data(), sizeof(double) * (m + 1), cudaMemcpyHostToDevice, s));
+            // first direction and its increment
+            fvm_launch(c, k_unscale<B>, grid_for(N, 256), 256, 0, s, N, U, K->scale.p, 0, ewt, K->t.p);
+            fvm_launch(c, k_sumsq, kRedBlocks, kRedThreads, 0, s, N, K->t.p, ewt, K->partial.p, K->counter.p,
+                       K->res.p);
+            fvm_launch(c, k_sigma_from_sumsq, 1, 1, 0, s, K->res.p, N, K->sigma.p);
+            const int* skip = &K->st.p->done;
+            int queued = 0;
+            for (;;) {
+                const int batch = std::min(m - queued, queued < 2 ? 2 : 4);
+                for (int q = 0; q < batch; ++q) {
+                    Perturb pt;
+                    pt.mode = 1;
+                    pt.cj = cj;
+                    pt.v = K->t.p;
+                    pt.sigma_dev = K->sigma.p;
+                    pt.skip = skip;
+                    launch_residual(c, y, yp, pt, F0, K->Jv.p);
+                    psolve_dev(c, K->Jv.p, K->z.p, skip);
+                    c->tm.begin(TM_CGS, s);
+                    int Ni = N;
+                    ArnState* stp = K->st.p;
+                    B* Ub = U;
+                    size_t ldv = ld;
+                    double* scp = K->scale.p;
+                    const double* jvp = K->z.p;
+                    const double* ew = ewt;
+                    double* Wp = K->W.p;
+                    double* pp = K->partial.p;
+                    unsigned* bp = K->bar.p;
+                    int* ep = K->err.p;
+                    double* tp = K->t.p;
+                    double* sgp = K->sigma.p;
+                    void* args[] = {&Ni, &stp, &Ub, &ldv, &scp, &jvp, &ew, &Wp, &pp, &bp, &ep, &tp, &sgp,
+                                    &H_d, &cs_d, &sn_d, &g_d};
+                    FVM_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi_cgs2<B>, dim3(K->coop_grid),
+                                                         dim3(kCgsThreads), args, 0, s));
+                    c->launches++;
+                    c->tm.end(TM_CGS, s);
+                }
+                queued += batch;
+                int* herr = reinterpret_cast<int*>(K->host + 4 * (m + 2) + 7);
+                FVM_CUDA(cudaMemcpyAsync(hst, K->st.p, sizeof(ArnState), cudaMemcpyDeviceToHost, s));
+                FVM_CUDA(cudaMemcpyAsync(herr, K->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+                FVM_CUDA(cudaStreamSynchronize(s));
+                if (*herr != 0) {
+                    // a grid barrier gave up: the step's numbers are not valid
+                    K->err.zero(s);
+                    K->bar.zero(s);
+                    *iters = total + hst->j;
+                    *res_norm = rnorm;
+                    return 2;
+                }
+                if (hst->done || queued >= m) break;
+            }
+            j = hst->j;
+            total += j;
+            c->n_residuals -= queued - j;   // evaluations queued after the stop were skipped
+            if (cnt) { cnt->njv += j; cnt->nps += j; }
+            if (hst->done == 3) { *iters = total; *res_norm = rnorm; return 2; }
+            rnorm = hst->rnorm;
+            conv = hst->done == 1;
+            // least-squares data of the cycle for the back substitution
+            FVM_CUDA(cudaMemcpyAsync(H.data(), H_d, sizeof(double) * (size_t)(m + 1) * m, cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaMemcpyAsync(g.data(), g_d, sizeof(double) * (m + 1), cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaMemcpyAsync(K->host + 3 * (m + 2), K->scale.p, sizeof(double) * std::max(j, 1),
+                                     cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaStreamSynchronize(s));
+        }
+        for (; K->coop_grid == 0 && j < m; ++j) {
+            // w = D P^-1 J D^-1 V_j (left preconditioning, scaled by D = ewt)
+            fvm_launch(c, k_unscale<B>, grid_for(N, 256), 256, 0, s, N, U + ld * j, K->scale.p, j, ewt, K->t.p);
+            jv_dev(c, K, cj, y, yp, F0, K->t.p, ewt, K->Jv.p);
             if (cnt) cnt->njv++;
             psolve_dev(c, K->Jv.p, K->z.p);
             if (cnt) cnt->nps++;
@@ -497,25 +623,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
             double* rb = K->res.p + (m + 2);
             double* rn = K->res.p + 2 * (m + 2);
             c->tm.begin(TM_CGS, s);
-            if (K->coop_grid > 0) {
-                int Ni = N, nvi = nv, ms = m + 2;
-                B* Ub = U;
-                size_t ldv = ld;
-                double* scp = K->scale.p;
-                const double* jvp = K->z.p;
-                const double* ew = ewt;
-                double* Wp = K->W.p;
-                double* pp = K->partial.p;
-                unsigned* bp = K->bar.p;
-                int* ep = K->err.p;
-                double* rp = K->res.p;
-                double* tp = K->t.p;
-                double* sgp = K->sigma.p;
-                void* args[] = {&Ni, &nvi, &ms, &Ub, &ldv, &scp, &jvp, &ew, &Wp, &pp, &bp, &ep, &rp, &tp, &sgp};
-                FVM_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi_cgs2<B>, dim3(K->coop_grid),
-                                                     dim3(kRedThreads), args, 0, s));
-                c->launches++;
-            } else {
+            {
                 fvm_launch(c, k_cgs_pass1<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->z.p, ewt, K->W.p, K->partial.p, K->counter.p, ra);
                 fvm_launch(c, k_cgs_pass2<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->scale.p, ra, K->W.p, K->partial.p, K->counter.p, rb);
                 fvm_launch(c, k_cgs_pass3<B>, kRedBlocks, kRedThreads, 0, s, N, nv, U, ld, K->scale.p, rb, K->W.p, K->partial.p, K->counter.p, rn);
@@ -524,17 +632,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
             c->tm.end(TM_CGS, s);
             FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, s));
             FVM_CUDA(cudaMemcpyAsync(K->host + 3 * (m + 2), K->scale.p, sizeof(double) * (nv), cudaMemcpyDeviceToHost, s));
-            int* herr = reinterpret_cast<int*>(K->host + 4 * (m + 2) + 7);
-            if (K->coop_grid > 0) FVM_CUDA(cudaMemcpyAsync(herr, K->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
             FVM_CUDA(cudaStreamSynchronize(s));
-            if (K->coop_grid > 0 && *herr != 0) {
-                // a grid barrier gave up: the step's numbers are not valid
-                K->err.zero(s);
-                K->bar.zero(s);
-                *iters = total;
-                *res_norm = rnorm;
-                return 2;
-            }
             const double* ha = K->host;
             const double* hb = K->host + (m + 2);
             const double* hsc = K->host + 3 * (m + 2);

@@ -51,6 +51,8 @@ struct BlockILU {
     DevBuf<int> bstart, lu_ptr, lu_src, lu_diag;
     DevBuf<unsigned short> lu_col;
     DevBuf<int> lvl_ptr, lvl_rows, blk_lvl, ulvl_ptr, ulvl_rows, blk_ulvl;
+    DevBuf<unsigned short> meta;   // per-block metadata records of the staged apply
+    DevBuf<int> meta_off;
     DevBuf<double> lu64;
     DevBuf<float> lu32;
     int factored = -1;        // precision of the current factor, -1 none
@@ -284,8 +286,9 @@ __global__ void __launch_bounds__(128) k_ilu_apply(const int* __restrict__ bstar
                                                    const int* __restrict__ blk_ulvl,
                                                    const T* __restrict__ lu,
                                                    const double* __restrict__ r,
-                                                   double* __restrict__ z) {
+                                                   double* __restrict__ z, const int* __restrict__ skip) {
     extern __shared__ unsigned char smem_raw[];
+    if (skip && *skip) return;
     T* x = reinterpret_cast<T*>(smem_raw);
     int b = blockIdx.x;
     int r0 = bstart[b], r1 = bstart[b + 1];
@@ -337,18 +340,26 @@ __device__ __forceinline__ IluWindow ilu_window(int e0, int e1) {
 }
 __host__ __device__ __forceinline__ size_t round16(size_t b) { return (b + 15) & ~(size_t)15; }
 
+// u16 words of a block's metadata record: rp (nr+1) | dg (nr) | lrow (nr) |
+// urow (nr) | lptr (nl+1) | uptr (nu+1), padded to 16 bytes
+__host__ __device__ __forceinline__ size_t ilu_meta_words(size_t nr, size_t nlev) {
+    return (4 * nr + 1 + nlev + 7) & ~(size_t)7;
+}
+
 // shared bytes of the staged kernels for one block (host and device agree);
 // nlev = nl + 1 + nu + 1 level offsets of the two sweeps
 __host__ __device__ __forceinline__ size_t ilu_stage_bytes(size_t nr, size_t wn, size_t nlev, size_t sz) {
-    return round16(round16(nr * sz) + wn * (sz + 2) + (4 * nr + 1 + nlev) * 2) + 16;
+    return round16(round16(nr * sz) + wn * (sz + 2) + ilu_meta_words(nr, nlev) * 2) + 16;
 }
 
 template <class T>
 __device__ __forceinline__ void ilu_stage_bulk(T* val, unsigned short* col, const T* lu,
-                                               const unsigned short* lu_col, IluWindow w, uint64_t* bar) {
+                                               const unsigned short* lu_col, IluWindow w, uint64_t* bar,
+                                               unsigned short* meta_dst = nullptr,
+                                               const unsigned short* meta_src = nullptr, int meta_words = 0) {
     if (threadIdx.x == 0) {
         uint32_t b = tc05::smem_u32(bar);
-        uint32_t bytes = (uint32_t)(w.wn * (sizeof(T) + sizeof(unsigned short)));
+        uint32_t bytes = (uint32_t)(w.wn * (sizeof(T) + sizeof(unsigned short)) + meta_words * 2);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes));
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                          tc05::smem_u32(val)),
@@ -358,6 +369,11 @@ __device__ __forceinline__ void ilu_stage_bulk(T* val, unsigned short* col, cons
                          tc05::smem_u32(col)),
                      "l"(lu_col + w.base), "r"((uint32_t)(w.wn * sizeof(unsigned short))), "r"(b)
                      : "memory");
+        if (meta_words)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             tc05::smem_u32(meta_dst)),
+                         "l"(meta_src), "r"((uint32_t)(meta_words * 2)), "r"(b)
+                         : "memory");
     }
 }
 
@@ -381,6 +397,8 @@ __device__ __forceinline__ void ilu_fetch(IluRow<T, KM, UPPER>& R, int l, int nl
                                           const unsigned short* dg, const unsigned short* rows,
                                           const unsigned short* lptr) {
     R.li = -1;
+#pragma unroll
+    for (int k = 0; k < KM; ++k) R.c[k] = 0;
     if (l >= nlv) return;
     const int q = lptr[l] + threadIdx.x;
     if (q >= lptr[l + 1]) return;
@@ -404,23 +422,33 @@ __device__ __forceinline__ void ilu_sweep(T* x, const T* val, const unsigned sho
     IluRow<T, KM, UPPER> cur, nxt;
     ilu_fetch(cur, l0, nlv, val, col, rp, dg, rows, lptr);
     for (int l = l0; l < nlv; ++l) {
+        // issue this level's x loads first (threads without a row read entry
+        // 0 and store nothing), then fetch the next level's row while they
+        // are in flight, then accumulate
+        const bool act = cur.li >= 0;
+        const int li = act ? cur.li : 0;
+        T xv[KM];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) xv[k] = x[cur.c[k]];
+        const T xi = x[li];
+        const int q0 = lptr[l], q1 = lptr[l + 1];
         ilu_fetch(nxt, l + 1, nlv, val, col, rp, dg, rows, lptr);
-        if (cur.li >= 0) {
+        if (act) {
             T acc = (T)0;
 #pragma unroll
             for (int k = 0; k < KM; ++k)
-                if (cur.p0 + k < cur.p1) acc += cur.v[k] * x[cur.c[k]];
+                if (cur.p0 + k < cur.p1) acc += cur.v[k] * xv[k];
             for (int p = cur.p0 + KM; p < cur.p1; ++p) acc += val[p] * x[col[p]];
-            x[cur.li] = UPPER ? (x[cur.li] - acc) * cur.piv : x[cur.li] - acc;
+            x[li] = UPPER ? (xi - acc) * cur.piv : xi - acc;
         }
         // rows of a level wider than the CTA
-        for (int q = lptr[l] + threadIdx.x + blockDim.x; q < lptr[l + 1]; q += blockDim.x) {
-            const int li = rows[q];
-            const int d = dg[li];
-            const int p0 = UPPER ? d + 1 : rp[li], p1 = UPPER ? rp[li + 1] : d;
+        for (int q = q0 + threadIdx.x + blockDim.x; q < q1; q += blockDim.x) {
+            const int lj = rows[q];
+            const int d = dg[lj];
+            const int p0 = UPPER ? d + 1 : rp[lj], p1 = UPPER ? rp[lj + 1] : d;
             T acc = (T)0;
             for (int p = p0; p < p1; ++p) acc += val[p] * x[col[p]];
-            x[li] = UPPER ? (x[li] - acc) * val[d] : x[li] - acc;
+            x[lj] = UPPER ? (x[lj] - acc) * val[d] : x[lj] - acc;
         }
         __syncthreads();
         cur = nxt;
@@ -430,18 +458,17 @@ __device__ __forceinline__ void ilu_sweep(T* x, const T* val, const unsigned sho
 template <class T, int KM>
 __global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __restrict__ bstart,
                                                         const int* __restrict__ lu_ptr,
-                                                        const int* __restrict__ lu_diag,
                                                         const unsigned short* __restrict__ lu_col,
-                                                        const int* __restrict__ lvl_ptr,
-                                                        const int* __restrict__ lvl_rows,
+                                                        const unsigned short* __restrict__ meta,
+                                                        const int* __restrict__ meta_off,
                                                         const int* __restrict__ blk_lvl,
-                                                        const int* __restrict__ ulvl_ptr,
-                                                        const int* __restrict__ ulvl_rows,
                                                         const int* __restrict__ blk_ulvl,
                                                         const T* __restrict__ lu,
                                                         const double* __restrict__ r,
-                                                        double* __restrict__ z, int* __restrict__ err) {
+                                                        double* __restrict__ z, int* __restrict__ err,
+                                                        const int* __restrict__ skip) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (skip && *skip) return;
     const int b = blockIdx.x;
     const int r0 = bstart[b], r1 = bstart[b + 1], nr = r1 - r0;
     const IluWindow w = ilu_window(lu_ptr[r0], lu_ptr[r1]);
@@ -462,17 +489,12 @@ __global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __res
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     __syncthreads();
-    ilu_stage_bulk(val, col, lu, lu_col, w, bar);
-    // a block's rows appear once in each level-ordered list, at [r0, r1)
-    for (int i = threadIdx.x; i <= nr; i += blockDim.x) rp[i] = (unsigned short)(lu_ptr[r0 + i] - w.base);
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
-        dg[i] = (unsigned short)(lu_diag[r0 + i] - w.base);
-        x[i] = (T)r[r0 + i];
-        lrow[i] = (unsigned short)(lvl_rows[r0 + i] - r0);
-        urow[i] = (unsigned short)(ulvl_rows[r0 + i] - r0);
-    }
-    for (int l = threadIdx.x; l <= nl; l += blockDim.x) lptr[l] = (unsigned short)(lvl_ptr[la + l] - r0);
-    for (int l = threadIdx.x; l <= nu; l += blockDim.x) uptr[l] = (unsigned short)(ulvl_ptr[ua + l] - r0);
+    // factor window and the block's metadata record (row pointers, pivot
+    // positions, level lists) by three bulk copies; the right-hand side by
+    // the threads meanwhile
+    const int mo = meta_off[b];
+    ilu_stage_bulk(val, col, lu, lu_col, w, bar, rp, meta + mo, meta_off[b + 1] - mo);
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) x[i] = (T)r[r0 + i];
     bool ok = tc05::mbar_wait(bar, 0);
     if (!ok) ok = tc05::mbar_wait(bar, 0);   // copies in flight get a second bounded chance
     if (!__syncthreads_and(ok ? 1 : 0)) {
@@ -692,6 +714,25 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
     P->nb = nb;
     P->maxb = maxb;
     P->nlevels_max = nlmax;
+    // per-block metadata records of the staged apply (layout of
+    // ilu_meta_words), 16-byte aligned
+    std::vector<unsigned short> meta;
+    std::vector<int> meta_off(1, 0);
+    for (int b = 0; b < nb; ++b) {
+        const int r0 = bstart[b], r1 = bstart[b + 1], nr = r1 - r0;
+        const int base = lu_ptr[r0] & ~7;
+        const int la = blk_lvl[b], nl = blk_lvl[b + 1] - la;
+        const int ua = blk_ulvl[b], nu = blk_ulvl[b + 1] - ua;
+        const size_t start = meta.size();
+        for (int i = 0; i <= nr; ++i) meta.push_back((unsigned short)(lu_ptr[r0 + i] - base));
+        for (int i = 0; i < nr; ++i) meta.push_back((unsigned short)(lu_diag[r0 + i] - base));
+        for (int i = 0; i < nr; ++i) meta.push_back((unsigned short)(lvl_rows[r0 + i] - r0));
+        for (int i = 0; i < nr; ++i) meta.push_back((unsigned short)(ulvl_rows[r0 + i] - r0));
+        for (int l = 0; l <= nl; ++l) meta.push_back((unsigned short)(lvl_ptr[la + l] - r0));
+        for (int l = 0; l <= nu; ++l) meta.push_back((unsigned short)(ulvl_ptr[ua + l] - r0));
+        meta.resize(start + ilu_meta_words(nr, (size_t)nl + nu + 2), 0);
+        meta_off.push_back((int)meta.size());
+    }
     {
         size_t need64 = 0, need32 = 0;
         bool fits16 = true;
@@ -748,6 +789,8 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
     P->lu_src.upload(lu_src, s);
     P->lu_diag.upload(lu_diag, s);
     P->lu_col.upload(lu_col, s);
+    P->meta.upload(meta, s);
+    P->meta_off.upload(meta_off, s);
     P->lvl_ptr.upload(lvl_ptr, s);
     P->lvl_rows.upload(lvl_rows, s);
     P->blk_lvl.upload(blk_lvl, s);
@@ -831,7 +874,7 @@ int ilu_status(fvm_ctx* c) {
 
 bool ilu_ready(fvm_ctx* c) { return c->ilu && c->ilu->factored >= 0; }
 
-void psolve_dev(fvm_ctx* c, const double* r, double* z) {
+void psolve_dev(fvm_ctx* c, const double* r, double* z, const int* skip) {
     BlockILU* P = c->ilu;
     if (!P || P->factored < 0) throw Error("psolve: preconditioner not set up");
     cudaStream_t s = c->stream;
@@ -843,9 +886,8 @@ void psolve_dev(fvm_ctx* c, const double* r, double* z) {
     if (P->smem_stage[P->factored]) {
         size_t sm = P->smem_stage[P->factored];
         auto go = [&](auto kern, const auto* lu) {
-            fvm_launch(c, kern, P->nb, kIluThreads, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p,
-                       P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p, P->ulvl_rows.p, P->blk_ulvl.p, lu,
-                       r, z, P->status.p);
+            fvm_launch(c, kern, P->nb, kIluThreads, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_col.p, P->meta.p,
+                       P->meta_off.p, P->blk_lvl.p, P->blk_ulvl.p, lu, r, z, P->status.p, skip);
         };
         if (P->factored) {
             if (P->lanes == 8) go(k_ilu_apply_smem<float, 8>, P->lu32.p);
@@ -858,12 +900,12 @@ void psolve_dev(fvm_ctx* c, const double* r, double* z) {
         size_t sm = sizeof(float) * P->maxb;
         fvm_launch(c, k_ilu_apply<float>, P->nb, 128, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
                                                  P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p, P->ulvl_rows.p,
-                                                 P->blk_ulvl.p, P->lu32.p, r, z);
+                                                 P->blk_ulvl.p, P->lu32.p, r, z, skip);
     } else {
         size_t sm = sizeof(double) * P->maxb;
         fvm_launch(c, k_ilu_apply<double>, P->nb, 128, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
                                                   P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p, P->ulvl_rows.p,
-                                                  P->blk_ulvl.p, P->lu64.p, r, z);
+                                                  P->blk_ulvl.p, P->lu64.p, r, z, skip);
     }
 }
 
