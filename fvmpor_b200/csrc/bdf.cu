@@ -257,12 +257,28 @@ struct DeviceOps {
         }
         fvm_launch(c, k_phi_update, g(), 256, 0, c->stream, N, k, set_kp2, ptrs(), e.p);
     }
+    // The learned iterate costs a network evaluation and one or two residual
+    // evaluations per attempt.  After a run of attempts that the residual
+    // test rejected, the next 2, 4, ... 32 steps use the BDF predictor
+    // without trying, so an unhelpful network costs little; one accepted
+    // attempt resets the back-off.
+    int guess_fails = 0, guess_skip = 0;
     bool newton_guess(double tnew, double h, double cj) {
         (void)tnew;
         if (!pred) return false;
+        if (guess_skip > 0) {
+            --guess_skip;
+            return false;
+        }
         bool kept = predictor_apply(c, pred, o.rtol, o.atol, h, cj, phi[0].p, hprev.p, ypred.p, yppred.p, y.p,
                                     yp.p, e.p, F.p);
         f_fresh = true;   // F holds the residual of whichever iterate was kept
+        if (kept) {
+            guess_fails = 0;
+        } else {
+            guess_fails = std::min(guess_fails + 1, 5);
+            guess_skip = (1 << guess_fails) - 1;
+        }
         return kept;
     }
 

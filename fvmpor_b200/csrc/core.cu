@@ -320,29 +320,11 @@ __global__ void __launch_bounds__(kElemThreads) k_elem_chunk(ElemArgs a) {
 // touches the node, at the chunk-major positions cpos[part_ptr[i] ..
 // part_ptr[i+1]) in ascending chunk order; sum them in that order.
 // F0 != nullptr turns the result into (F - F0) * inv_sigma.
-__global__ void k_gather(int N, const int* __restrict__ part_ptr, const int* __restrict__ cpos,
-                         const double* __restrict__ part, const double* __restrict__ invV,
-                         const double* __restrict__ bterm, const double* __restrict__ hD,
-                         const unsigned char* __restrict__ ntype, const double* __restrict__ h,
-                         const double* __restrict__ stor, const double* __restrict__ F0,
-                         double inv_sigma, const double* __restrict__ sigma_dev,
-                         double* __restrict__ out, const int* __restrict__ skip) {
+__global__ void k_gather(int N, GatherSrc g, double* __restrict__ out, const int* __restrict__ skip) {
     if (skip && *skip) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    double r;
-    if (ntype[i]) {
-        r = hD[i] - h[i];
-    } else {
-        double s = 0.0;
-        int p1 = part_ptr[i + 1];
-        for (int p = part_ptr[i]; p < p1; ++p) s += part[cpos[p]];
-        r = s * invV[i];
-        r = r + bterm[i];
-        r = r - stor[i];
-    }
-    if (F0) r = (r - F0[i]) * (sigma_dev ? 1.0 / *sigma_dev : inv_sigma);
-    out[i] = r;
+    out[i] = gather_row(g, i);
 }
 
 // begin-step element pass: averaged-weight face fluxes in the global edge
@@ -563,8 +545,8 @@ static void build_chunks(fvm_ctx* c, int CE) {
     FVM_CUDA(cudaStreamSynchronize(s));
 }
 
-void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Perturb& pt,
-                     const double* F0, double* out) {
+GatherSrc launch_residual_partials(fvm_ctx* c, const double* y, const double* yp, const Perturb& pt,
+                                   const double* F0) {
     cudaStream_t s = c->stream;
     const double* h = pt.mode ? c->hstar.p : y;
     c->tm.begin(TM_NODE, s);
@@ -575,15 +557,33 @@ void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Pertur
     c->tm.begin(TM_ELEM, s);
     launch_elem(c, h, pt.skip);
     c->tm.end(TM_ELEM, s);
-    double inv_sigma = 0.0;
-    if (F0 && !pt.sigma_dev) inv_sigma = 1.0 / pt.sigma;
-    c->tm.begin(TM_GATHER, s);
-    fvm_launch(c, k_gather, grid_for(c->N, kBlock), kBlock, 0, s, c->N, c->part_ptr.p, c->ch_cpos.p, c->part.p,
-                                                        c->invV.p, c->bterm.p, c->hD.p, c->ntype.p,
-                                                        h, c->stor.p, F0, inv_sigma,
-                                                        F0 ? pt.sigma_dev : nullptr, out, pt.skip);
-    c->tm.end(TM_GATHER, s);
     c->n_residuals++;
+    GatherSrc g;
+    g.part_ptr = c->part_ptr.p;
+    g.cpos = c->ch_cpos.p;
+    g.part = c->part.p;
+    g.invV = c->invV.p;
+    g.bterm = c->bterm.p;
+    g.hD = c->hD.p;
+    g.ntype = c->ntype.p;
+    g.h = h;
+    g.stor = c->stor.p;
+    g.F0 = F0;
+    g.inv_sigma = (F0 && !pt.sigma_dev) ? 1.0 / pt.sigma : 0.0;
+    g.sigma_dev = F0 ? pt.sigma_dev : nullptr;
+    return g;
+}
+
+void gather_into(fvm_ctx* c, const GatherSrc& g, double* out, const int* skip) {
+    c->tm.begin(TM_GATHER, c->stream);
+    fvm_launch(c, k_gather, grid_for(c->N, kBlock), kBlock, 0, c->stream, c->N, g, out, skip);
+    c->tm.end(TM_GATHER, c->stream);
+}
+
+void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Perturb& pt,
+                     const double* F0, double* out) {
+    const GatherSrc g = launch_residual_partials(c, y, yp, pt, F0);
+    gather_into(c, g, out, pt.skip);
 }
 
 void launch_begin_step(fvm_ctx* c, const double* y, const double* yp) {

@@ -116,6 +116,45 @@ struct Perturb {
                                      // (a device-driven loop that has already finished)
 };
 
+// Node gather of the residual chain: the sum of a node's per-chunk element
+// partials (chunk-major positions cpos[part_ptr[i] .. part_ptr[i+1]), in
+// ascending chunk order), times 1/V, plus the boundary-flux term, minus the
+// storage term; Dirichlet rows h_D - h (residual_evaluation,
+// fvmpor_ODE_impl.cpp:99-116).  With F0 set the result becomes the
+// difference quotient (F - F0) / sigma.
+struct GatherSrc {
+    const int* part_ptr;
+    const int* cpos;
+    const double* part;
+    const double* invV;
+    const double* bterm;
+    const double* hD;
+    const unsigned char* ntype;
+    const double* h;
+    const double* stor;
+    const double* F0;
+    double inv_sigma;
+    const double* sigma_dev;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ double gather_row(const GatherSrc& g, int i) {
+    double r;
+    if (g.ntype[i]) {
+        r = g.hD[i] - g.h[i];
+    } else {
+        double s = 0.0;
+        const int p1 = g.part_ptr[i + 1];
+        for (int p = g.part_ptr[i]; p < p1; ++p) s += g.part[g.cpos[p]];
+        r = s * g.invV[i];
+        r = r + g.bterm[i];
+        r = r - g.stor[i];
+    }
+    if (g.F0) r = (r - g.F0[i]) * (g.sigma_dev ? 1.0 / *g.sigma_dev : g.inv_sigma);
+    return r;
+}
+#endif
+
 struct BlockILU;   // precond.cu
 struct Krylov;     // linalg.cu
 struct Predictor;  // predictor.cu
@@ -215,6 +254,11 @@ inline void fvm_launch(fvm_ctx* c, void (*k)(KArgs...), dim3 grid, dim3 block, s
 void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Perturb& pt,
                      const double* F0, double* out);
 void launch_begin_step(fvm_ctx* c, const double* y, const double* yp);
+// the node and element passes of launch_residual without the gather; the
+// returned source describes the gather a consumer performs per row
+GatherSrc launch_residual_partials(fvm_ctx* c, const double* y, const double* yp, const Perturb& pt,
+                                   const double* F0);
+void gather_into(fvm_ctx* c, const GatherSrc& g, double* out, const int* skip);
 // back to the averaged 0.5/0.5 face weights used before the first step
 void reset_upwind(fvm_ctx* c);
 

@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __res
         // the factor never arrived: report it and pass the vector through
         // unpreconditioned instead of reading unfilled shared memory
         if (threadIdx.x == 0) atomicExch(err, 2);
-        for (int i = threadIdx.x; i < nr; i += blockDim.x) z[r0 + i] = r[r0 + i];
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) z[r0 + i] = (double)x[i];
         return;
     }
     // level 0 of the lower sweep has no off-diagonal entries
