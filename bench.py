@@ -37,6 +37,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 METRIC = "sim-s/wall-s, 200k-node 3D Richards @1e-6: learned+FP32 vs plain FP64, 1×B200"
+# DRAM bytes (read + write) of one residual evaluation of this workload --
+# node pass 8.3 MB, element pass 62.6 MB, gather 13.1 MB -- as measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the --profile-case
+# residual workload.  The algorithmic 331.7 MB assume stored face
+# coefficients; the rebuilt-geometry element pass reads a fifth of that.
+CHAIN_DRAM_BYTES = 84.0e6
 UNIT = "sim-s/wall-s"
 
 
@@ -207,6 +213,45 @@ def train_predictor(fb, torch, dev, seed, horizon):
     return P, info
 
 
+def profile_case(name):
+    """Small fixed workloads of single kernels for profiler captures (not a
+    bench line): 'residual' evaluates the residual five times at the
+    hydrostatic head; 'precond' sets up the FP32 preconditioner three times
+    and applies it 20 times after each set-up; 'krylov' integrates the first
+    2 days with the FP32 Krylov path."""
+    import torch
+
+    import fvmpor_b200 as fb
+
+    dev = torch.device("cuda", 0)
+    p = fb.make_problem("richards3d")
+    ph = fb.Physics(p)
+    N = p.n_nodes
+    y = torch.empty(N, dtype=torch.float64, device=dev)
+    ph.initial_head(y)
+    yp = torch.zeros_like(y)
+    r = torch.empty_like(y)
+    if name == "residual":
+        for _ in range(5):
+            ph.residual(0.0, y, yp, r)
+    elif name == "precond":
+        ph.begin_step(0.0, y, yp)
+        ph.residual(0.0, y, yp, r)
+        pc = fb.Preconditioner(ph)
+        ewt = torch.full_like(y, 1e6)
+        v = torch.randn(N, dtype=torch.float64, device=dev, generator=torch.Generator(device=dev).manual_seed(1))
+        z = torch.empty_like(y)
+        for _ in range(3):
+            pc.setup(0.0, 1e-2, 100.0, y, yp, r, ewt, precision=1)
+            for _ in range(20):
+                pc.apply(v, z)
+    else:
+        ye = torch.empty_like(y)
+        fb.Integrator(ph, krylov_dim=40, max_restarts=5, precision=1, max_order=5).integrate(0.0, 2 * 86400.0, y, ye)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": name, "ok": True}))
+
+
 def run_reference(args):
     ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
@@ -249,9 +294,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--days", type=float, default=30.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", choices=["residual", "precond", "krylov"],
+                    help="run one small fixed workload for a profiler capture instead of the bench")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -357,7 +407,7 @@ def main():
         "stats": {k: st0[k] for k in ("nst", "nni", "nli", "npe", "nps", "nre", "ncfn", "netf", "npred",
                                       "last_order")},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": CHAIN_DRAM_BYTES,
                      "kernel": "residual evaluation (node pass + element pass + node gather)",
                      "algorithmic_bytes_per_launch": alg_bytes, "avg_ms": chain_ms,
                      "peak_kind": peak_kind},
