@@ -141,6 +141,8 @@ def _declare(L):
     L.fvm_problem_richards3d.argtypes = [_I, _I, _I, _D, _D, _D, _D, C.c_uint64, _D, _D, _D, _D, _D,
                                          C.POINTER(ProblemStruct)]
     L.fvm_problem_free.argtypes = [C.POINTER(ProblemStruct)]
+    L.fvm_problem_ensemble2d.argtypes = [_I, _I, _I, C.c_uint64, C.POINTER(ProblemStruct), _P]
+    L.fvm_set_members.argtypes = [_P, _I, _P]
     L.fvm_precond_info.argtypes = [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]
     L.fvm_precond_jacobian.argtypes = [_P, _P, _P, _P]
     L.fvm_profile.argtypes = [_P, _I]
@@ -191,18 +193,96 @@ class Problem:
                                          kw.get("jitter", 0.15), kw.get("seed", 1), kw.get("ln_var", 1.0),
                                          kw.get("cx", 10.0), kw.get("cy", 10.0), kw.get("cz", 2.0),
                                          kw.get("Kg", 1e-5), C.byref(self._s))
+        elif kind == "ensemble2d":
+            nmem = kw.get("n_members", 256)
+            mp = (C.c_int * (nmem + 1))()
+            r = L.fvm_problem_ensemble2d(nmem, kw.get("nmin", 2000), kw.get("nmax", 40000), kw.get("seed", 1),
+                                         C.byref(self._s), mp)
+            self.member_ptr = np.array(mp[:], dtype=np.int32)
         else:
             raise ValueError(kind)
         if r != 0:
             raise _err("problem generation", r)
         self.kind = kind
+        if kind != "ensemble2d":
+            self.member_ptr = None
 
     def __del__(self):
         try:
-            if getattr(self, "_s", None) is not None and _lib is not None:
+            if getattr(self, "_owned", True) and getattr(self, "_s", None) is not None and _lib is not None:
                 _lib.fvm_problem_free(C.byref(self._s))
         except Exception:
             pass
+
+    @classmethod
+    def from_arrays(cls, dim, coords, elem_nodes, elem_zone, bface_nodes, bface_elem, bface_tag, node_tag,
+                    zones, bcs, elem_K=None, water_table=0.0, t_end=86400.0, rho0=1000.0):
+        """a problem from host arrays (kept alive by the object)"""
+        self = cls.__new__(cls)
+        self._owned = False
+        self.kind = "arrays"
+        self.member_ptr = None
+        keep = {
+            "coords": np.ascontiguousarray(coords, np.float64).reshape(-1, 3),
+            "elem_nodes": np.ascontiguousarray(elem_nodes, np.int32),
+            "elem_zone": np.ascontiguousarray(elem_zone, np.int32),
+            "bface_nodes": np.ascontiguousarray(bface_nodes, np.int32),
+            "bface_elem": np.ascontiguousarray(bface_elem, np.int32),
+            "bface_tag": np.ascontiguousarray(bface_tag, np.int32),
+            "node_tag": np.ascontiguousarray(node_tag, np.int32),
+        }
+        if elem_K is not None:
+            keep["elem_K"] = np.ascontiguousarray(elem_K, np.float64)
+        self._zones = (Zone * len(zones))(*zones)
+        self._bcs = (BC * len(bcs))(*bcs)
+        self._keep = keep
+        s = ProblemStruct()
+        m = s.mesh
+        m.dim = dim
+        m.n_nodes = keep["coords"].shape[0]
+        m.n_elements = keep["elem_zone"].shape[0]
+        m.n_bfaces = keep["bface_tag"].shape[0]
+
+        def ptr(a, t):
+            return a.ctypes.data_as(C.POINTER(t))
+
+        m.coords = ptr(keep["coords"], C.c_double)
+        m.elem_nodes = ptr(keep["elem_nodes"], C.c_int)
+        m.elem_zone = ptr(keep["elem_zone"], C.c_int)
+        m.elem_K = ptr(keep["elem_K"], C.c_double) if "elem_K" in keep else None
+        m.bface_nodes = ptr(keep["bface_nodes"], C.c_int)
+        m.bface_elem = ptr(keep["bface_elem"], C.c_int)
+        m.bface_tag = ptr(keep["bface_tag"], C.c_int)
+        m.node_tag = ptr(keep["node_tag"], C.c_int)
+        s.phys.n_zones = len(zones)
+        s.phys.zones = C.cast(self._zones, C.POINTER(Zone))
+        s.phys.n_bcs = len(bcs)
+        s.phys.bcs = C.cast(self._bcs, C.POINTER(BC))
+        s.phys.rho0 = rho0
+        s.water_table = water_table
+        s.t_end = t_end
+        self._s = s
+        return self
+
+    def member(self, m):
+        """member m of an ensemble problem as a standalone problem"""
+        a, b = int(self.member_ptr[m]), int(self.member_ptr[m + 1])
+        arr = self.arrays()
+        d = self.mesh.dim
+        en = arr["elem_nodes"]
+        sel = (en[:, 0] >= a) & (en[:, 0] < b)
+        eidx = np.nonzero(sel)[0]
+        bf = arr["bface_nodes"]
+        bsel = (bf[:, 0] >= a) & (bf[:, 0] < b)
+        be = np.ctypeslib.as_array(self.mesh.bface_elem, (self.mesh.n_bfaces,))[bsel]
+        emap = np.full(self.n_elements, -1, np.int64)
+        emap[eidx] = np.arange(len(eidx))
+        zones = [self.phys.zones[i] for i in range(self.phys.n_zones)]
+        bcs = [self.phys.bcs[i] for i in range(self.phys.n_bcs)]
+        return Problem.from_arrays(d, arr["coords"][a:b], en[sel] - a, arr["elem_zone"][sel], bf[bsel] - a,
+                                   emap[be], arr["bface_tag"][bsel], arr["node_tag"][a:b], zones, bcs,
+                                   elem_K=arr["elem_K"][sel] if "elem_K" in arr else None,
+                                   water_table=self.water_table, t_end=self.t_end, rho0=self.phys.rho0)
 
     @property
     def mesh(self) -> Mesh:
@@ -264,6 +344,9 @@ class Physics:
     def __init__(self, problem: Problem, flags: int = 0):
         self.problem = problem
         self._c = lib().fvm_create(C.byref(problem._s.mesh), C.byref(problem._s.phys), flags)
+        if self._c and getattr(problem, "member_ptr", None) is not None:
+            mp = np.ascontiguousarray(problem.member_ptr, np.int32)
+            _check(lib().fvm_set_members(self._c, len(mp) - 1, mp.ctypes.data), "fvm_set_members")
         if not self._c:
             raise _err("fvm_create")
         self.N = problem.n_nodes
@@ -492,6 +575,8 @@ class Config:
 CONFIGS = {
     "richards2d": Config("richards2d: 81x41 jittered Delaunay, 2 layers, 1 day", "2d",
                          dict(nx=81, ny=41, Lx=10.0, Ly=5.0, jitter=0.2, seed=1)),
+    "ensemble2d": Config("ensemble2d: 256 independent 2D meshes, 2k-40k nodes each, own lognormal Ks, 1 day",
+                         "ensemble2d", dict(n_members=256, nmin=2000, nmax=40000, seed=1)),
     "richards3d": Config("richards3d: 100x100x20 hex -> 6 tets (214,221 nodes), lognormal Ks, 30 days", "3d",
                          dict(nx=100, ny=100, nz=20, Lx=100.0, Ly=100.0, Lz=20.0, jitter=0.15, seed=1,
                               ln_var=1.0, cx=10.0, cy=10.0, cz=2.0, Kg=1e-5)),

@@ -109,6 +109,72 @@ __global__ void k_err_norms(int N, int k, PhiPtrs ph, const double* __restrict__
     last_block_reduce(partial, 4, counter, out);
 }
 
+// Ensemble versions (one block per member, member m = nodes [mp[m],
+// mp[m+1])): the same updates, with the squared norms summed per member in a
+// fixed order into out[m * nq + q].
+__global__ void k_newton_update_seg(const int* __restrict__ mp, const double* __restrict__ x, double cj,
+                                    const double* __restrict__ ewt, double* __restrict__ y,
+                                    double* __restrict__ yp, double* __restrict__ e, double* out) {
+    const int m = blockIdx.x;
+    double s = 0.0;
+    for (int i = mp[m] + threadIdx.x; i < mp[m + 1]; i += blockDim.x) {
+        double d = x[i];
+        y[i] -= d;
+        yp[i] -= cj * d;
+        e[i] -= d;
+        double w = d * ewt[i];
+        s += w * w;
+    }
+    double t = block_sum(s);
+    if (threadIdx.x == 0) out[m] = t;
+}
+
+__global__ void k_err_norms_seg(const int* __restrict__ mp, int k, PhiPtrs ph, const double* __restrict__ e,
+                                const double* __restrict__ ewt, double* out) {
+    const int m = blockIdx.x;
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int i = mp[m] + threadIdx.x; i < mp[m + 1]; i += blockDim.x) {
+        double w = ewt[i], ei = e[i];
+        double a = ei * w;
+        s0 += a * a;
+        double d1 = ph.p[k][i] + ei;
+        double b = d1 * w;
+        s1 += b * b;
+        if (k >= 2) {
+            double d2 = ph.p[k - 1][i] + d1;
+            double c2 = d2 * w;
+            s2 += c2 * c2;
+        }
+        if (k + 1 < kNPhi) {
+            double d3 = ei - ph.p[k + 1][i];
+            double c3 = d3 * w;
+            s3 += c3 * c3;
+        }
+    }
+    double t0 = block_sum(s0);
+    double t1 = block_sum(s1);
+    double t2 = block_sum(s2);
+    double t3 = block_sum(s3);
+    if (threadIdx.x == 0) {
+        out[4 * m + 0] = t0;
+        out[4 * m + 1] = t1;
+        out[4 * m + 2] = t2;
+        out[4 * m + 3] = t3;
+    }
+}
+
+__global__ void k_sumsq_seg(const int* __restrict__ mp, const double* __restrict__ x,
+                            const double* __restrict__ w, double* out) {
+    const int m = blockIdx.x;
+    double s = 0.0;
+    for (int i = mp[m] + threadIdx.x; i < mp[m + 1]; i += blockDim.x) {
+        double v = x[i] * w[i];
+        s += v * v;
+    }
+    double t = block_sum(s);
+    if (threadIdx.x == 0) out[m] = t;
+}
+
 // phi_{k+1} = e (set_kp2), phi_k += e, phi_j += phi_{j+1} for j = k-1..0
 __global__ void k_phi_update(int N, int k, int set_kp2, PhiPtrs ph, const double* __restrict__ e) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -158,14 +224,26 @@ struct DeviceOps {
     DevBuf<float> feat;
     bool f_fresh = false;          // F already holds F(t, y, y')
 
+    int nm = 1;                    // ensemble members (per-member norms when > 1)
+
     DeviceOps(fvm_ctx* ctx, const fvm_opts& opts) : c(ctx), o(opts), N(ctx->N) {
         for (int j = 0; j < kNPhi; ++j) { phi[j].alloc(N); phi[j].zero(c->stream); }
         y.alloc(N); yp.alloc(N); e.alloc(N); ewt.alloc(N); F.alloc(N); x.alloc(N); tmp.alloc(N);
         partial.alloc((size_t)kRedBlocks * 4);
-        res.alloc(8);
+        nm = c->n_members;
+        res.alloc(std::max(8, 4 * nm));
         counter.alloc(1);
         counter.zero(c->stream);
-        FVM_CUDA(cudaMallocHost(&host, sizeof(double) * 8));
+        FVM_CUDA(cudaMallocHost(&host, sizeof(double) * std::max(8, 4 * nm)));
+    }
+    // largest per-member WRMS norm from per-member squared sums out[m*nq + q]
+    double member_max(int nq, int q) const {
+        double best = 0.0;
+        for (int m = 0; m < nm; ++m) {
+            const int nmem = c->h_member_ptr[m + 1] - c->h_member_ptr[m];
+            if (nmem > 0) best = std::max(best, std::sqrt(host[(size_t)m * nq + q] / nmem));
+        }
+        return best;
     }
     ~DeviceOps() {
         if (host) cudaFreeHost(host);
@@ -238,11 +316,23 @@ struct DeviceOps {
         return r;
     }
     double newton_update(double cj) {
+        if (nm > 1) {
+            fvm_launch(c, k_newton_update_seg, nm, 256, 0, c->stream, c->member_ptr.p, x.p, cj, ewt.p, y.p, yp.p,
+                       e.p, res.p);
+            fetch(nm);
+            return member_max(1, 0);
+        }
         fvm_launch(c, k_newton_update, kRedBlocks, kRedThreads, 0, c->stream, N, x.p, cj, ewt.p, y.p, yp.p, e.p,
                                                                    partial.p, counter.p, res.p);
         return std::sqrt(fetch(1) / N);
     }
     void err_norms(int k, double out[4]) {
+        if (nm > 1) {
+            fvm_launch(c, k_err_norms_seg, nm, 256, 0, c->stream, c->member_ptr.p, k, ptrs(), e.p, ewt.p, res.p);
+            fetch(4 * nm);
+            for (int q = 0; q < 4; ++q) out[q] = member_max(4, q);
+            return;
+        }
         fvm_launch(c, k_err_norms, kRedBlocks, kRedThreads, 0, c->stream, N, k, ptrs(), e.p, ewt.p, partial.p,
                                                                counter.p, res.p);
         fetch(4);
@@ -294,7 +384,14 @@ struct DeviceOps {
         launch_residual(c, y.p, tmp.p, none, nullptr, x.p);   // leaves ahh * 1 in c->stor
         fvm_launch(c, k_initial_yp, g(), 256, 0, s, N, F.p, c->stor.p, c->ntype.p, yp.p);
         fvm_launch(c, k_ewt, g(), 256, 0, s, N, y.p, o.rtol, o.atol, ewt.p);
-        double ypn = std::sqrt(reduce_sumsq(c, yp.p, ewt.p) / N);
+        double ypn;
+        if (nm > 1) {
+            fvm_launch(c, k_sumsq_seg, nm, 256, 0, s, c->member_ptr.p, yp.p, ewt.p, res.p);
+            fetch(nm);
+            ypn = member_max(1, 0);
+        } else {
+            ypn = std::sqrt(reduce_sumsq(c, yp.p, ewt.p) / N);
+        }
         double h = bdf_first_step(t0, tout, ypn, o.h0, o.hmax);
         FVM_CUDA(cudaMemcpyAsync(phi[0].p, y.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
         fvm_launch(c, k_scale_vec, g(), 256, 0, s, N, h, yp.p, phi[1].p);

@@ -1051,6 +1051,20 @@ extern "C" int fvm_jv(fvm_ctx* c, double t, double cj, const double* y, const do
     FVM_API_END
 }
 
+extern "C" int fvm_set_members(fvm_ctx* c, int n_members, const int* member_ptr) {
+    FVM_API_BEGIN
+    if (!c || !member_ptr || n_members < 1) throw Error("fvm_set_members: bad argument");
+    if (member_ptr[0] != 0 || member_ptr[n_members] != c->N) throw Error("fvm_set_members: ranges must cover the mesh");
+    for (int m = 0; m < n_members; ++m)
+        if (member_ptr[m + 1] <= member_ptr[m]) throw Error("fvm_set_members: empty or decreasing range");
+    c->n_members = n_members;
+    c->h_member_ptr.assign(member_ptr, member_ptr + n_members + 1);
+    c->member_ptr.upload(c->h_member_ptr, c->stream);
+    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    return 0;
+    FVM_API_END
+}
+
 extern "C" int fvm_autotune(fvm_ctx* c, fvm_tune_result* out) {
     FVM_API_BEGIN
     if (!c) throw Error("fvm_autotune: null context");

@@ -228,6 +228,11 @@ struct fvm_ctx {
                                      // CV surface area (learned predictor inputs)
 
     int ilu_per_sm = 1;              // block-ILU blocks per SM on large meshes
+    // ensemble of independent members (disjoint node ranges): the integrator's
+    // error and Newton tests take the largest per-member WRMS norm
+    int n_members = 1;
+    std::vector<int> h_member_ptr;
+    fvmb::DevBuf<int> member_ptr;
     fvmb::BlockILU* ilu = nullptr;
     fvmb::Krylov* kry = nullptr;
     fvmb::Predictor* pred = nullptr;

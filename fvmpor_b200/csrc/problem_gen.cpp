@@ -457,6 +457,62 @@ extern "C" int fvm_problem_richards3d(int nx, int ny, int nz, double Lx, double 
     }
 }
 
+// Ensemble of independent 2D problems as one disjoint mesh: member m has
+// N_m ~ U[nmin, nmax] nodes on the 10 m x 5 m box (nx ~ sqrt(2 N_m)), its own
+// jitter seed and its own lognormal Ks field (ln-variance ~ U[0.5, 2],
+// correlation length ~ U[0.5, 3] m), the two soil layers and the boundary
+// conditions of the 2D problem.  Node, element and boundary-face ids of the
+// members are offset so that member m owns nodes [member_ptr[m],
+// member_ptr[m+1]); elements and faces never couple two members.
+extern "C" int fvm_problem_ensemble2d(int n_members, int nmin, int nmax, uint64_t seed, fvm_problem* out,
+                                      int* member_ptr) {
+    try {
+        if (n_members < 1 || nmin < 16 || nmax < nmin || !out || !member_ptr)
+            throw Error("fvm_problem_ensemble2d: bad arguments");
+        Rng rng(seed);
+        std::vector<double> coords, eK;
+        std::vector<int> en, ez, bn, be, bt, nt;
+        std::vector<fvm_zone> zones;
+        std::vector<fvm_bc> bcs;
+        member_ptr[0] = 0;
+        for (int m = 0; m < n_members; ++m) {
+            const double target = nmin + (nmax - nmin) * rng.uniform();
+            const int nx = std::max(3, (int)std::lround(std::sqrt(2.0 * target)));
+            const int ny = std::max(3, (int)std::lround(target / nx));
+            const double ln_var = 0.5 + 1.5 * rng.uniform();
+            const double corr = 0.5 + 2.5 * rng.uniform();
+            const uint64_t ms = rng.next();
+            fvm_problem pm;
+            if (fvm_problem_richards2d(nx, ny, 10.0, 5.0, 0.2, ms, ln_var, corr, &pm) != 0)
+                throw Error("fvm_problem_ensemble2d: member generation failed");
+            const int n0 = (int)(coords.size() / 3), e0 = (int)ez.size();
+            const fvm_mesh& mm = pm.mesh;
+            coords.insert(coords.end(), mm.coords, mm.coords + 3 * (size_t)mm.n_nodes);
+            for (int q = 0; q < 3 * mm.n_elements; ++q) en.push_back(mm.elem_nodes[q] + n0);
+            ez.insert(ez.end(), mm.elem_zone, mm.elem_zone + mm.n_elements);
+            if (mm.elem_K) eK.insert(eK.end(), mm.elem_K, mm.elem_K + mm.n_elements);
+            else for (int e = 0; e < mm.n_elements; ++e) eK.push_back(pm.zones[mm.elem_zone[e]].Kxx);
+            for (int q = 0; q < 2 * mm.n_bfaces; ++q) bn.push_back(mm.bface_nodes[q] + n0);
+            for (int q = 0; q < mm.n_bfaces; ++q) be.push_back(mm.bface_elem[q] + e0);
+            bt.insert(bt.end(), mm.bface_tag, mm.bface_tag + mm.n_bfaces);
+            nt.insert(nt.end(), mm.node_tag, mm.node_tag + mm.n_nodes);
+            if (m == 0) {
+                zones.assign(pm.zones, pm.zones + pm.phys.n_zones);
+                bcs.assign(pm.bcs, pm.bcs + pm.phys.n_bcs);
+            }
+            member_ptr[m + 1] = n0 + mm.n_nodes;
+            fvm_problem_free(&pm);
+        }
+        finish_problem(out, 2, coords, en, ez, eK, bn, be, bt, nt, zones, bcs, (int)(coords.size() / 3), 1, 1);
+        out->water_table = 0.0;
+        out->t_end = 86400.0;
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
 extern "C" void fvm_problem_free(fvm_problem* p) {
     if (!p) return;
     std::free(p->coords); std::free(p->elem_nodes); std::free(p->elem_zone); std::free(p->elem_K);

@@ -231,6 +231,14 @@ int fvm_wrms_noalloc(const double* x, const double* ewt, long n,
  * current choice.  No counterpart in the reference, whose residual is a
  * fixed sequence of cuSPARSE SpMVs (fvmpor.h:948-1124). */
 int fvm_autotune(fvm_ctx* ctx, fvm_tune_result* out);
+/* Ensemble of independent problems in one context: member m owns nodes
+ * [member_ptr[m], member_ptr[m+1]) (host array of n_members + 1 entries,
+ * 0 .. n_nodes, no coupling between members).  The integrator's Newton
+ * and error tests then use the largest per-member WRMS norm, so every
+ * member meets the tolerances on its own; the residual, preconditioner
+ * and Krylov kernels run over all members in the same launches.  No
+ * counterpart in the reference (one mesh per run). */
+int fvm_set_members(fvm_ctx* ctx, int n_members, const int* member_ptr);
 /* Block-ILU partition on large meshes: per_sm (1..16) blocks per SM.  Fewer,
  * larger blocks couple more nodes inside the factor (fewer Krylov
  * iterations); more, smaller ones shorten the level chains of the
@@ -354,6 +362,13 @@ int fvm_problem_richards3d(int nx, int ny, int nz, double Lx, double Ly,
                            double Lz, double jitter, uint64_t seed,
                            double ln_var, double cx, double cy, double cz,
                            double Kg, fvm_problem* out);
+/* Ensemble: n_members independent 2D problems (node counts uniform in
+ * [nmin, nmax], each with its own jitter and lognormal Ks field: ln-variance
+ * uniform in [0.5, 2], correlation length uniform in [0.5, 3] m) as one
+ * disjoint mesh; member m owns nodes [member_ptr[m], member_ptr[m+1])
+ * (member_ptr has n_members + 1 entries, caller-allocated). */
+int fvm_problem_ensemble2d(int n_members, int nmin, int nmax, uint64_t seed,
+                           fvm_problem* out, int* member_ptr);
 void fvm_problem_free(fvm_problem* p);
 
 #ifdef __cplusplus
