@@ -125,14 +125,9 @@ def dist_setup():
 
 
 def max_over_ranks(x, ws, dev):
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from fvmpor_b200.replicas import max_over_ranks as mor
 
-    t = torch.tensor([x], dtype=torch.float64, device=dev)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return x if ws == 1 else mor(x, dev)
 
 
 def barrier(ws):
@@ -314,7 +309,9 @@ def main():
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    prob = fb.make_problem("richards3d", seed=1 + rank)
+    from fvmpor_b200.replicas import job_throughput, replica_seed
+
+    prob = fb.make_problem("richards3d", seed=replica_seed(1, rank))
     horizon = args.days * 86400.0
     ph = fb.Physics(prob)
     N, T = prob.n_nodes, prob.n_elements
@@ -370,11 +367,10 @@ def main():
     ms_plain, st_plain, _ = timed(plain, k_extra)
     y_plain = yend.clone()
     ms_e2e, _, _ = timed(learned, k_extra, host=True)
-    sim = horizon * args.steps * ws
-    value = sim / (ms_learn / 1e3)
-    mixed_value = horizon * k_extra * ws / (ms_mixed / 1e3)
-    plain_value = horizon * k_extra * ws / (ms_plain / 1e3)
-    e2e_value = horizon * k_extra * ws / (ms_e2e / 1e3)
+    value = job_throughput(horizon * args.steps, ws, ms_learn / 1e3)
+    mixed_value = job_throughput(horizon * k_extra, ws, ms_mixed / 1e3)
+    plain_value = job_throughput(horizon * k_extra, ws, ms_plain / 1e3)
+    e2e_value = job_throughput(horizon * k_extra, ws, ms_e2e / 1e3)
     head_diff = float((y_learn - y_plain).abs().max() / y_plain.abs().max())
 
     # roofline of the residual evaluation (node pass + element pass + gather):
