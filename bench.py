@@ -181,7 +181,7 @@ def train_predictor(fb, torch, dev, seed, horizon):
     X = torch.zeros((cap, 8), dtype=torch.float32, device=dev)
     Y = torch.zeros(cap, dtype=torch.float32, device=dev)
     rec = fb.Integrator(pht, krylov_dim=40, max_restarts=5, precision=0, max_order=5)
-    rc, st, cnt = rec.integrate_record(0.0, horizon, y0, ye, X, Y, stride=211)
+    rc, st, cnt = rec.integrate_record(0.0, horizon, y0, ye, X, Y, stride=29)
     if rc != 0 or cnt < 1000:
         raise RuntimeError(f"training trajectory failed rc={rc} samples={cnt}")
     t_rec = time.perf_counter() - t0
@@ -284,7 +284,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--days", type=float, default=30.0)
@@ -347,18 +347,21 @@ def main():
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         c1 = ph.counters()
-        prof = ph.profile_read() if profile else None
+        prof = ph.profile_read() if profile else {}
         if profile:
             ph.profile(False)
-            prof["_launches"] = (0.0, c1["launches"] - c0["launches"])
+        prof["_launches"] = (0.0, c1["launches"] - c0["launches"])
         barrier(ws)
         return max_over_ranks(ms, ws, dev), stats, prof
 
     for _ in range(args.warmup):
         learned.integrate(0.0, horizon, y0, yend)
     with ClockSampler(local) as clk:
-        ms_learn, st_learn, prof = timed(learned, args.steps, profile=True)
+        ms_learn, st_learn, cnt = timed(learned, args.steps)
     y_learn = yend.clone()
+    # per-kernel CUDA-event profile on one more run outside the timed region
+    # (the events themselves slow the run down)
+    _, _, prof = timed(learned, 1, profile=True)
     # the comparison paths and the host-buffer path are timed on fewer runs
     # (each run is a whole 30-day integration) to keep the bench short
     k_extra = max(1, args.steps // 2)
@@ -414,7 +417,7 @@ def main():
     }
     # every kernel launch of the library inside the timed region (counted by
     # the context: residual chain, Krylov, preconditioner, controller)
-    line["gpu_launches"] = int(prof.pop("_launches")[1])
+    line["gpu_launches"] = int(cnt["_launches"][1])
     line["kernel_ms"].pop("_launches", None)
     if rank == 0 and not args.no_cpu_baseline:
         v, wall, msteps, st = cpu_sample(15.0)

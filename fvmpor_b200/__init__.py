@@ -93,7 +93,7 @@ class Opts(C.Structure):
     _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("max_order", C.c_int),
                 ("krylov_dim", C.c_int), ("max_restarts", C.c_int), ("precision", C.c_int),
                 ("use_predictor", C.c_int), ("h0", C.c_double), ("hmax", C.c_double),
-                ("max_steps", C.c_long)]
+                ("max_steps", C.c_long), ("eps_lin", C.c_double)]
 
 
 class Stats(C.Structure):
@@ -162,7 +162,8 @@ def _declare(L):
                                        _I, C.POINTER(C.c_long)]
 
 
-PROFILE_CATEGORIES = ("node", "element", "gather", "ilu_apply", "gram_schmidt", "ilu_factor", "fd_jacobian")
+PROFILE_CATEGORIES = ("node", "element", "gather", "ilu_apply", "gram_schmidt", "ilu_factor", "fd_jacobian",
+                      "mlp", "learned_attempt")
 
 
 def _err(prefix, code=None):

@@ -419,6 +419,7 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
     bo.max_order = o.max_order;
     bo.hmax = o.hmax;
     bo.use_guess = o.use_predictor != 0;
+    if (o.eps_lin > 0.0) bo.eps_lin = o.eps_lin;
     BdfController<DeviceOps> ctl(ops, bo);
     long nre0 = c->n_residuals;
     double h0 = ops.start(t0, y0, t_end);
@@ -463,6 +464,7 @@ extern "C" void fvm_opts_default(fvm_opts* o) {
     o->max_order = 5;
     o->krylov_dim = 30;
     o->max_restarts = 5;
+    o->eps_lin = 5e-4;
 }
 
 extern "C" int fvm_integrate(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end,

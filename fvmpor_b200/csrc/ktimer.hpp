@@ -19,8 +19,10 @@ enum TimerCat {
     TM_ILU_APPLY = 3, // block-ILU(0) forward/backward
     TM_CGS = 4,       // Gram-Schmidt passes
     TM_ILU_FACTOR = 5,
-    TM_FD_JAC = 6,    // coloured finite-difference Jacobian (whole set-up)
-    TM_NCAT = 7
+    TM_FD_JAC = 6,    // finite-difference Jacobian (whole set-up)
+    TM_MLP = 7,       // learned iterate: features + network forward
+    TM_PRED = 8,      // learned iterate: the whole attempt (residuals, test, blend)
+    TM_NCAT = 9
 };
 
 struct KernelTimer {

@@ -625,8 +625,15 @@ bool predictor_apply(fvm_ctx* c, Predictor* p, double rtol, double atol, double 
                      const double* h_prev, const double* ypred, const double* yppred, double* y, double* yp,
                      double* e, double* F) {
     const int N = c->N;
+    c->tm.begin(TM_PRED, c->stream);
+    struct EndTimer {
+        fvm_ctx* c;
+        ~EndTimer() { c->tm.end(TM_PRED, c->stream); }
+    } end_timer{c};
+    c->tm.begin(TM_MLP, c->stream);
     predictor_features(c, h_n, h_prev, ypred, dt, p->X.p);
     predictor_forward(c, p, p->X.p, N, p->out.p);
+    c->tm.end(TM_MLP, c->stream);
     fvm_launch(c, k_apply_guess, grid_for(N, 256), 256, 0, c->stream, N, p->out.p, ypred, yppred, h_n, c->ntype.p,
                rtol, atol, cj, p->yg.p, p->ypg.p);
     Perturb none;

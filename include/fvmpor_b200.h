@@ -196,9 +196,10 @@ double fvm_dot(fvm_ctx* ctx, const double* x, const double* y);
  * preconditioner time_J/time_M/time_apply accumulators, preconditioner_dss.
  * cpp:297-373).  fvm_profile(ctx, 1) resets and starts, (ctx, 0) stops;
  * fvm_profile_read fills FVM_PROF_NCAT milliseconds / launch counts in
- * the order node pass, element pass, node gather, ILU apply, Gram-Schmidt,
- * ILU factor, FD Jacobian. */
-#define FVM_PROF_NCAT 7
+ * the order node pass, element pass, node gather, ILU apply, Gram-Schmidt
+ * (with the Givens update), ILU factor, FD Jacobian, learned-iterate
+ * network (features + forward), learned-iterate attempt (all of it). */
+#define FVM_PROF_NCAT 9
 int fvm_profile(fvm_ctx* ctx, int enable);
 int fvm_profile_read(fvm_ctx* ctx, double* ms, long* counts);
 
@@ -269,6 +270,12 @@ typedef struct {
     double h0;               /* first step, 0 = automatic                  */
     double hmax;             /* 0 = unbounded                              */
     long max_steps;
+    double eps_lin;          /* Krylov tolerance factor: GMRES stops at
+                                eps_lin * 0.33 weighted units (IDA's
+                                epslin); default and 0: 5e-4, tighter
+                                than IDA's 0.05 because block-ILU(0) is
+                                far weaker than the reference's direct
+                                factorisation                            */
 } fvm_opts;
 
 typedef struct {

@@ -1103,6 +1103,7 @@ int orc_integrate(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, doub
     bo.atol = opts->atol;
     bo.max_order = opts->max_order;
     bo.hmax = opts->hmax;
+    if (opts->eps_lin > 0.0) bo.eps_lin = opts->eps_lin;
     fvmb::BdfController<CpuOps> ctl(ops, bo);
     long nre0 = o->n_res;
     std::fill(o->w_front.begin(), o->w_front.end(), 0.5);   // averaged weights before step 1
