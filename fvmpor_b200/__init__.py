@@ -89,11 +89,22 @@ class ProblemStruct(C.Structure):
     ]
 
 
+class PmeshStruct(C.Structure):
+    _fields_ = [("n_dom", C.c_int), ("dom_id", C.c_int), ("dim", C.c_int), ("n_nodes", C.c_int),
+                ("n_elements", C.c_int), ("n_bfaces", C.c_int), ("coords", C.POINTER(C.c_double)),
+                ("elem_nodes", C.POINTER(C.c_int)), ("elem_tag", C.POINTER(C.c_int)),
+                ("bface_nodes", C.POINTER(C.c_int)), ("bface_elem", C.POINTER(C.c_int)),
+                ("bface_tag", C.POINTER(C.c_int)), ("node_bc_ptr", C.POINTER(C.c_int)),
+                ("node_bc", C.POINTER(C.c_int)), ("perm", C.POINTER(C.c_int)), ("bandwidth_file", C.c_int),
+                ("bandwidth", C.c_int)]
+
+
 class Opts(C.Structure):
     _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("max_order", C.c_int),
                 ("krylov_dim", C.c_int), ("max_restarts", C.c_int), ("precision", C.c_int),
                 ("use_predictor", C.c_int), ("h0", C.c_double), ("hmax", C.c_double),
-                ("max_steps", C.c_long), ("eps_lin", C.c_double)]
+                ("max_steps", C.c_long), ("eps_lin", C.c_double), ("cj_refresh", C.c_double),
+                ("psetup_age", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -143,6 +154,12 @@ def _declare(L):
     L.fvm_problem_free.argtypes = [C.POINTER(ProblemStruct)]
     L.fvm_problem_ensemble2d.argtypes = [_I, _I, _I, C.c_uint64, C.POINTER(ProblemStruct), _P]
     L.fvm_set_members.argtypes = [_P, _I, _P]
+    L.fvm_pmesh_read.argtypes = [C.c_char_p, _I, C.POINTER(PmeshStruct)]
+    L.fvm_pmesh_write.argtypes = [C.c_char_p, C.POINTER(PmeshStruct)]
+    L.fvm_pmesh_free.argtypes = [C.POINTER(PmeshStruct)]
+    L.fvm_problem_from_pmesh.argtypes = [C.POINTER(PmeshStruct), _I, C.POINTER(Zone), _I, C.POINTER(BC), _D,
+                                         C.POINTER(ProblemStruct)]
+    L.fvm_write_vtu.argtypes = [C.c_char_p, _I, _I, _I, C.POINTER(Mesh), _P]
     L.fvm_precond_info.argtypes = [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]
     L.fvm_precond_jacobian.argtypes = [_P, _P, _P, _P]
     L.fvm_profile.argtypes = [_P, _I]
@@ -264,6 +281,35 @@ class Problem:
         s.t_end = t_end
         self._s = s
         return self
+
+    @classmethod
+    def from_pmesh(cls, mesh, zones, bcs, rho0=1000.0, t_end=0.0, rcm=True):
+        """a problem on a .pmesh mesh (a path or a Pmesh): zones indexed by
+        the element's physical tag - 100, Dirichlet node tags from the
+        boundary conditions (fvm_problem_from_pmesh)"""
+        pm = mesh if isinstance(mesh, Pmesh) else read_pmesh(mesh, rcm=rcm)
+        self = cls.__new__(cls)
+        self._s = ProblemStruct()
+        zs = (Zone * len(zones))(*zones)
+        bs = (BC * max(1, len(bcs)))(*bcs)
+        r = lib().fvm_problem_from_pmesh(C.byref(pm._s), len(zones), zs, len(bcs), bs, rho0, C.byref(self._s))
+        if r != 0:
+            self._s = None
+            raise _err("fvm_problem_from_pmesh", r)
+        self._s.t_end = t_end
+        self.kind = "pmesh"
+        self.member_ptr = None
+        self.pmesh = pm
+        return self
+
+    def write_vtu(self, stem, step, head, rank=0, n_ranks=1):
+        """VTK XML output of a head field (<stem>_dom<rank>_<step>.vtu and,
+        on rank 0, <stem>_head_<step>.pvtu)"""
+        h = np.ascontiguousarray(np.asarray(head, dtype=np.float64))
+        if h.shape != (self.n_nodes,):
+            raise ValueError(f"head must have {self.n_nodes} values")
+        _check(lib().fvm_write_vtu(str(stem).encode(), step, rank, n_ranks, C.byref(self._s.mesh),
+                                   h.ctypes.data), "fvm_write_vtu")
 
     def member(self, m):
         """member m of an ensemble problem as a standalone problem"""
@@ -571,6 +617,99 @@ class Config:
     name: str
     kind: str
     params: dict
+
+
+class Pmesh:
+    """A .pmesh mesh read by the library (fvm_pmesh_read); the arrays are
+    numpy views of library-owned memory, released with the object."""
+
+    def __init__(self, s: PmeshStruct):
+        self._s = s
+        d = s.dim
+        n, ne, nb = s.n_nodes, s.n_elements, s.n_bfaces
+
+        def view(p, shape):
+            return np.ctypeslib.as_array(p, shape) if int(np.prod(shape)) > 0 else np.zeros(shape, np.int32)
+
+        self.dim, self.n_nodes, self.n_elements, self.n_bfaces = d, n, ne, nb
+        self.coords = view(s.coords, (n, 3))
+        self.elem_nodes = view(s.elem_nodes, (ne, d + 1))
+        self.elem_tag = view(s.elem_tag, (ne,))
+        self.bface_nodes = view(s.bface_nodes, (nb, d))
+        self.bface_elem = view(s.bface_elem, (nb,))
+        self.bface_tag = view(s.bface_tag, (nb,))
+        self.node_bc_ptr = view(s.node_bc_ptr, (n + 1,))
+        self.node_bc = view(s.node_bc, (int(self.node_bc_ptr[-1]),))
+        self.perm = view(s.perm, (n,))
+        self.bandwidth_file, self.bandwidth = s.bandwidth_file, s.bandwidth
+
+    @classmethod
+    def from_problem(cls, problem: "Problem"):
+        """the mesh of a problem as a Pmesh (physical tag = zone, node
+        boundary tags = the Dirichlet node tags), e.g. to write it as a
+        .pmesh file; the arrays belong to the object"""
+        a = problem.arrays()
+        m = problem.mesh
+        nt = np.ascontiguousarray(a["node_tag"], np.int32)
+        keep = {
+            "coords": np.ascontiguousarray(a["coords"], np.float64),
+            "elem_nodes": np.ascontiguousarray(a["elem_nodes"], np.int32),
+            "elem_tag": np.ascontiguousarray(a["elem_zone"], np.int32),
+            "bface_nodes": np.ascontiguousarray(a["bface_nodes"], np.int32),
+            "bface_elem": np.ascontiguousarray(np.ctypeslib.as_array(m.bface_elem, (m.n_bfaces,)), np.int32),
+            "bface_tag": np.ascontiguousarray(a["bface_tag"], np.int32),
+            "node_bc_ptr": np.concatenate([[0], np.cumsum(nt != 0)]).astype(np.int32),
+            "node_bc": np.ascontiguousarray(nt[nt != 0], np.int32),
+            "perm": np.arange(m.n_nodes, dtype=np.int32),
+        }
+        s = PmeshStruct()
+        s.n_dom, s.dom_id, s.dim = 1, 0, m.dim
+        s.n_nodes, s.n_elements, s.n_bfaces = m.n_nodes, m.n_elements, m.n_bfaces
+        for k, v in keep.items():
+            setattr(s, k, v.ctypes.data_as(C.POINTER(C.c_double if v.dtype == np.float64 else C.c_int)))
+        self = cls(s)
+        self._owned_arrays = keep
+        return self
+
+    def write(self, path):
+        _check(lib().fvm_pmesh_write(str(path).encode(), C.byref(self._s)), "fvm_pmesh_write")
+
+    def __del__(self):
+        try:
+            if getattr(self, "_owned_arrays", None) is not None:
+                return
+            if _lib is not None and getattr(self, "_s", None) is not None:
+                _lib.fvm_pmesh_free(C.byref(self._s))
+                self._s = None
+        except Exception:
+            pass
+
+
+def read_pmesh(path, rcm=True) -> Pmesh:
+    """reads a one-domain .pmesh of triangles or tetrahedra; rcm renumbers
+    the nodes by reverse Cuthill-McKee as the reference's Mesh does"""
+    s = PmeshStruct()
+    r = lib().fvm_pmesh_read(str(path).encode(), FVM_PMESH_RCM if rcm else 0, C.byref(s))
+    if r != 0:
+        raise _err(f"fvm_pmesh_read({path})", r)
+    return Pmesh(s)
+
+
+FVM_PMESH_RCM = 1
+
+
+def cassion_physics():
+    """zones and boundary conditions of the reference's caisson
+    infiltration problem (examples/fvmporMinlin/cassion.h:36-116; the EEM
+    example uses the same file): four van Genuchten zones with K =
+    rho0 g / mu * k, no-flow tag 1, inflow of 2.3148e-7 m/s on tag 2
+    (prescribed flux, positive outwards), uniform initial head -7.34 m"""
+    factor = 1000.0 * 9.80665 / 1e-3
+    rows = [(9.33e-12, 0.368, 3.34, 1.982, 0.2771), (5.55e-12, 0.3510, 3.63, 1.632, 0.2806),
+            (4.898e-12, 0.3250, 3.45, 1.573, 0.2643), (4.898e-11, 0.3250, 3.45, 1.573, 0.2643)]
+    zones = [Zone(factor * k, factor * k, factor * k, phi, a, n, sr) for k, phi, a, n, sr in rows]
+    bcs = [BC(1, 3, 0.0, 0.0, 0.0), BC(2, 3, -2.3148e-7, 0.0, 0.0)]
+    return zones, bcs, -7.34
 
 
 CONFIGS = {

@@ -420,6 +420,8 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
     bo.hmax = o.hmax;
     bo.use_guess = o.use_predictor != 0;
     if (o.eps_lin > 0.0) bo.eps_lin = o.eps_lin;
+    if (o.cj_refresh > 1.0) bo.cj_refresh = o.cj_refresh;
+    if (o.psetup_age > 0) bo.psetup_age = o.psetup_age;
     BdfController<DeviceOps> ctl(ops, bo);
     long nre0 = c->n_residuals;
     double h0 = ops.start(t0, y0, t_end);
@@ -465,6 +467,8 @@ extern "C" void fvm_opts_default(fvm_opts* o) {
     o->krylov_dim = 30;
     o->max_restarts = 5;
     o->eps_lin = 5e-4;
+    o->cj_refresh = 1.05;
+    o->psetup_age = 1;
 }
 
 extern "C" int fvm_integrate(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end,

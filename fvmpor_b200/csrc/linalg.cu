@@ -201,12 +201,13 @@ __device__ __forceinline__ void block_reduce_all(const double* partial, int nv, 
 
 constexpr int kCgsThreads = 512;
 
-// block-local dot products <U_i, W> over rows [k0, k1) for i < nv: the
-// warps split the (vector, row segment) pairs, the segments of a vector are
-// then summed in segment order.  Row nv of the output (when with_norm) is
-// sum W^2.  out[i] is valid in every thread after the call.
+// block-local dot products <U_i, W> over rows [k0, k1) for i < nv, with the
+// block's W rows in shared memory (Wl[k - k0]): the warps split the
+// (vector, row segment) pairs, the segments of a vector are then summed in
+// segment order.  Row nv of the output (when with_norm) is sum W^2.  out[i]
+// is valid in every thread after the call.
 template <class B>
-__device__ __forceinline__ void block_dots(const B* __restrict__ U, size_t ld, const double* __restrict__ W, int k0,
+__device__ __forceinline__ void block_dots(const B* __restrict__ U, size_t ld, const double* __restrict__ Wl, int k0,
                                            int k1, int nv, bool with_norm, double* seg_sums, double* out) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int nvec = nv + (with_norm ? 1 : 0);
@@ -218,9 +219,9 @@ __device__ __forceinline__ void block_dots(const B* __restrict__ U, size_t ld, c
         double sacc = 0.0;
         if (i < nv) {
             const B* Ui = U + ld * i;
-            for (int k = a + lane; k < b; k += 32) sacc += ldb(Ui, k) * W[k];
+            for (int k = a + lane; k < b; k += 32) sacc += ldb(Ui, k) * Wl[k - k0];
         } else {
-            for (int k = a + lane; k < b; k += 32) sacc += W[k] * W[k];
+            for (int k = a + lane; k < b; k += 32) sacc += Wl[k - k0] * Wl[k - k0];
         }
         sacc = warp_sum(sacc);
         if (lane == 0) seg_sums[idx] = sacc;
@@ -257,6 +258,8 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
                                                               double* __restrict__ H, double* __restrict__ cs,
                                                               double* __restrict__ sn, double* __restrict__ g) {
     __shared__ double ca[64], cb[64], seg[64];
+    extern __shared__ double Ws[];   // this block's rows of W (the vector being orthogonalised)
+    (void)W;
     if (st->done) return;            // the device-driven loop has finished
     const int j = st->j, nv = j + 1, m = st->m;
     const int nblk = gridDim.x;
@@ -265,9 +268,9 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
     double* pa = partial;
     double* pb = partial + (size_t)nblk * 64;
     // pass 1: a = U^T W
-    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) W[k] = ewt[k] * Jv[k];
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) Ws[k - k0] = ewt[k] * Jv[k];
     __syncthreads();
-    block_dots(U, ld, W, k0, k1, nv, false, seg, ca);
+    block_dots(U, ld, Ws, k0, k1, nv, false, seg, ca);
     for (int i = threadIdx.x; i < nv; i += blockDim.x) pa[(size_t)blockIdx.x * nv + i] = ca[i];
     if (!grid_barrier(bar, bar + 1, err)) return;
     block_reduce_all(pa, nv, nblk, ca);
@@ -276,11 +279,12 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
     // pass 2: W' = W - U diag(s^2) a; b = U^T W', ||W'||^2
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
         double acc = 0.0;
+#pragma unroll 8
         for (int i = 0; i < nv; ++i) acc += cb[i] * ldb(U + ld * i, k);
-        W[k] = W[k] - acc;
+        Ws[k - k0] = Ws[k - k0] - acc;
     }
     __syncthreads();
-    block_dots(U, ld, W, k0, k1, nv, true, seg, cb);
+    block_dots(U, ld, Ws, k0, k1, nv, true, seg, cb);
     for (int i = threadIdx.x; i <= nv; i += blockDim.x) pb[(size_t)blockIdx.x * (nv + 1) + i] = cb[i];
     if (!grid_barrier(bar, bar + 1, err)) return;
     block_reduce_all(pb, nv + 1, nblk, cb);
@@ -298,8 +302,9 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
     B* Un = U + ld * nv;
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
         double acc = 0.0;
+#pragma unroll 8
         for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
-        const B u = (B)(W[k] - acc);
+        const B u = (B)(Ws[k - k0] - acc);
         Un[k] = u;
         t_next[k] = snv * (double)u / ewt[k];
     }
@@ -437,8 +442,10 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
             FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<float>, kCgsThreads, 0));
         else
             FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<double>, kCgsThreads, 0));
-        // one block per SM: fewer arrivals at each grid barrier
-        K->coop_grid = (coop && per_sm > 0 && m + 1 <= 63) ? nsm : 0;
+        // one block per SM: fewer arrivals at each grid barrier; the block's
+        // rows of W (at most 48 KB) live in its shared memory
+        const size_t wsm = sizeof(double) * (size_t)((c->N + nsm - 1) / nsm);
+        K->coop_grid = (coop && per_sm > 0 && m + 1 <= 63 && wsm <= 48 * 1024) ? nsm : 0;
     }
     K->res.alloc(3 * (m + 2) + 8);
     K->sigma.alloc(1);
@@ -577,8 +584,9 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                     double* sgp = K->sigma.p;
                     void* args[] = {&Ni, &stp, &Ub, &ldv, &scp, &jvp, &ew, &Wp, &pp, &bp, &ep, &tp, &sgp,
                                     &H_d, &cs_d, &sn_d, &g_d};
+                    const size_t wsm = sizeof(double) * (size_t)((N + K->coop_grid - 1) / K->coop_grid);
                     FVM_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi_cgs2<B>, dim3(K->coop_grid),
-                                                         dim3(kCgsThreads), args, 0, s));
+                                                         dim3(kCgsThreads), args, wsm, s));
                     c->launches++;
                     c->tm.end(TM_CGS, s);
                 }

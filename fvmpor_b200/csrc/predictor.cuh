@@ -41,7 +41,7 @@ void predictor_forward(fvm_ctx* c, Predictor* p, const float* X, int n, float* o
 // Replaces the Newton starting point (y, y', e) with the network's guess
 // y_pred + a w MLP, a in (0, 1] the minimiser of the residual norm along
 // the learned direction (linearised from the residuals at both ends), when
-// that lowers the BDF predictor's residual.  ypred/yppred hold the BDF
+// that at least halves the BDF predictor's residual norm.  ypred/yppred hold the BDF
 // predictor; F receives the residual of the kept iterate.  Returns true when
 // the learned iterate was kept.
 bool predictor_apply(fvm_ctx* c, Predictor* p, double rtol, double atol, double dt, double cj,

@@ -276,6 +276,11 @@ typedef struct {
                                 than IDA's 0.05 because block-ILU(0) is
                                 far weaker than the reference's direct
                                 factorisation                            */
+    double cj_refresh;       /* new preconditioner when cj moved by more
+                                than this factor since the last set-up
+                                (0 = 1.05)                               */
+    int psetup_age;          /* ... or after this many steps (0 = 1:
+                                every step)                              */
 } fvm_opts;
 
 typedef struct {
@@ -377,6 +382,61 @@ int fvm_problem_richards3d(int nx, int ny, int nz, double Lx, double Ly,
 int fvm_problem_ensemble2d(int n_members, int nmin, int nmax, uint64_t seed,
                            fvm_problem* out, int* member_ptr);
 void fvm_problem_free(fvm_problem* p);
+
+/* ------------------------------------------------------------------ */
+/* Mesh files and output.                                               */
+/* ------------------------------------------------------------------ */
+/* A .pmesh mesh (the text format Mesh::read_mesh_data parses,
+ * src/fvm/mesh.cpp:102-366) of triangles or tetrahedra, single domain.
+ * elem_tag is the file's physical tag minus 100 (mesh.cpp:288), the index
+ * of the element's zone.  Boundary faces are the element faces with a
+ * non-zero boundary id, in element order.  Node boundary tags are kept as
+ * CSR (node_bc_ptr[n_nodes + 1], node_bc).  With FVM_PMESH_RCM the nodes
+ * are renumbered by reverse Cuthill-McKee as Mesh::reorder_nodes_edges does
+ * (mesh.cpp:116-148); perm[new] = the node's index in the file.  Arrays
+ * are malloc'd by the library and released with fvm_pmesh_free. */
+#define FVM_PMESH_RCM 1
+typedef struct {
+    int n_dom, dom_id;       /* header: domain count and this domain's id  */
+    int dim;                 /* 2 triangles, 3 tetrahedra                  */
+    int n_nodes, n_elements, n_bfaces;
+    double* coords;          /* [n_nodes][3]                               */
+    int* elem_nodes;         /* [n_elements][dim+1]                        */
+    int* elem_tag;           /* [n_elements]                               */
+    int* bface_nodes;        /* [n_bfaces][dim]                            */
+    int* bface_elem;         /* [n_bfaces]                                 */
+    int* bface_tag;          /* [n_bfaces], > 0                            */
+    int* node_bc_ptr;        /* [n_nodes + 1]                              */
+    int* node_bc;            /* node boundary tags                         */
+    int* perm;               /* [n_nodes] new -> file node index           */
+    int bandwidth_file;      /* node-graph bandwidth in file order         */
+    int bandwidth;           /* ... in the returned order                  */
+} fvm_pmesh;
+
+/* 0 ok; -1 I/O, -2 malformed file (fvm_last_error gives file:line),
+ * -3 halo nodes (multi-domain file), -4 element type other than triangle
+ * or tetrahedron.  Replaces Mesh::Mesh's file reading (mesh.cpp:70-80). */
+int fvm_pmesh_read(const char* path, int flags, fvm_pmesh* out);
+/* writes m as a one-domain .pmesh (node_bc_ptr may be NULL: no tags) */
+int fvm_pmesh_write(const char* path, const fvm_pmesh* m);
+void fvm_pmesh_free(fvm_pmesh* m);
+/* A problem on a .pmesh mesh: element zone = elem_tag (0 <= tag < n_zones,
+ * as physical_zone() asserts, fvmpor.h:1128-1132); node_tag = the node's
+ * last boundary tag whose condition is Dirichlet (types 1, 4), as
+ * VarSatPhysicsImpl::initialise_vectors sets is_dirichlet_h_vec_
+ * (fvmpor.h:405-417).  Every boundary-face tag must have a condition.
+ * Release with fvm_problem_free. */
+int fvm_problem_from_pmesh(const fvm_pmesh* m, int n_zones, const fvm_zone* zones,
+                           int n_bcs, const fvm_bc* bcs, double rho0,
+                           fvm_problem* out);
+
+/* VTK XML output of a head field (host array, n_nodes values) as
+ * <stem>_dom<rank>_<step>.vtu and, from rank 0, the header
+ * <stem>_head_<step>.pvtu naming n_ranks pieces: the files
+ * util::Solution::write_timestep_VTK_XML writes (include/util/solution.h:
+ * 175-357). */
+int fvm_write_vtu(const char* stem, int step, int rank, int n_ranks,
+                  const fvm_mesh* mesh, const double* head);
 
 #ifdef __cplusplus
 }

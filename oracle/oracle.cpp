@@ -1104,6 +1104,8 @@ int orc_integrate(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, doub
     bo.max_order = opts->max_order;
     bo.hmax = opts->hmax;
     if (opts->eps_lin > 0.0) bo.eps_lin = opts->eps_lin;
+    if (opts->cj_refresh > 1.0) bo.cj_refresh = opts->cj_refresh;
+    if (opts->psetup_age > 0) bo.psetup_age = opts->psetup_age;
     fvmb::BdfController<CpuOps> ctl(ops, bo);
     long nre0 = o->n_res;
     std::fill(o->w_front.begin(), o->w_front.end(), 0.5);   // averaged weights before step 1
