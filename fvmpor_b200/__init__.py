@@ -99,6 +99,11 @@ class PmeshStruct(C.Structure):
                 ("bandwidth", C.c_int)]
 
 
+class StepRecord(C.Structure):
+    _fields_ = [("t", C.c_double), ("h", C.c_double), ("err", C.c_double), ("order", C.c_int),
+                ("attempts", C.c_int), ("nni", C.c_int), ("nli", C.c_int), ("npe", C.c_int), ("learned", C.c_int)]
+
+
 class Opts(C.Structure):
     _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("max_order", C.c_int),
                 ("krylov_dim", C.c_int), ("max_restarts", C.c_int), ("precision", C.c_int),
@@ -154,6 +159,8 @@ def _declare(L):
     L.fvm_problem_free.argtypes = [C.POINTER(ProblemStruct)]
     L.fvm_problem_ensemble2d.argtypes = [_I, _I, _I, C.c_uint64, C.POINTER(ProblemStruct), _P]
     L.fvm_set_members.argtypes = [_P, _I, _P]
+    L.fvm_step_trace.restype = C.c_long
+    L.fvm_step_trace.argtypes = [_P, C.POINTER(StepRecord), C.c_long]
     L.fvm_pmesh_read.argtypes = [C.c_char_p, _I, C.POINTER(PmeshStruct)]
     L.fvm_pmesh_write.argtypes = [C.c_char_p, C.POINTER(PmeshStruct)]
     L.fvm_pmesh_free.argtypes = [C.POINTER(PmeshStruct)]
@@ -522,6 +529,17 @@ class Integrator:
         if r < 0:
             raise _err("fvm_integrate", r)
         return r, st.as_dict()
+
+    def trace(self):
+        """the accepted steps of the last integration on this context, as a
+        numpy record array (t, h, err, order, attempts, nni, nli, npe,
+        learned)"""
+        L = lib()
+        n = L.fvm_step_trace(self.ph._c, None, 0)
+        buf = (StepRecord * max(1, n))()
+        L.fvm_step_trace(self.ph._c, buf, n)
+        dt = np.dtype([(k, np.float64 if t is C.c_double else np.int32) for k, t in StepRecord._fields_])
+        return np.frombuffer(bytes(buf), dtype=dt, count=n).copy() if n > 0 else np.zeros(0, dt)
 
     def integrate_host(self, t0, t_end, y0: np.ndarray, y_end: np.ndarray):
         st = Stats()

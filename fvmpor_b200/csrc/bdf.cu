@@ -406,6 +406,7 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
     if (o.max_order < 1 || o.max_order > 5) throw Error("integrate: max_order must be 1..5");
     if (!(o.rtol > 0) || !(o.atol > 0)) throw Error("integrate: tolerances must be positive");
     if (!(t_end > t0)) throw Error("integrate: t_end must exceed t0");
+    c->last_trace.clear();
     DeviceOps ops(c, o);
     Predictor* pred = nullptr;
     if (o.use_predictor) {
@@ -435,6 +436,7 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
     }
     FVM_CUDA(cudaMemcpyAsync(y_end, ops.phi[0].p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
     FVM_CUDA(cudaStreamSynchronize(c->stream));
+    c->last_trace.swap(ctl.trace);
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
         stats->nst = ctl.st.nst;
@@ -533,4 +535,11 @@ extern "C" int fvm_integrate_host(fvm_ctx* c, const fvm_opts* opts, double t0, d
         set_error(ex.what());
         return -1;
     }
+}
+
+extern "C" long fvm_step_trace(const fvm_ctx* c, fvm_step_record* out, long cap) {
+    if (!c) return -1;
+    const long n = (long)c->last_trace.size();
+    if (out && cap > 0) std::memcpy(out, c->last_trace.data(), sizeof(fvm_step_record) * (size_t)std::min(n, cap));
+    return n;
 }

@@ -41,6 +41,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <vector>
+
+#include "../../include/fvmpor_b200.h"
 
 namespace fvmb {
 
@@ -78,6 +81,7 @@ template <class Ops> struct BdfController {
     static constexpr int kMaxOrd = 5;
     Ops& ops;
     BdfOptions o;
+    std::vector<fvm_step_record> trace;   // one record per accepted step
     BdfStats st;
     double psi[kMaxOrd + 2] = {}, alpha[kMaxOrd + 2] = {}, beta[kMaxOrd + 2] = {},
            sigma[kMaxOrd + 2] = {}, gamma[kMaxOrd + 2] = {};
@@ -112,6 +116,8 @@ template <class Ops> struct BdfController {
         const double uround = 2.220446049250313e-16;
         const double epcon = 0.33;
         int nef = 0, ncf = 0;
+        const long nni0 = st.nni, nli0 = st.nli, npe0 = st.npe;
+        int attempts = 0;
         if (t + h > tstop) h = tstop - t;
         ops.ewt_from_phi0(o.rtol, o.atol);
         ops.begin_step();
@@ -140,7 +146,18 @@ template <class Ops> struct BdfController {
             double tnew = t + h;
             ops.predict(k, gamma, h);
             double pnorm = ops.wrms_y();
-            if (o.use_guess && ops.newton_guess(tnew, h, cj)) st.npred++;
+            bool guessed = false;
+            ++attempts;
+            // The learned iterate is tried only on a retry after a failed
+            // corrector, where the BDF predictor has shown itself a poor
+            // start.  Accepted on ordinary steps (where the predictor's
+            // residual is already near the Krylov tolerance), a learned
+            // start that Newton accepts after one update leaves errors near
+            // the Newton tolerance in the state; every later step then
+            // spends 20-30 Krylov iterations removing them (30-day 3D run:
+            // 4 accepted guesses in the first 2 h raised the run from 221
+            // to 256 steps and from 5.2k to 6.4k Krylov iterations).
+            if (o.use_guess && ncf > 0 && ops.newton_guess(tnew, h, cj)) { st.npred++; guessed = true; }
             bool converged = false, fresh_p = false;
             // refresh the preconditioner on the first step, when cj has moved
             // by more than cj_refresh since the last factorisation, after
@@ -227,6 +244,12 @@ template <class Ops> struct BdfController {
                     t = tnew;
                     cj_last = cj;
                     st.nst++;
+                    fvm_step_record rec;
+                    rec.t = t; rec.h = h; rec.err = err;
+                    rec.order = kstep; rec.attempts = attempts;
+                    rec.nni = (int)(st.nni - nni0); rec.nli = (int)(st.nli - nli0);
+                    rec.npe = (int)(st.npe - npe0); rec.learned = guessed ? 1 : 0;
+                    trace.push_back(rec);
                     double hnew = h;
                     if (knew == k - 1 || k == o.max_order) iphase = 1;
                     bool doubled = false;

@@ -173,6 +173,7 @@ struct fvm_ctx {
 
     // host copies needed by the preconditioner set-up and the integrator
     std::vector<int> h_elem_nodes;   // [T][npe]
+    std::vector<fvm_step_record> last_trace;   // steps of the last integration
     std::vector<int> h_node_type;    // 0 free, 1 Dirichlet
     std::vector<double> h_vert;      // elevation of each node
     std::vector<double> h_hD;        // Dirichlet head (valid where type 1)

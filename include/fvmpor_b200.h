@@ -301,6 +301,21 @@ typedef struct {
 
 void fvm_opts_default(fvm_opts* o);
 
+/* One accepted BDF step of the last integration on a context: its end
+ * time, step size, order, local error test value (<= 1 accepts), the
+ * attempts it took (error-test or corrector failures + 1) and the Newton
+ * iterations, Krylov iterations and preconditioner set-ups spent on it,
+ * and whether the corrector started from the learned iterate.  The
+ * reference prints the same counters in aggregate (fvmpor_ODE.cpp:35-61). */
+typedef struct {
+    double t, h, err;
+    int order, attempts, nni, nli, npe, learned;
+} fvm_step_record;
+
+/* Copies up to cap records of the last fvm_integrate* call into out and
+ * returns how many that call produced. */
+long fvm_step_trace(const fvm_ctx* ctx, fvm_step_record* out, long cap);
+
 /* Integrate from (t0, y0) to t_end.  y0 / y_end are HOST buffers; the
  * solve itself runs on the device.  Returns 0 on success. */
 int fvm_integrate_host(fvm_ctx* ctx, const fvm_opts* opts, double t0,

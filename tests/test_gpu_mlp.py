@@ -100,13 +100,22 @@ def test_learned_iterate_in_the_integrator(cuda):
     perm = torch.randperm(cnt, device=cuda)
     rc, hist = pr.train(X[:cnt][perm].contiguous(), Y[:cnt][perm].contiguous(), epochs=20, batch=2048, lr=2e-3)
     assert rc == 0 and hist[-1] < hist[0]
-    learned = fb.Integrator(ph, krylov_dim=20, use_predictor=1)
+    # the learned iterate is tried on retries after a failed corrector; a
+    # one-hour first step makes the corrector fail early in the run
+    plain_h0 = fb.Integrator(ph, krylov_dim=20, h0=3600.0)
+    rc, st = plain_h0.integrate(0.0, 7200.0, y0, y_plain)
+    assert rc == 0
+    learned = fb.Integrator(ph, krylov_dim=20, use_predictor=1, h0=3600.0)
     y_learn = torch.empty_like(y0)
     ph.profile(True)
     rc, st2 = learned.integrate(0.0, 7200.0, y0, y_learn)
     attempts = ph.profile_read()["learned_attempt"][1]
     ph.profile(False)
     assert rc == 0
+    assert st2["ncfn"] > 0
+    tr = learned.trace()
+    assert len(tr) == st2["nst"] and int(tr["learned"].sum()) == st2["npred"]
+    assert int(tr["nli"].sum()) <= st2["nli"]
     # the learned iterate only changes where Newton starts: both runs solve
     # the same BDF problem to the same tolerance
     span = y_plain.abs().max().item()
@@ -114,7 +123,7 @@ def test_learned_iterate_in_the_integrator(cuda):
     # what the trained network gains over the plain predictor on this
     # problem: how often it was tried and how often the residual test kept
     # its iterate, and the Krylov and Newton work beside the plain run's
-    assert attempts > 0
+    assert attempts > 0   # one per retry after a failed corrector, outside the back-off
     gain = {"attempts": attempts, "accepted_steps": st2["npred"], "steps": st2["nst"],
             "krylov_per_newton_learned": st2["nli"] / st2["nni"], "krylov_per_newton_plain": st["nli"] / st["nni"],
             "newton_per_step_learned": st2["nni"] / st2["nst"], "newton_per_step_plain": st["nni"] / st["nst"]}
