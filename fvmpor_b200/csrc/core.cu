@@ -979,7 +979,8 @@ extern "C" void fvm_destroy(fvm_ctx* c) {
     if (!c) return;
     cudaStreamSynchronize(c->stream);
     fvmb_destroy_ilu(c->ilu);
-    fvmb_destroy_krylov(c->kry);
+    fvmb_destroy_krylov(c->kry[0]);
+    fvmb_destroy_krylov(c->kry[1]);
     fvmb_destroy_predictor(c->pred);
     cudaStream_t s = c->stream;
     delete c;

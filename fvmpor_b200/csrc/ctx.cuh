@@ -235,7 +235,8 @@ struct fvm_ctx {
     std::vector<int> h_member_ptr;
     fvmb::DevBuf<int> member_ptr;
     fvmb::BlockILU* ilu = nullptr;
-    fvmb::Krylov* kry = nullptr;
+    fvmb::Krylov* kry[2] = {nullptr, nullptr};   // Krylov workspaces by precision (0 FP64, 1 FP32)
+    fvmb::Krylov* kry_last = nullptr;            // the one used last (scratch for reductions)
     fvmb::Predictor* pred = nullptr;
 
     long n_residuals = 0;

@@ -43,6 +43,9 @@ struct GmresCounters {
 };
 
 Krylov* krylov_get(fvm_ctx* c, int m, int precision);
+// the workspace used last (created small if none): reduction scratch for
+// the controller and the learned iterate
+inline Krylov* krylov_scratch(fvm_ctx* c) { return c->kry_last ? c->kry_last : krylov_get(c, 1, 0); }
 void fvmb_destroy_krylov_impl(Krylov* K);
 double reduce_sumsq(fvm_ctx* c, const double* x, const double* w);
 double reduce_dot(fvm_ctx* c, const double* x, const double* y);

@@ -186,53 +186,132 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, int
 
 // out[v] = sum over blocks b (ascending, lane-strided, fixed shuffle tree) of
 // partial[b * nv + v] -- the order of last_block_reduce, so every block gets
-// the same bits; written to shared memory
+// the same bits; written to shared memory.  The partials were written by
+// other blocks before the grid barrier: they are read through L2 (ld.cg,
+// never a stale L1 line), a warp taking 4 vectors and each lane 5 blocks at
+// a time so that 20 loads per lane are in flight.
 __device__ __forceinline__ void block_reduce_all(const double* partial, int nv, int nblk, double* out) {
+    constexpr int kQ = 4, kI = 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const volatile double* vp = partial;
-    for (int v = warp; v < nv; v += nw) {
-        double s = 0.0;
-        for (int b = lane; b < nblk; b += 32) s += vp[(size_t)b * nv + v];
-        s = warp_sum(s);
-        if (lane == 0) out[v] = s;
+    for (int v0 = warp; v0 < nv; v0 += kQ * nw) {
+        double s[kQ];
+#pragma unroll
+        for (int q = 0; q < kQ; ++q) s[q] = 0.0;
+        for (int b0 = 0; b0 < nblk; b0 += 32 * kI) {
+            double x[kI][kQ];
+#pragma unroll
+            for (int i = 0; i < kI; ++i) {
+                const int b = b0 + lane + 32 * i;
+#pragma unroll
+                for (int q = 0; q < kQ; ++q) {
+                    const int v = v0 + q * nw;
+                    x[i][q] = (b < nblk && v < nv) ? __ldcg(partial + (size_t)b * nv + v) : 0.0;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < kI; ++i)
+#pragma unroll
+                for (int q = 0; q < kQ; ++q) s[q] += x[i][q];
+        }
+#pragma unroll
+        for (int q = 0; q < kQ; ++q) {
+            const double t = warp_sum(s[q]);
+            const int v = v0 + q * nw;
+            if (lane == 0 && v < nv) out[v] = t;
+        }
     }
     __syncthreads();
 }
 
 constexpr int kCgsThreads = 512;
+constexpr int kCgsGroup = 8;   // basis vectors whose loads are in flight together
+
+// rows per block of the fused orthogonalisation: ceil(N / nblk) rounded up
+// to 4, so every block's rows start on a 4-row (16-byte FP32 / 32-byte
+// FP64) boundary and each thread owns whole quads of rows
+__host__ __device__ inline int cgs_chunk(int N, int nblk) {
+    const int c = (N + nblk - 1) / nblk;
+    return (c + 3) & ~3;
+}
+
+// four consecutive basis values starting at a 4-aligned row (the basis
+// allocation is padded to a multiple of 64 rows and zeroed, so a quad that
+// straddles row N reads zeros)
+__device__ __forceinline__ void ld4(const float* p, double v[4]) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double v[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
 
 // block-local dot products <U_i, W> over rows [k0, k1) for i < nv, with the
-// block's W rows in shared memory (Wl[k - k0]): the warps split the
-// (vector, row segment) pairs, the segments of a vector are then summed in
-// segment order.  Row nv of the output (when with_norm) is sum W^2.  out[i]
-// is valid in every thread after the call.
+// block's W rows in shared memory (Wl[k - k0]).  Each thread owns quads of
+// rows; the vectors are taken kCgsGroup at a time so that many loads are in
+// flight per thread.  Per vector: the thread's quads in row order, then the
+// warp's lanes by a fixed shuffle tree, then the warps in warp order.  Row
+// nv of the output (when with_norm) is sum W^2.  out[i] is valid in every
+// thread after the call.  red holds kCgsGroup doubles per warp.
 template <class B>
 __device__ __forceinline__ void block_dots(const B* __restrict__ U, size_t ld, const double* __restrict__ Wl, int k0,
-                                           int k1, int nv, bool with_norm, double* seg_sums, double* out) {
+                                           int k1, int nv, bool with_norm, double* red, double* out) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int nvec = nv + (with_norm ? 1 : 0);
-    const int nseg = max(1, nw / nvec);
-    const int len = (k1 - k0 + nseg - 1) / nseg;
-    for (int idx = warp; idx < nvec * nseg; idx += nw) {
-        const int i = idx / nseg, sg = idx - i * nseg;
-        const int a = k0 + sg * len, b = min(k1, a + len);
-        double sacc = 0.0;
-        if (i < nv) {
-            const B* Ui = U + ld * i;
-            for (int k = a + lane; k < b; k += 32) sacc += ldb(Ui, k) * Wl[k - k0];
-        } else {
-            for (int k = a + lane; k < b; k += 32) sacc += Wl[k - k0] * Wl[k - k0];
+    for (int i0 = 0; i0 < nvec; i0 += kCgsGroup) {
+        double acc[kCgsGroup];
+#pragma unroll
+        for (int q = 0; q < kCgsGroup; ++q) acc[q] = 0.0;
+        for (int r = k0 + 4 * threadIdx.x; r < k1; r += 4 * blockDim.x) {
+            double w[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) w[e] = r + e < k1 ? Wl[r + e - k0] : 0.0;
+#pragma unroll
+            for (int q = 0; q < kCgsGroup; ++q) {
+                const int i = i0 + q;
+                if (i < nv) {
+                    double u[4];
+                    ld4(U + ld * i + r, u);
+                    acc[q] += u[0] * w[0] + u[1] * w[1] + u[2] * w[2] + u[3] * w[3];
+                } else if (i == nv && with_norm) {
+                    acc[q] += w[0] * w[0] + w[1] * w[1] + w[2] * w[2] + w[3] * w[3];
+                }
+            }
         }
-        sacc = warp_sum(sacc);
-        if (lane == 0) seg_sums[idx] = sacc;
+#pragma unroll
+        for (int q = 0; q < kCgsGroup; ++q) acc[q] = warp_sum(acc[q]);
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < kCgsGroup; ++q) red[warp * kCgsGroup + q] = acc[q];
+        }
+        __syncthreads();
+        if (threadIdx.x < kCgsGroup && i0 + threadIdx.x < nvec) {
+            double t = 0.0;
+            for (int w2 = 0; w2 < nw; ++w2) t += red[w2 * kCgsGroup + threadIdx.x];
+            out[i0 + threadIdx.x] = t;
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
-        double t = 0.0;
-        for (int sg = 0; sg < nseg; ++sg) t += seg_sums[i * nseg + sg];
-        out[i] = t;
+}
+
+// acc[e] = sum_i coef[i] U_i[r + e], e < 4, vectors kCgsGroup at a time
+template <class B>
+__device__ __forceinline__ void quad_combine(const B* __restrict__ U, size_t ld, const double* coef, int nv, int r,
+                                             double acc[4]) {
+    acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
+    for (int i0 = 0; i0 < nv; i0 += kCgsGroup) {
+#pragma unroll
+        for (int q = 0; q < kCgsGroup; ++q) {
+            const int i = i0 + q;
+            if (i < nv) {
+                double u[4];
+                ld4(U + ld * i + r, u);
+                const double c = coef[i];
+                acc[0] += c * u[0]; acc[1] += c * u[1]; acc[2] += c * u[2]; acc[3] += c * u[3];
+            }
+        }
     }
-    __syncthreads();
 }
 
 // One Arnoldi step of the device-driven GMRES in one cooperative launch:
@@ -246,7 +325,9 @@ __device__ __forceinline__ void block_dots(const B* __restrict__ U, size_t ld, c
 // The last line is Pythagoras on the re-orthogonalisation: b is a
 // rounding-level correction, so the norm needs no third reduction.  Two grid
 // barriers per step.  Every reduction is fixed-order (per-block partials in
-// block order), so results are bitwise reproducible.
+// block order), so results are bitwise reproducible.  Block b owns rows
+// [b c, min(N, (b+1) c)) with c = cgs_chunk(N, gridDim.x); its rows of W
+// live in dynamic shared memory (c doubles).
 template <class B>
 __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* st, B* __restrict__ U, size_t ld,
                                                               double* __restrict__ scale,
@@ -257,34 +338,36 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
                                                               double* __restrict__ t_next, double* sigma_next,
                                                               double* __restrict__ H, double* __restrict__ cs,
                                                               double* __restrict__ sn, double* __restrict__ g) {
-    __shared__ double ca[64], cb[64], seg[64];
+    __shared__ double ca[64], cb[64], coef[64];
+    __shared__ double red[(kCgsThreads / 32) * kCgsGroup];
     extern __shared__ double Ws[];   // this block's rows of W (the vector being orthogonalised)
     (void)W;
     if (st->done) return;            // the device-driven loop has finished
     const int j = st->j, nv = j + 1, m = st->m;
     const int nblk = gridDim.x;
-    const int chunk = (N + nblk - 1) / nblk;
-    const int k0 = blockIdx.x * chunk, k1 = min(N, k0 + chunk);
+    const int chunk = cgs_chunk(N, nblk);
+    const int k0 = min(N, blockIdx.x * chunk), k1 = min(N, k0 + chunk);
     double* pa = partial;
     double* pb = partial + (size_t)nblk * 64;
     // pass 1: a = U^T W
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) Ws[k - k0] = ewt[k] * Jv[k];
     __syncthreads();
-    block_dots(U, ld, Ws, k0, k1, nv, false, seg, ca);
+    block_dots(U, ld, Ws, k0, k1, nv, false, red, ca);
     for (int i = threadIdx.x; i < nv; i += blockDim.x) pa[(size_t)blockIdx.x * nv + i] = ca[i];
     if (!grid_barrier(bar, bar + 1, err)) return;
     block_reduce_all(pa, nv, nblk, ca);
-    for (int i = threadIdx.x; i < nv; i += blockDim.x) cb[i] = ca[i] * scale[i] * scale[i];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = ca[i] * scale[i] * scale[i];
     __syncthreads();
     // pass 2: W' = W - U diag(s^2) a; b = U^T W', ||W'||^2
-    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-        double acc = 0.0;
-#pragma unroll 8
-        for (int i = 0; i < nv; ++i) acc += cb[i] * ldb(U + ld * i, k);
-        Ws[k - k0] = Ws[k - k0] - acc;
+    for (int r = k0 + 4 * threadIdx.x; r < k1; r += 4 * blockDim.x) {
+        double acc[4];
+        quad_combine(U, ld, coef, nv, r, acc);
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (r + e < k1) Ws[r + e - k0] -= acc[e];
     }
     __syncthreads();
-    block_dots(U, ld, Ws, k0, k1, nv, true, seg, cb);
+    block_dots(U, ld, Ws, k0, k1, nv, true, red, cb);
     for (int i = threadIdx.x; i <= nv; i += blockDim.x) pb[(size_t)blockIdx.x * (nv + 1) + i] = cb[i];
     if (!grid_barrier(bar, bar + 1, err)) return;
     block_reduce_all(pb, nv + 1, nblk, cb);
@@ -295,18 +378,22 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
     }
     nrm2 = nrm2 > 0.0 ? nrm2 : 0.0;
     const double snv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
-    __shared__ double coef[64];
     for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = cb[i] * scale[i] * scale[i];
     __syncthreads();
     // pass 3: the new basis vector and the next direction
     B* Un = U + ld * nv;
-    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-        double acc = 0.0;
-#pragma unroll 8
-        for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
-        const B u = (B)(Ws[k - k0] - acc);
-        Un[k] = u;
-        t_next[k] = snv * (double)u / ewt[k];
+    for (int r = k0 + 4 * threadIdx.x; r < k1; r += 4 * blockDim.x) {
+        double acc[4];
+        quad_combine(U, ld, coef, nv, r, acc);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int k = r + e;
+            if (k < k1) {
+                const B u = (B)(Ws[k - k0] - acc[e]);
+                Un[k] = u;
+                t_next[k] = snv * (double)u / ewt[k];
+            }
+        }
     }
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     scale[nv] = snv;
@@ -409,15 +496,23 @@ __global__ void k_sub(int N, const double* __restrict__ a, const double* __restr
 
 // ------------------------------------------------------------------ Krylov
 Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
-    Krylov* K = c->kry;
-    if (K && K->m >= m && K->precision == precision) return K;
-    if (K) fvmb_destroy_krylov_impl(K);
+    precision = precision ? 1 : 0;
+    Krylov* K = c->kry[precision];
+    if (K && K->m >= m) return c->kry_last = K;
+    if (K) {
+        FVM_CUDA(cudaStreamSynchronize(c->stream));
+        fvmb_destroy_krylov_impl(K);
+        c->kry[precision] = nullptr;
+    }
     K = new Krylov();
     K->m = m;
     K->precision = precision;
     K->ld = ((size_t)c->N + 63) / 64 * 64;
     size_t bytes = (precision ? sizeof(float) : sizeof(double)) * K->ld * (m + 1);
     FVM_CUDA(cudaMalloc(&K->U, bytes));
+    // rows N .. ld of every basis vector stay zero: the fused
+    // orthogonalisation reads them in its last row quad
+    FVM_CUDA(cudaMemsetAsync(K->U, 0, bytes, c->stream));
     K->scale.alloc(m + 2);
     K->W.alloc(c->N);
     K->t.alloc(c->N);
@@ -438,13 +533,13 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
         FVM_CUDA(cudaGetDevice(&dev));
         FVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         FVM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        if (precision)
-            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<float>, kCgsThreads, 0));
-        else
-            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<double>, kCgsThreads, 0));
         // one block per SM: fewer arrivals at each grid barrier; the block's
         // rows of W (at most 48 KB) live in its shared memory
-        const size_t wsm = sizeof(double) * (size_t)((c->N + nsm - 1) / nsm);
+        const size_t wsm = sizeof(double) * (size_t)cgs_chunk(c->N, nsm);
+        if (precision)
+            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<float>, kCgsThreads, wsm));
+        else
+            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<double>, kCgsThreads, wsm));
         K->coop_grid = (coop && per_sm > 0 && m + 1 <= 63 && wsm <= 48 * 1024) ? nsm : 0;
     }
     K->res.alloc(3 * (m + 2) + 8);
@@ -452,8 +547,8 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
     // results of the three passes, the m+1 basis scales, a status word and
     // the device-driven Arnoldi state
     FVM_CUDA(cudaMallocHost(&K->host, sizeof(double) * (4 * (m + 2) + 8) + sizeof(ArnState)));
-    c->kry = K;
-    return K;
+    c->kry[precision] = K;
+    return c->kry_last = K;
 }
 
 void fvmb_destroy_krylov_impl(Krylov* K) {
@@ -465,7 +560,7 @@ void fvmb_destroy_krylov_impl(Krylov* K) {
 
 // host-synchronous reductions used by the controller
 double reduce_sumsq(fvm_ctx* c, const double* x, const double* w) {
-    Krylov* K = krylov_get(c, c->kry ? c->kry->m : 1, c->kry ? c->kry->precision : 0);
+    Krylov* K = krylov_scratch(c);
     fvm_launch(c, k_sumsq, kRedBlocks, kRedThreads, 0, c->stream, c->N, x, w, K->partial.p, K->counter.p, K->res.p);
     FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     FVM_CUDA(cudaStreamSynchronize(c->stream));
@@ -473,7 +568,7 @@ double reduce_sumsq(fvm_ctx* c, const double* x, const double* w) {
 }
 
 double reduce_dot(fvm_ctx* c, const double* x, const double* y) {
-    Krylov* K = krylov_get(c, c->kry ? c->kry->m : 1, c->kry ? c->kry->precision : 0);
+    Krylov* K = krylov_scratch(c);
     fvm_launch(c, k_dot, kRedBlocks, kRedThreads, 0, c->stream, c->N, x, y, K->partial.p, K->counter.p, K->res.p);
     FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     FVM_CUDA(cudaStreamSynchronize(c->stream));
@@ -584,7 +679,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                     double* sgp = K->sigma.p;
                     void* args[] = {&Ni, &stp, &Ub, &ldv, &scp, &jvp, &ew, &Wp, &pp, &bp, &ep, &tp, &sgp,
                                     &H_d, &cs_d, &sn_d, &g_d};
-                    const size_t wsm = sizeof(double) * (size_t)((N + K->coop_grid - 1) / K->coop_grid);
+                    const size_t wsm = sizeof(double) * (size_t)cgs_chunk(N, K->coop_grid);
                     FVM_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi_cgs2<B>, dim3(K->coop_grid),
                                                          dim3(kCgsThreads), args, wsm, s));
                     c->launches++;

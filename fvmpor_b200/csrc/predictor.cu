@@ -648,7 +648,7 @@ bool predictor_apply(fvm_ctx* c, Predictor* p, double rtol, double atol, double 
     //   |F(a)|^2 ~ A + 2a (B - A) + a^2 (A - 2B + C),  A = F0.F0, B = F0.F1, C = F1.F1.
     // Take its minimiser on [0, 1]; keep the BDF predictor when the learned
     // direction does not lower the residual.
-    Krylov* K = krylov_get(c, c->kry ? c->kry->m : 1, c->kry ? c->kry->precision : 0);
+    Krylov* K = krylov_scratch(c);
     fvm_launch(c, k_dot3, kRedBlocks, kRedThreads, 0, c->stream, N, F, p->Fg.p, K->partial.p, K->counter.p,
                K->res.p);
     FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

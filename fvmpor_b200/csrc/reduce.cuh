@@ -47,11 +47,22 @@ static __device__ __forceinline__ void last_block_reduce(double* partial, int nv
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // partials of the other blocks are read through L2 (ld.cg), a lane
+    // keeping 8 of them in flight; summed in ascending block order per lane
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const volatile double* vp = partial;
+    const int nblk = (int)gridDim.x;
     for (int v = warp; v < nv; v += nw) {
         double s = 0.0;
-        for (int b = lane; b < (int)gridDim.x; b += 32) s += vp[(size_t)b * nv + v];
+        for (int b0 = 0; b0 < nblk; b0 += 32 * 8) {
+            double x[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int b = b0 + lane + 32 * i;
+                x[i] = b < nblk ? __ldcg(partial + (size_t)b * nv + v) : 0.0;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) s += x[i];
+        }
         s = warp_sum(s);
         if (lane == 0) out[v] = s;
     }
