@@ -370,11 +370,12 @@ def main():
     mixed.integrate(0.0, horizon, y0, yend)   # warm the FP32 and FP64 factor/basis buffers
     plain.integrate(0.0, horizon, y0, yend)
     runs_mixed, runs_plain = [], []
-    for _ in range(k_extra):
-        ms, st_mixed, _ = timed(mixed, 1)
-        runs_mixed.append(ms)
-        ms, st_plain, _ = timed(plain, 1)
-        runs_plain.append(ms)
+    with ClockSampler(local) as clk_cmp:
+        for _ in range(k_extra):
+            ms, st_mixed, _ = timed(mixed, 1)
+            runs_mixed.append(ms)
+            ms, st_plain, _ = timed(plain, 1)
+            runs_plain.append(ms)
     y_plain = yend.clone()
     ms_mixed = float(np.median(runs_mixed)) * k_extra
     ms_plain = float(np.median(runs_plain)) * k_extra
@@ -410,7 +411,7 @@ def main():
                        "ratio_learned_fp32_over_plain": value / plain_value,
                        "stats": {k: st_plain[0][k] for k in ("nst", "nni", "nli", "npe", "nre")}},
         "fp32_without_learned": {"value": mixed_value, "ms_per_step": ms_mixed / k_extra, "runs": k_extra,
-                                 "ms_each_run": runs_mixed,
+                                 "ms_each_run": runs_mixed, "clocks_fp32_and_fp64_runs": clk_cmp.summary(),
                                  "stats": {k: st_mixed[0][k] for k in ("nst", "nni", "nli", "npe", "nre")}},
         "learned_predictor": dict(train_info, accepted_steps=st0["npred"]),
         "final_head_rel_diff_vs_plain_fp64": head_diff,
@@ -425,6 +426,9 @@ def main():
                       for k, v in prof.items()},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N},
         "clocks": clocks,
+        # the run is driven by one host thread: a busy host shows up as
+        # slower, more variable runs
+        "host_loadavg_1min": os.getloadavg()[0],
     }
     # every kernel launch of the library inside the timed region (counted by
     # the context: residual chain, Krylov, preconditioner, controller)

@@ -100,7 +100,7 @@ class PmeshStruct(C.Structure):
 
 
 class StepRecord(C.Structure):
-    _fields_ = [("t", C.c_double), ("h", C.c_double), ("err", C.c_double), ("order", C.c_int),
+    _fields_ = [("t", C.c_double), ("h", C.c_double), ("err", C.c_double), ("wall", C.c_double), ("order", C.c_int),
                 ("attempts", C.c_int), ("nni", C.c_int), ("nli", C.c_int), ("npe", C.c_int), ("learned", C.c_int)]
 
 
@@ -532,7 +532,7 @@ class Integrator:
 
     def trace(self):
         """the accepted steps of the last integration on this context, as a
-        numpy record array (t, h, err, order, attempts, nni, nli, npe,
+        numpy record array (t, h, err, wall, order, attempts, nni, nli, npe,
         learned)"""
         L = lib()
         n = L.fvm_step_trace(self.ph._c, None, 0)

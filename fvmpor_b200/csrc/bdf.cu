@@ -208,33 +208,76 @@ __global__ void k_scale_vec(int N, double a, const double* __restrict__ x, doubl
     if (i < N) y[i] = a * x[i];
 }
 
-struct DeviceOps {
-    fvm_ctx* c;
-    const fvm_opts& o;
-    int N;
+} // namespace fvmb
+
+// The integrator's vectors, kept by the context from its first integration
+// on, so that an integration allocates and frees nothing (cudaFree and
+// cudaFreeHost synchronise the device and occasionally stall for a
+// fraction of a second on a busy host).
+struct fvmb::IntegWork {
     DevBuf<double> phi[kNPhi];
     DevBuf<double> y, yp, e, ewt, F, x, tmp;
     DevBuf<double> partial, res;
     DevBuf<unsigned> counter;
-    double* host = nullptr;
+    DevBuf<double> ypred, yppred, hprev;
+    DevBuf<float> feat;
+    DevBuf<double> host_in, host_out;   // device copies for fvm_integrate_host
+    double* host = nullptr;             // pinned
+    size_t host_n = 0;
+    ~IntegWork() {
+        if (host) cudaFreeHost(host);
+    }
+};
+
+void fvmb_destroy_integ_work(fvmb::IntegWork* w) { delete w; }
+
+namespace fvmb {
+
+static IntegWork& integ_work(fvm_ctx* c) {
+    if (!c->work) c->work = new IntegWork();
+    IntegWork& w = *c->work;
+    const int N = c->N;
+    for (int j = 0; j < kNPhi; ++j) w.phi[j].alloc(N);
+    w.y.alloc(N); w.yp.alloc(N); w.e.alloc(N); w.ewt.alloc(N); w.F.alloc(N); w.x.alloc(N); w.tmp.alloc(N);
+    w.partial.alloc((size_t)kRedBlocks * 4);
+    const size_t nh = (size_t)std::max(8, 4 * c->n_members);
+    w.res.alloc(nh);
+    w.counter.alloc(1);
+    if (w.host_n < nh) {
+        if (w.host) FVM_CUDA(cudaFreeHost(w.host));
+        w.host = nullptr;
+        FVM_CUDA(cudaMallocHost(&w.host, sizeof(double) * nh));
+        w.host_n = nh;
+    }
+    return w;
+}
+
+struct DeviceOps {
+    fvm_ctx* c;
+    const fvm_opts& o;
+    int N;
+    IntegWork& w;
+    DevBuf<double> (&phi)[kNPhi];
+    DevBuf<double> &y, &yp, &e, &ewt, &F, &x, &tmp;
+    DevBuf<double> &partial, &res;
+    DevBuf<unsigned>& counter;
+    double* host;
     double tcur = 0.0, hcur = 0.0;
     Predictor* pred = nullptr;     // learned Newton iterate (optional)
     Recorder* rec = nullptr;       // training-set recorder (optional)
-    DevBuf<double> ypred, yppred, hprev;
-    DevBuf<float> feat;
+    DevBuf<double> &ypred, &yppred, &hprev;
+    DevBuf<float>& feat;
     bool f_fresh = false;          // F already holds F(t, y, y')
 
     int nm = 1;                    // ensemble members (per-member norms when > 1)
 
-    DeviceOps(fvm_ctx* ctx, const fvm_opts& opts) : c(ctx), o(opts), N(ctx->N) {
-        for (int j = 0; j < kNPhi; ++j) { phi[j].alloc(N); phi[j].zero(c->stream); }
-        y.alloc(N); yp.alloc(N); e.alloc(N); ewt.alloc(N); F.alloc(N); x.alloc(N); tmp.alloc(N);
-        partial.alloc((size_t)kRedBlocks * 4);
+    DeviceOps(fvm_ctx* ctx, const fvm_opts& opts)
+        : c(ctx), o(opts), N(ctx->N), w(integ_work(ctx)), phi(w.phi), y(w.y), yp(w.yp), e(w.e), ewt(w.ewt),
+          F(w.F), x(w.x), tmp(w.tmp), partial(w.partial), res(w.res), counter(w.counter), host(w.host),
+          ypred(w.ypred), yppred(w.yppred), hprev(w.hprev), feat(w.feat) {
+        for (int j = 0; j < kNPhi; ++j) phi[j].zero(c->stream);
         nm = c->n_members;
-        res.alloc(std::max(8, 4 * nm));
-        counter.alloc(1);
         counter.zero(c->stream);
-        FVM_CUDA(cudaMallocHost(&host, sizeof(double) * std::max(8, 4 * nm)));
     }
     // largest per-member WRMS norm from per-member squared sums out[m*nq + q]
     double member_max(int nq, int q) const {
@@ -244,9 +287,6 @@ struct DeviceOps {
             if (nmem > 0) best = std::max(best, std::sqrt(host[(size_t)m * nq + q] / nmem));
         }
         return best;
-    }
-    ~DeviceOps() {
-        if (host) cudaFreeHost(host);
     }
     int g() const { return grid_for(N, 256); }
     PhiPtrs ptrs() const {
@@ -519,7 +559,9 @@ extern "C" int fvm_integrate_host(fvm_ctx* c, const fvm_opts* opts, double t0, d
                                   const double* y0_host, double* y_end_host, fvm_stats* stats) {
     try {
         if (!c || !opts || !y0_host || !y_end_host) throw Error("fvm_integrate_host: null argument");
-        DevBuf<double> a, b;
+        IntegWork& w = integ_work(c);
+        DevBuf<double>& a = w.host_in;
+        DevBuf<double>& b = w.host_out;
         a.alloc(c->N);
         b.alloc(c->N);
         FVM_CUDA(cudaMemcpyAsync(a.p, y0_host, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));

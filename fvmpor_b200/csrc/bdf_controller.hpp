@@ -40,6 +40,7 @@
 #pragma once
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <vector>
 
@@ -82,6 +83,7 @@ template <class Ops> struct BdfController {
     Ops& ops;
     BdfOptions o;
     std::vector<fvm_step_record> trace;   // one record per accepted step
+    std::chrono::steady_clock::time_point wall0 = std::chrono::steady_clock::now();
     BdfStats st;
     double psi[kMaxOrd + 2] = {}, alpha[kMaxOrd + 2] = {}, beta[kMaxOrd + 2] = {},
            sigma[kMaxOrd + 2] = {}, gamma[kMaxOrd + 2] = {};
@@ -100,6 +102,7 @@ template <class Ops> struct BdfController {
         k = 1; kold = 0; hold = 0; psi[0] = h; cj = 1.0 / h; iphase = 0; ns = 0;
         rate_s = 20.0; cj_last = 0.0;
         have_p = false;
+        wall0 = std::chrono::steady_clock::now();
     }
 
     void restore() {
@@ -246,6 +249,7 @@ template <class Ops> struct BdfController {
                     st.nst++;
                     fvm_step_record rec;
                     rec.t = t; rec.h = h; rec.err = err;
+                    rec.wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
                     rec.order = kstep; rec.attempts = attempts;
                     rec.nni = (int)(st.nni - nni0); rec.nli = (int)(st.nli - nli0);
                     rec.npe = (int)(st.npe - npe0); rec.learned = guessed ? 1 : 0;

@@ -958,6 +958,7 @@ using namespace fvmb;
 
 void fvmb_destroy_ilu(fvmb::BlockILU* p);
 void fvmb_destroy_krylov(fvmb::Krylov* p);
+void fvmb_destroy_integ_work(fvmb::IntegWork* w);
 void fvmb_destroy_predictor(fvmb::Predictor* p);
 
 extern "C" const char* fvm_last_error(void) { return g_last_error.c_str(); }
@@ -981,6 +982,7 @@ extern "C" void fvm_destroy(fvm_ctx* c) {
     fvmb_destroy_ilu(c->ilu);
     fvmb_destroy_krylov(c->kry[0]);
     fvmb_destroy_krylov(c->kry[1]);
+    fvmb_destroy_integ_work(c->work);
     fvmb_destroy_predictor(c->pred);
     cudaStream_t s = c->stream;
     delete c;

@@ -158,6 +158,7 @@ __device__ __forceinline__ double gather_row(const GatherSrc& g, int i) {
 struct BlockILU;   // precond.cu
 struct Krylov;     // linalg.cu
 struct Predictor;  // predictor.cu
+struct IntegWork;  // bdf.cu
 
 } // namespace fvmb
 
@@ -237,6 +238,7 @@ struct fvm_ctx {
     fvmb::BlockILU* ilu = nullptr;
     fvmb::Krylov* kry[2] = {nullptr, nullptr};   // Krylov workspaces by precision (0 FP64, 1 FP32)
     fvmb::Krylov* kry_last = nullptr;            // the one used last (scratch for reductions)
+    fvmb::IntegWork* work = nullptr;             // the integrator's vectors (bdf.cu)
     fvmb::Predictor* pred = nullptr;
 
     long n_residuals = 0;

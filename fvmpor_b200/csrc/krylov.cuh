@@ -32,6 +32,7 @@ struct Krylov {
     DevBuf<unsigned> bar;     // grid barrier of the fused orthogonalisation
     DevBuf<int> err;          // 3 = a grid barrier timed out
     int coop_grid = 0;        // blocks of the cooperative launch, 0 = three-pass path
+    size_t coop_smem = 0;     // dynamic shared memory of the fused kernel
     DevBuf<ArnState> st;      // device-driven Arnoldi state
     DevBuf<double> ls;        // H [(m+1) x m], cs [m], sn [m], g [m+1]
     double* host = nullptr;   // pinned

@@ -246,6 +246,14 @@ __device__ __forceinline__ void ld4(const double* p, double v[4]) {
     const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
+// the basis, read by row quads through the read-only path (the block's
+// rows of the vectors stay in L1 between the three passes)
+template <class B>
+struct BasisRows {
+    const B* U;
+    size_t ld;
+    __device__ __forceinline__ void quad(int i, int r, double v[4]) const { ld4(U + ld * i + r, v); }
+};
 
 // block-local dot products <U_i, W> over rows [k0, k1) for i < nv, with the
 // block's W rows in shared memory (Wl[k - k0]).  Each thread owns quads of
@@ -255,8 +263,8 @@ __device__ __forceinline__ void ld4(const double* p, double v[4]) {
 // nv of the output (when with_norm) is sum W^2.  out[i] is valid in every
 // thread after the call.  red holds kCgsGroup doubles per warp.
 template <class B>
-__device__ __forceinline__ void block_dots(const B* __restrict__ U, size_t ld, const double* __restrict__ Wl, int k0,
-                                           int k1, int nv, bool with_norm, double* red, double* out) {
+__device__ __forceinline__ void block_dots(const BasisRows<B>& U, const double* __restrict__ Wl, int k0, int k1,
+                                           int nv, bool with_norm, double* red, double* out) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int nvec = nv + (with_norm ? 1 : 0);
     for (int i0 = 0; i0 < nvec; i0 += kCgsGroup) {
@@ -272,7 +280,7 @@ __device__ __forceinline__ void block_dots(const B* __restrict__ U, size_t ld, c
                 const int i = i0 + q;
                 if (i < nv) {
                     double u[4];
-                    ld4(U + ld * i + r, u);
+                    U.quad(i, r, u);
                     acc[q] += u[0] * w[0] + u[1] * w[1] + u[2] * w[2] + u[3] * w[3];
                 } else if (i == nv && with_norm) {
                     acc[q] += w[0] * w[0] + w[1] * w[1] + w[2] * w[2] + w[3] * w[3];
@@ -297,7 +305,7 @@ __device__ __forceinline__ void block_dots(const B* __restrict__ U, size_t ld, c
 
 // acc[e] = sum_i coef[i] U_i[r + e], e < 4, vectors kCgsGroup at a time
 template <class B>
-__device__ __forceinline__ void quad_combine(const B* __restrict__ U, size_t ld, const double* coef, int nv, int r,
+__device__ __forceinline__ void quad_combine(const BasisRows<B>& U, const double* coef, int nv, int r,
                                              double acc[4]) {
     acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
     for (int i0 = 0; i0 < nv; i0 += kCgsGroup) {
@@ -306,7 +314,7 @@ __device__ __forceinline__ void quad_combine(const B* __restrict__ U, size_t ld,
             const int i = i0 + q;
             if (i < nv) {
                 double u[4];
-                ld4(U + ld * i + r, u);
+                U.quad(i, r, u);
                 const double c = coef[i];
                 acc[0] += c * u[0]; acc[1] += c * u[1]; acc[2] += c * u[2]; acc[3] += c * u[3];
             }
@@ -327,7 +335,11 @@ __device__ __forceinline__ void quad_combine(const B* __restrict__ U, size_t ld,
 // barriers per step.  Every reduction is fixed-order (per-block partials in
 // block order), so results are bitwise reproducible.  Block b owns rows
 // [b c, min(N, (b+1) c)) with c = cgs_chunk(N, gridDim.x); its rows of W
-// live in dynamic shared memory (c doubles).
+// live in dynamic shared memory (c doubles).  Its rows of the basis are
+// read three times, by row quads; they stay in L1 between the passes.
+// (Staging them in shared memory by bulk copies was measured slower: 50 us
+// against 45 us at 40 vectors, the 226 KB of shared memory leaving L1 too
+// little for the rest.)
 template <class B>
 __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* st, B* __restrict__ U, size_t ld,
                                                               double* __restrict__ scale,
@@ -352,7 +364,8 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
     // pass 1: a = U^T W
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) Ws[k - k0] = ewt[k] * Jv[k];
     __syncthreads();
-    block_dots(U, ld, Ws, k0, k1, nv, false, red, ca);
+    const BasisRows<B> UR{U, ld};
+    block_dots(UR, Ws, k0, k1, nv, false, red, ca);
     for (int i = threadIdx.x; i < nv; i += blockDim.x) pa[(size_t)blockIdx.x * nv + i] = ca[i];
     if (!grid_barrier(bar, bar + 1, err)) return;
     block_reduce_all(pa, nv, nblk, ca);
@@ -361,13 +374,13 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
     // pass 2: W' = W - U diag(s^2) a; b = U^T W', ||W'||^2
     for (int r = k0 + 4 * threadIdx.x; r < k1; r += 4 * blockDim.x) {
         double acc[4];
-        quad_combine(U, ld, coef, nv, r, acc);
+        quad_combine(UR, coef, nv, r, acc);
 #pragma unroll
         for (int e = 0; e < 4; ++e)
             if (r + e < k1) Ws[r + e - k0] -= acc[e];
     }
     __syncthreads();
-    block_dots(U, ld, Ws, k0, k1, nv, true, red, cb);
+    block_dots(UR, Ws, k0, k1, nv, true, red, cb);
     for (int i = threadIdx.x; i <= nv; i += blockDim.x) pb[(size_t)blockIdx.x * (nv + 1) + i] = cb[i];
     if (!grid_barrier(bar, bar + 1, err)) return;
     block_reduce_all(pb, nv + 1, nblk, cb);
@@ -384,7 +397,7 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
     B* Un = U + ld * nv;
     for (int r = k0 + 4 * threadIdx.x; r < k1; r += 4 * blockDim.x) {
         double acc[4];
-        quad_combine(U, ld, coef, nv, r, acc);
+        quad_combine(UR, coef, nv, r, acc);
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const int k = r + e;
@@ -395,34 +408,46 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
             }
         }
     }
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    if (blockIdx.x != 0) return;
+    // block 0: the Hessenberg column (in ca) and the earlier rotations are
+    // loaded by the whole block into shared memory; one thread then applies
+    // the rotations in sequence, carrying the running entry in a register
+    __shared__ double rc[64], rs[64];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) ca[i] = scale[i] * (ca[i] + cb[i]);
+    for (int i = threadIdx.x; i < j; i += blockDim.x) { rc[i] = cs[i]; rs[i] = sn[i]; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     scale[nv] = snv;
     // ||t||_wrms^2 = sum_k (s U_k)^2 / N
     const double tw = snv * snv * nrm2 / (double)N;
     *sigma_next = tw > 0.0 ? 1.0 / sqrt(tw) : 1.0;
     // Hessenberg column, rotations, least-squares residual
-    double hc[65];
-    for (int i = 0; i < nv; ++i) hc[i] = scale[i] * (ca[i] + cb[i]);
+    double* hc = ca;
     const double hn = sqrt(nrm2);
     hc[nv] = hn;
     if (!isfinite(hn) || !isfinite(hc[j])) {
         st->done = 3;
         return;
     }
+    double cur = hc[0];
     for (int i = 0; i < j; ++i) {
-        const double t0 = cs[i] * hc[i] + sn[i] * hc[i + 1];
-        const double t1 = -sn[i] * hc[i] + cs[i] * hc[i + 1];
-        hc[i] = t0;
-        hc[i + 1] = t1;
+        const double nx = hc[i + 1];
+        hc[i] = rc[i] * cur + rs[i] * nx;
+        cur = -rs[i] * cur + rc[i] * nx;
     }
+    hc[j] = cur;
     const double den = hypot(hc[j], hc[j + 1]);
-    if (den == 0.0) { cs[j] = 1.0; sn[j] = 0.0; }
-    else { cs[j] = hc[j] / den; sn[j] = hc[j + 1] / den; }
+    double cj_, sj_;
+    if (den == 0.0) { cj_ = 1.0; sj_ = 0.0; }
+    else { cj_ = hc[j] / den; sj_ = hc[j + 1] / den; }
+    cs[j] = cj_;
+    sn[j] = sj_;
     hc[j] = den;
-    g[j + 1] = -sn[j] * g[j];
-    g[j] = cs[j] * g[j];
+    const double gj = g[j];
+    g[j + 1] = -sj_ * gj;
+    g[j] = cj_ * gj;
     for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hc[i];
-    const double rn = fabs(g[j + 1]) / st->sqrtN;
+    const double rn = fabs(-sj_ * gj) / st->sqrtN;
     st->rnorm = rn;
     st->j = j + 1;
     if (rn <= st->tol || hn == 0.0) st->done = 1;
@@ -535,12 +560,12 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
         FVM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         // one block per SM: fewer arrivals at each grid barrier; the block's
         // rows of W (at most 48 KB) live in its shared memory
-        const size_t wsm = sizeof(double) * (size_t)cgs_chunk(c->N, nsm);
-        if (precision)
-            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<float>, kCgsThreads, wsm));
-        else
-            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_cgs2<double>, kCgsThreads, wsm));
-        K->coop_grid = (coop && per_sm > 0 && m + 1 <= 63 && wsm <= 48 * 1024) ? nsm : 0;
+        const void* kfn = precision ? (const void*)k_arnoldi_cgs2<float> : (const void*)k_arnoldi_cgs2<double>;
+        K->coop_smem = sizeof(double) * (size_t)cgs_chunk(c->N, nsm);
+        const bool fits = K->coop_smem <= 48 * 1024;
+        if (fits)
+            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kCgsThreads, K->coop_smem));
+        K->coop_grid = (coop && fits && per_sm > 0 && m + 1 <= 63) ? nsm : 0;
     }
     K->res.alloc(3 * (m + 2) + 8);
     K->sigma.alloc(1);
@@ -679,9 +704,8 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                     double* sgp = K->sigma.p;
                     void* args[] = {&Ni, &stp, &Ub, &ldv, &scp, &jvp, &ew, &Wp, &pp, &bp, &ep, &tp, &sgp,
                                     &H_d, &cs_d, &sn_d, &g_d};
-                    const size_t wsm = sizeof(double) * (size_t)cgs_chunk(N, K->coop_grid);
                     FVM_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi_cgs2<B>, dim3(K->coop_grid),
-                                                         dim3(kCgsThreads), args, wsm, s));
+                                                         dim3(kCgsThreads), args, K->coop_smem, s));
                     c->launches++;
                     c->tm.end(TM_CGS, s);
                 }

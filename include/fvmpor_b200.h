@@ -302,13 +302,15 @@ typedef struct {
 void fvm_opts_default(fvm_opts* o);
 
 /* One accepted BDF step of the last integration on a context: its end
- * time, step size, order, local error test value (<= 1 accepts), the
- * attempts it took (error-test or corrector failures + 1) and the Newton
- * iterations, Krylov iterations and preconditioner set-ups spent on it,
- * and whether the corrector started from the learned iterate.  The
- * reference prints the same counters in aggregate (fvmpor_ODE.cpp:35-61). */
+ * time, step size, order, local error test value (<= 1 accepts), the host
+ * wall-clock seconds since the integration started when the step was
+ * accepted, the attempts it took (error-test or corrector failures + 1)
+ * and the Newton iterations, Krylov iterations and preconditioner set-ups
+ * spent on it, and whether the corrector started from the learned iterate.
+ * The reference prints the same counters in aggregate
+ * (fvmpor_ODE.cpp:35-61). */
 typedef struct {
-    double t, h, err;
+    double t, h, err, wall;
     int order, attempts, nni, nli, npe, learned;
 } fvm_step_record;
 
