@@ -49,6 +49,14 @@ struct BlockILU {
     DevBuf<double> krwb, krwp, dstor;
     int nb = 0, maxb = 0;
     DevBuf<int> bstart, lu_ptr, lu_src, lu_diag;
+    // ILU(0) elimination schedule of the shared-memory factorisation, one
+    // contiguous segment per level (upd[seg_ptr[g] .. seg_ptr[g+1]) for the
+    // global level g): the offset of each row's list in the segment, then
+    // per row and per L entry in column order a count word followed by that
+    // many (target | source << 16) window positions
+    DevBuf<int> seg_ptr;
+    DevBuf<unsigned> upd;
+    int scr_words[2] = {0, 0};   // shared-memory schedule scratch of the factorisation (words), by precision
     DevBuf<unsigned short> lu_col;
     DevBuf<int> lvl_ptr, lvl_rows, blk_lvl, ulvl_ptr, ulvl_rows, blk_ulvl;
     DevBuf<unsigned short> meta;   // per-block metadata records of the staged apply
@@ -127,7 +135,9 @@ __global__ void k_fd_node(int N, const double* __restrict__ y, const double* __r
 // per element: the npe x npe changes of its corner partials, one column
 // (perturbed node m) at a time, divided by d_m, into their slots
 template <int NPE, int NFE, bool RC, bool MZ>
-__global__ void __launch_bounds__(256) k_fd_elem(int T, int N, const int4* __restrict__ en,
+// (two blocks per SM: 128 registers, no spills; the unbounded build took
+// 130 and ran one block of 8 warps per SM)
+__global__ void __launch_bounds__(256, 2) k_fd_elem(int T, int N, const int4* __restrict__ en,
                                                  const double* __restrict__ coef, const double* __restrict__ xyz,
                                                  const double* __restrict__ eK, int kiso, int estride,
                                                  const int* __restrict__ ezone, const double* __restrict__ y,
@@ -522,6 +532,9 @@ __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__
                                                          const int* __restrict__ lvl_ptr,
                                                          const int* __restrict__ lvl_rows,
                                                          const int* __restrict__ blk_lvl,
+                                                         const int* __restrict__ seg_ptr,
+                                                         const unsigned* __restrict__ upd, int scr_off,
+                                                         int scr_words,
                                                          const double* __restrict__ J, T* __restrict__ lu,
                                                          int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -549,19 +562,35 @@ __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__
     }
     for (int l = threadIdx.x; l <= nl; l += blockDim.x) lptr[l] = (unsigned short)(lvl_ptr[la + l] - lq0);
     __syncthreads();
+    // each level's schedule segment goes to shared memory by one coalesced
+    // copy of the whole block (read in place from global when it is larger
+    // than the scratch), so a row's update chain never waits on global loads
+    unsigned* scr = reinterpret_cast<unsigned*>(smem_raw + scr_off);
     for (int l = 0; l < nl; ++l) {
-        for (int q = lptr[l] + threadIdx.x; q < lptr[l + 1]; q += blockDim.x) {
-            int li = lrow[q];
-            int s0 = rp[li], s1 = rp[li + 1], di = dg[li];
+        const int sg0 = seg_ptr[la + l], len = seg_ptr[la + l + 1] - sg0;
+        const unsigned* L = upd + sg0;
+        if (len <= scr_words) {
+#pragma unroll 4
+            for (int t = threadIdx.x; t < len; t += blockDim.x) scr[t] = L[t];
+            __syncthreads();
+            L = scr;
+        }
+        const int q0 = lptr[l], nq = lptr[l + 1] - q0;
+        for (int qq = threadIdx.x; qq < nq; qq += blockDim.x) {
+            int li = lrow[q0 + qq];
+            int s0 = rp[li], di = dg[li];
+            // IKJ with the precomputed schedule: the updates of the L entry
+            // kk, in the order a merge of row li with U(k) would find them
+            int t = (int)L[qq];
             for (int kk = s0; kk < di; ++kk) {
-                int k = col[kk];
+                const int cnt = (int)L[t++];
+                const int k = col[kk];
                 T lik = val[kk] * val[dg[k]];
                 val[kk] = lik;
-                int kpos = dg[k] + 1, kend = rp[k + 1];
-                for (int jj = kk + 1; jj < s1 && kpos < kend; ++jj) {
-                    int j = col[jj];
-                    while (kpos < kend && col[kpos] < j) ++kpos;
-                    if (kpos < kend && col[kpos] == j) val[jj] = val[jj] - lik * val[kpos];
+                for (int u = 0; u < cnt; ++u) {
+                    const unsigned pr = L[t++];
+                    const int jj = (int)(pr & 0xffffu), kp = (int)(pr >> 16);
+                    val[jj] = val[jj] - lik * val[kp];
                 }
             }
             T d = val[di];
@@ -711,6 +740,43 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
         }
         blk_ulvl.push_back((int)ulvl_ptr.size() - 1);
     }
+    // elimination schedule in level order (window positions relative to
+    // each block's 8-aligned window base, as the factorisation indexes); the
+    // same update set and order as merging row i with U(k) for each L entry
+    std::vector<int> seg_ptr(lvl_ptr.size(), 0);
+    std::vector<unsigned> upd;
+    size_t seg_max = 0;
+    for (int b = 0; b < nb; ++b) {
+        const int r0 = bstart[b];
+        const int base = lu_ptr[r0] & ~7;
+        for (int g = blk_lvl[b]; g < blk_lvl[b + 1]; ++g) {
+            seg_ptr[g] = (int)upd.size();
+            const int q0 = lvl_ptr[g], q1 = lvl_ptr[g + 1];
+            const size_t head = upd.size();
+            upd.resize(head + (q1 - q0), 0u);
+            for (int q = q0; q < q1; ++q) {
+                const int i = lvl_rows[q];
+                upd[head + (q - q0)] = (unsigned)(upd.size() - head);
+                for (int p = lu_ptr[i]; p < lu_diag[i]; ++p) {
+                    const size_t cw = upd.size();
+                    upd.push_back(0u);
+                    const int k = r0 + lu_col[p];
+                    int kpos = lu_diag[k] + 1;
+                    const int kend = lu_ptr[k + 1];
+                    for (int jj = p + 1; jj < lu_ptr[i + 1] && kpos < kend; ++jj) {
+                        const int j = lu_col[jj];
+                        while (kpos < kend && lu_col[kpos] < j) ++kpos;
+                        if (kpos < kend && lu_col[kpos] == j)
+                            upd.push_back((unsigned)(jj - base) | ((unsigned)(kpos - base) << 16));
+                    }
+                    upd[cw] = (unsigned)(upd.size() - cw - 1);
+                }
+            }
+            seg_max = std::max(seg_max, upd.size() - head);
+        }
+        seg_ptr[blk_lvl[b + 1]] = (int)upd.size();
+    }
+    if (upd.size() >= (size_t)INT32_MAX) throw Error("block-ILU: elimination schedule too large");
     P->nb = nb;
     P->maxb = maxb;
     P->nlevels_max = nlmax;
@@ -750,6 +816,11 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
         }
         P->smem_stage[0] = (fits16 && need64 <= kMaxDynSmem) ? need64 : 0;
         P->smem_stage[1] = (fits16 && need32 <= kMaxDynSmem) ? need32 : 0;
+        for (int pr = 0; pr < 2; ++pr) {
+            const size_t st = round16(P->smem_stage[pr]);
+            const size_t room = P->smem_stage[pr] && st < kMaxDynSmem ? (kMaxDynSmem - st) / 4 : 0;
+            P->scr_words[pr] = (int)std::min<size_t>(std::min<size_t>(seg_max, room), 8192);
+        }
         // entries per row held in registers by the staged triangular sweeps:
         // 8 covers the lower or upper part of a 3D row, 4 of a 2D row
         P->lanes = (double)lu_ptr[N] / N > 9.0 ? 8 : 4;
@@ -759,7 +830,7 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)P->smem_stage[0]));
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_factor_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)P->smem_stage[0]));
+                                          (int)(round16(P->smem_stage[0]) + 4 * (size_t)P->scr_words[0])));
         }
         if (P->smem_stage[1]) {
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -767,7 +838,7 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)P->smem_stage[1]));
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_factor_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)P->smem_stage[1]));
+                                          (int)(round16(P->smem_stage[1]) + 4 * (size_t)P->scr_words[1])));
         }
     }
     cudaStream_t s = c->stream;
@@ -789,6 +860,9 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
     P->lu_src.upload(lu_src, s);
     P->lu_diag.upload(lu_diag, s);
     P->lu_col.upload(lu_col, s);
+    if (upd.empty()) upd.push_back(0u);
+    P->seg_ptr.upload(seg_ptr, s);
+    P->upd.upload(upd, s);
     P->meta.upload(meta, s);
     P->meta_off.upload(meta_off, s);
     P->lvl_ptr.upload(lvl_ptr, s);
@@ -838,17 +912,19 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     size_t nlu = P->lu_src.n;
     c->tm.begin(TM_ILU_FACTOR, s);
     if (P->smem_stage[precision]) {
-        size_t sm = P->smem_stage[precision];
+        const int so = (int)round16(P->smem_stage[precision]);
+        const int sw = P->scr_words[precision];
+        size_t sm = (size_t)so + 4 * (size_t)sw;
         if (precision) {
             P->lu32.alloc(nlu);
             fvm_launch(c, k_ilu_factor_smem<float>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p,
-                       P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->J.p, P->lu32.p,
-                       P->status.p);
+                       P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->seg_ptr.p, P->upd.p,
+                       so, sw, P->J.p, P->lu32.p, P->status.p);
         } else {
             P->lu64.alloc(nlu);
             fvm_launch(c, k_ilu_factor_smem<double>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p,
-                       P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->J.p, P->lu64.p,
-                       P->status.p);
+                       P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->seg_ptr.p, P->upd.p,
+                       so, sw, P->J.p, P->lu64.p, P->status.p);
         }
     } else if (precision) {
         P->lu32.alloc(nlu);
