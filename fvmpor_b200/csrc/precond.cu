@@ -523,6 +523,9 @@ __global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __res
 // Shared-memory factorisation: gather the block's Jacobian entries into the
 // same copy window the apply uses, eliminate level by level in shared
 // memory (IKJ, pivots inverted after their row), write the block back.
+// schedule words of the next level each of the 256 threads holds
+constexpr int kIluFactorPre = 12;
+
 template <class T>
 __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__ bstart,
                                                          const int* __restrict__ lu_ptr,
@@ -562,19 +565,37 @@ __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__
     }
     for (int l = threadIdx.x; l <= nl; l += blockDim.x) lptr[l] = (unsigned short)(lvl_ptr[la + l] - lq0);
     __syncthreads();
-    // each level's schedule segment goes to shared memory by one coalesced
-    // copy of the whole block (read in place from global when it is larger
-    // than the scratch), so a row's update chain never waits on global loads
-    unsigned* scr = reinterpret_cast<unsigned*>(smem_raw + scr_off);
-    for (int l = 0; l < nl; ++l) {
-        const int sg0 = seg_ptr[la + l], len = seg_ptr[la + l + 1] - sg0;
-        const unsigned* L = upd + sg0;
-        if (len <= scr_words) {
+    // Each level's schedule segment is in shared memory when its rows run
+    // (read in place from global when it is larger than a buffer), so a
+    // row's update chain never waits on global loads: two buffers; while a
+    // level's rows run, every thread holds its share of the next level's
+    // segment in registers (loads issued before the rows, stored after).
+    unsigned* const buf0 = reinterpret_cast<unsigned*>(smem_raw + scr_off);
+    unsigned* const buf1 = buf0 + scr_words;
+    int sgc = seg_ptr[la], lenc = seg_ptr[la + 1] - sgc;
+    bool cur_smem = lenc <= scr_words;
+    if (cur_smem) {
 #pragma unroll 4
-            for (int t = threadIdx.x; t < len; t += blockDim.x) scr[t] = L[t];
-            __syncthreads();
-            L = scr;
+        for (int t = threadIdx.x; t < lenc; t += blockDim.x) buf0[t] = upd[sgc + t];
+    }
+    __syncthreads();
+    for (int l = 0; l < nl; ++l) {
+        int sgn = 0, lenn = 0;
+        bool nxt_smem = false;
+        unsigned pre[kIluFactorPre];
+        if (l + 1 < nl) {
+            sgn = seg_ptr[la + l + 1];
+            lenn = seg_ptr[la + l + 2] - sgn;
+            nxt_smem = lenn <= scr_words;
+            if (nxt_smem) {
+#pragma unroll
+                for (int i = 0; i < kIluFactorPre; ++i) {
+                    const int t = threadIdx.x + i * blockDim.x;
+                    pre[i] = t < lenn ? upd[sgn + t] : 0u;
+                }
+            }
         }
+        const unsigned* L = cur_smem ? ((l & 1) ? buf1 : buf0) : upd + sgc;
         const int q0 = lptr[l], nq = lptr[l + 1] - q0;
         for (int qq = threadIdx.x; qq < nq; qq += blockDim.x) {
             int li = lrow[q0 + qq];
@@ -600,7 +621,18 @@ __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__
             }
             val[di] = (T)1 / d;
         }
+        if (nxt_smem) {
+            unsigned* nb = (l & 1) ? buf0 : buf1;   // the buffer of level l - 1, finished
+#pragma unroll
+            for (int i = 0; i < kIluFactorPre; ++i) {
+                const int t = threadIdx.x + i * blockDim.x;
+                if (t < lenn) nb[t] = pre[i];
+            }
+        }
         __syncthreads();
+        sgc = sgn;
+        lenc = lenn;
+        cur_smem = nxt_smem;
     }
     for (int p = e0 + threadIdx.x; p < e1; p += blockDim.x) lu[p] = val[p - w.base];
 }
@@ -816,10 +848,12 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
         }
         P->smem_stage[0] = (fits16 && need64 <= kMaxDynSmem) ? need64 : 0;
         P->smem_stage[1] = (fits16 && need32 <= kMaxDynSmem) ? need32 : 0;
+        // two schedule buffers of scr_words words (at most what 256 threads
+        // hold in kIluFactorPre registers each)
         for (int pr = 0; pr < 2; ++pr) {
             const size_t st = round16(P->smem_stage[pr]);
-            const size_t room = P->smem_stage[pr] && st < kMaxDynSmem ? (kMaxDynSmem - st) / 4 : 0;
-            P->scr_words[pr] = (int)std::min<size_t>(std::min<size_t>(seg_max, room), 8192);
+            const size_t room = P->smem_stage[pr] && st < kMaxDynSmem ? (kMaxDynSmem - st) / 8 : 0;
+            P->scr_words[pr] = (int)std::min<size_t>(std::min<size_t>(seg_max, room), 256 * kIluFactorPre);
         }
         // entries per row held in registers by the staged triangular sweeps:
         // 8 covers the lower or upper part of a 3D row, 4 of a 2D row
@@ -830,7 +864,7 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)P->smem_stage[0]));
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_factor_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)(round16(P->smem_stage[0]) + 4 * (size_t)P->scr_words[0])));
+                                          (int)(round16(P->smem_stage[0]) + 8 * (size_t)P->scr_words[0])));
         }
         if (P->smem_stage[1]) {
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -838,7 +872,7 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)P->smem_stage[1]));
             FVM_CUDA(cudaFuncSetAttribute(k_ilu_factor_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)(round16(P->smem_stage[1]) + 4 * (size_t)P->scr_words[1])));
+                                          (int)(round16(P->smem_stage[1]) + 8 * (size_t)P->scr_words[1])));
         }
     }
     cudaStream_t s = c->stream;
@@ -914,7 +948,7 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     if (P->smem_stage[precision]) {
         const int so = (int)round16(P->smem_stage[precision]);
         const int sw = P->scr_words[precision];
-        size_t sm = (size_t)so + 4 * (size_t)sw;
+        size_t sm = (size_t)so + 8 * (size_t)sw;
         if (precision) {
             P->lu32.alloc(nlu);
             fvm_launch(c, k_ilu_factor_smem<float>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p,
