@@ -151,9 +151,11 @@ struct Oracle {
     int ncol = 0;
     std::vector<double> J;
     std::vector<int> bstart;
-    std::vector<int> diagpos;
-    std::vector<double> LU;   // ILU(0) of the block-diagonal part, stored over the full pattern
-    std::vector<char> inblock;
+    // ILU(0) of the block-diagonal part, each block's rows in colour order:
+    // factor position q is global row frow[q]; fptr/fcol/fdiag index
+    // positions, fsrc the source entry of J
+    std::vector<int> frow, fptr, fcol, fsrc, fdiag;
+    std::vector<double> LU;
 
     void build(const fvm_mesh* m, const fvm_physics* ph);
     void residual(double t, const double* y, const double* yp, double* res);
@@ -723,41 +725,84 @@ void Oracle::psetup(double t, double cj, double hh, const double* y, const doubl
     for (int b = 0; b <= nb; ++b) bstart[b] = (int)(((long)N * b) / nb);
 }
 
-// ILU(0) on the block-diagonal part (decomp/ILU.c:12-115, pivot of row i
-// inverted after its elimination)
-int Oracle::ilu_factor() {
-    LU = J;
-    diagpos.assign(N, -1);
-    inblock.assign(jcol.size(), 0);
-    int nb = (int)bstart.size() - 1;
-    std::vector<int> blk(N);
-    for (int b = 0; b < nb; ++b)
-        for (int i = bstart[b]; i < bstart[b + 1]; ++i) blk[i] = b;
-    for (int i = 0; i < N; ++i)
+// Colour order of the rows [r0, r1) of a block (offsets from r0): greedy
+// colouring in natural order (smallest colour unused by an earlier coupled
+// row of the block), then stable by colour.  The same rule as the device
+// factor's set-up: rows of one colour are uncoupled, so each triangular
+// sweep of a block has as many levels as colours.
+static std::vector<int> block_colour_order(const std::vector<int>& jrow, const std::vector<int>& jcol, int r0,
+                                           int r1) {
+    const int nr = r1 - r0;
+    std::vector<int> colour(nr, 0), ord(nr);
+    for (int i = r0; i < r1; ++i) {
+        std::vector<int> used;
         for (int p = jrow[i]; p < jrow[i + 1]; ++p) {
-            inblock[p] = blk[jcol[p]] == blk[i];
-            if (jcol[p] == i) diagpos[i] = p;
+            const int j = jcol[p];
+            if (j >= r0 && j < i) used.push_back(colour[j - r0]);
         }
+        std::sort(used.begin(), used.end());
+        int cc = 0;
+        for (int u : used)
+            if (u == cc) ++cc;
+        colour[i - r0] = cc;
+    }
+    for (int ii = 0; ii < nr; ++ii) ord[ii] = ii;
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return colour[a] < colour[b]; });
+    return ord;
+}
+
+// ILU(0) on the block-diagonal part (decomp/ILU.c:12-115, pivot of row i
+// inverted after its elimination), each block in its colour order
+int Oracle::ilu_factor() {
+    int nb = (int)bstart.size() - 1;
+    frow.assign(N, 0);
+    fptr.assign(N + 1, 0);
+    fdiag.assign(N, -1);
+    fcol.clear();
+    fsrc.clear();
+    std::vector<std::pair<int, int>> ent;
+    for (int b = 0; b < nb; ++b) {
+        const int r0 = bstart[b], r1 = bstart[b + 1];
+        const std::vector<int> ord = block_colour_order(jrow, jcol, r0, r1);
+        std::vector<int> linv(r1 - r0);
+        for (int ii = 0; ii < r1 - r0; ++ii) linv[ord[ii]] = ii;
+        for (int ii = 0; ii < r1 - r0; ++ii) {
+            const int i = r0 + ord[ii], q = r0 + ii;
+            frow[q] = i;
+            ent.clear();
+            for (int p = jrow[i]; p < jrow[i + 1]; ++p) {
+                const int j = jcol[p];
+                if (j >= r0 && j < r1) ent.emplace_back(r0 + linv[j - r0], p);
+            }
+            std::sort(ent.begin(), ent.end());
+            for (auto& e : ent) {
+                if (e.first == q) fdiag[q] = (int)fcol.size();
+                fcol.push_back(e.first);
+                fsrc.push_back(e.second);
+            }
+            fptr[q + 1] = (int)fcol.size();
+        }
+    }
+    LU.resize(fcol.size());
+    for (size_t p = 0; p < fcol.size(); ++p) LU[p] = J[fsrc[p]];
     int bad = 0;
 #pragma omp parallel for schedule(dynamic) reduction(+ : bad)
     for (int b = 0; b < nb; ++b) {
         for (int i = bstart[b]; i < bstart[b + 1]; ++i) {
-            for (int kk = jrow[i]; kk < diagpos[i]; ++kk) {
-                if (!inblock[kk]) continue;
-                int k = jcol[kk];
-                LU[kk] *= LU[diagpos[k]];
-                int kpos = diagpos[k] + 1;
-                for (int jj = kk + 1; jj < jrow[i + 1]; ++jj) {
-                    if (!inblock[jj]) continue;
-                    int j = jcol[jj];
-                    while (kpos < jrow[k + 1] && jcol[kpos] < j) ++kpos;
-                    if (kpos == jrow[k + 1]) break;
-                    if (jcol[kpos] == j && inblock[kpos]) LU[jj] -= LU[kk] * LU[kpos];
+            for (int kk = fptr[i]; kk < fdiag[i]; ++kk) {
+                int k = fcol[kk];
+                LU[kk] *= LU[fdiag[k]];
+                int kpos = fdiag[k] + 1;
+                for (int jj = kk + 1; jj < fptr[i + 1]; ++jj) {
+                    int j = fcol[jj];
+                    while (kpos < fptr[k + 1] && fcol[kpos] < j) ++kpos;
+                    if (kpos == fptr[k + 1]) break;
+                    if (fcol[kpos] == j) LU[jj] -= LU[kk] * LU[kpos];
                 }
             }
-            double d = LU[diagpos[i]];
+            double d = LU[fdiag[i]];
             if (d == 0.0 || !std::isfinite(d)) { bad++; d = 1.0; }
-            LU[diagpos[i]] = 1.0 / d;
+            LU[fdiag[i]] = 1.0 / d;
         }
     }
     return bad ? 1 : 0;
@@ -767,18 +812,19 @@ void Oracle::psolve(const double* r, double* z) const {
     int nb = (int)bstart.size() - 1;
 #pragma omp parallel for schedule(dynamic)
     for (int b = 0; b < nb; ++b) {
-        for (int i = bstart[b]; i < bstart[b + 1]; ++i) {
-            double acc = r[i];
-            for (int p = jrow[i]; p < diagpos[i]; ++p)
-                if (inblock[p]) acc -= LU[p] * z[jcol[p]];
-            z[i] = acc;
+        const int r0 = bstart[b], r1 = bstart[b + 1];
+        std::vector<double> x(r1 - r0);
+        for (int q = r0; q < r1; ++q) {
+            double acc = r[frow[q]];
+            for (int p = fptr[q]; p < fdiag[q]; ++p) acc -= LU[p] * x[fcol[p] - r0];
+            x[q - r0] = acc;
         }
-        for (int i = bstart[b + 1] - 1; i >= bstart[b]; --i) {
-            double acc = z[i];
-            for (int p = diagpos[i] + 1; p < jrow[i + 1]; ++p)
-                if (inblock[p]) acc -= LU[p] * z[jcol[p]];
-            z[i] = acc * LU[diagpos[i]];
+        for (int q = r1 - 1; q >= r0; --q) {
+            double acc = x[q - r0];
+            for (int p = fdiag[q] + 1; p < fptr[q + 1]; ++p) acc -= LU[p] * x[fcol[p] - r0];
+            x[q - r0] = acc * LU[fdiag[q]];
         }
+        for (int q = r0; q < r1; ++q) z[frow[q]] = x[q - r0];
     }
 }
 
