@@ -527,7 +527,7 @@ __global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __res
 // same copy window the apply uses, eliminate level by level in shared
 // memory (IKJ, pivots inverted after their row), write the block back.
 // schedule words of the next level each of the 256 threads holds
-constexpr int kIluFactorPre = 12;
+constexpr int kIluFactorPre = 32;
 
 template <class T>
 __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__ bstart,
