@@ -50,6 +50,7 @@ __global__ void k_node(int N, const double* __restrict__ y, const double* __rest
                        const int* __restrict__ nz_ptr, const int* __restrict__ nz_zone,
                        const double* __restrict__ nz_w, double rho0, double* __restrict__ krw,
                        double* __restrict__ hstar, double* __restrict__ stor, NodeCopies cp) {
+    pdl_wait_and_trigger();
     if (pt.skip && *pt.skip) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
@@ -206,6 +207,7 @@ __global__ void __launch_bounds__(kElemThreads) k_elem_chunk(ElemArgs a) {
     double* cc = reinterpret_cast<double*>(smem_e + 2 * L.bytes);               // [NPE][CE]
     int4* meta = reinterpret_cast<int4*>(cc + (size_t)NPE * a.CE);                // [2]
     uint64_t* full = reinterpret_cast<uint64_t*>(meta + 2);                      // [2]
+    pdl_wait_and_trigger();
     if ((int)blockIdx.x >= a.nch) return;
     if (a.skip && *a.skip) return;
     if (threadIdx.x == 0) {
@@ -321,6 +323,7 @@ __global__ void __launch_bounds__(kElemThreads) k_elem_chunk(ElemArgs a) {
 // part_ptr[i+1]) in ascending chunk order; sum them in that order.
 // F0 != nullptr turns the result into (F - F0) * inv_sigma.
 __global__ void k_gather(int N, GatherSrc g, double* __restrict__ out, const int* __restrict__ skip) {
+    pdl_wait_and_trigger();
     if (skip && *skip) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
@@ -443,7 +446,7 @@ static void launch_elem(fvm_ctx* c, const double* h, const int* skip = nullptr) 
     a.coef = c->coef.p; a.ch_xyz = c->ch_xyz.p; a.eK = c->eK.p; a.ezone = c->ezone.p;
     a.krw = c->krw.p; a.ch_h = c->ch_h.p; a.ch_krw = c->ch_krw.p; a.upw = c->upw.p; a.rho0 = c->rho0;
     a.part = c->part.p; a.err = c->elem_err.p; a.P = c->ch_node.n;
-    with_elem_kernel(c, [&](auto k) { fvm_launch(c, k, c->chunk_grid, kElemThreads, c->chunk_smem, c->stream, a); });
+    with_elem_kernel(c, [&](auto k) { fvm_launch_pdl(c, k, c->chunk_grid, kElemThreads, c->chunk_smem, c->stream, a); });
 }
 
 // Chunk the elements (consecutive ids, CE per chunk) and build the tables
@@ -550,9 +553,8 @@ GatherSrc launch_residual_partials(fvm_ctx* c, const double* y, const double* yp
     cudaStream_t s = c->stream;
     const double* h = pt.mode ? c->hstar.p : y;
     c->tm.begin(TM_NODE, s);
-    fvm_launch(c, k_node, grid_for(c->N, kBlock), kBlock, 0, s, c->N, y, yp, pt, c->zones.p, c->nz, c->nz_ptr.p,
-                                                      c->nz_zone.p, c->nz_w.p, c->rho0, c->krw.p,
-                                                      c->hstar.p, c->stor.p, node_copies(c));
+    fvm_launch_pdl(c, k_node, grid_for(c->N, kBlock), kBlock, 0, s, c->N, y, yp, pt, c->zones.p, c->nz, c->nz_ptr.p,
+                   c->nz_zone.p, c->nz_w.p, c->rho0, c->krw.p, c->hstar.p, c->stor.p, node_copies(c));
     c->tm.end(TM_NODE, s);
     c->tm.begin(TM_ELEM, s);
     launch_elem(c, h, pt.skip);
@@ -576,7 +578,7 @@ GatherSrc launch_residual_partials(fvm_ctx* c, const double* y, const double* yp
 
 void gather_into(fvm_ctx* c, const GatherSrc& g, double* out, const int* skip) {
     c->tm.begin(TM_GATHER, c->stream);
-    fvm_launch(c, k_gather, grid_for(c->N, kBlock), kBlock, 0, c->stream, c->N, g, out, skip);
+    fvm_launch_pdl(c, k_gather, grid_for(c->N, kBlock), kBlock, 0, c->stream, c->N, g, out, skip);
     c->tm.end(TM_GATHER, c->stream);
 }
 

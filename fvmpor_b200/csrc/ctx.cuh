@@ -258,6 +258,37 @@ inline void fvm_launch(fvm_ctx* c, void (*k)(KArgs...), dim3 grid, dim3 block, s
     c->launches++;
 }
 
+// Programmatic dependent launch for the short kernels of the Krylov step
+// (node pass, element pass, gather, preconditioner apply): the launch may
+// be processed, and the kernel's blocks made resident, while the previous
+// kernel on the stream finishes.  Every kernel launched this way calls
+// pdl_wait_and_trigger() first, so it reads nothing before its predecessor
+// has completed and its writes are visible.
+template <typename... KArgs, typename... Args>
+inline void fvm_launch_pdl(fvm_ctx* c, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                           cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    FVM_CUDA(cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...));
+    c->launches++;
+}
+
+// first statement of a kernel launched by fvm_launch_pdl: wait for the
+// previous kernel's completion (a no-op after an ordinary launch), then let
+// the next programmatic launch begin
+__device__ __forceinline__ void pdl_wait_and_trigger() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // residual driver shared by fvm_residual / fvm_jv / the FD Jacobian
 // out = F(t, y~, y'~) (or (F - F0) / sigma when F0 != nullptr)
 void launch_residual(fvm_ctx* c, const double* y, const double* yp, const Perturb& pt,

@@ -300,6 +300,7 @@ __global__ void __launch_bounds__(128) k_ilu_apply(const int* __restrict__ bstar
                                                    const double* __restrict__ r,
                                                    double* __restrict__ z, const int* __restrict__ skip) {
     extern __shared__ unsigned char smem_raw[];
+    pdl_wait_and_trigger();
     if (skip && *skip) return;
     T* x = reinterpret_cast<T*>(smem_raw);
     int b = blockIdx.x;
@@ -481,6 +482,7 @@ __global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __res
                                                         double* __restrict__ z, int* __restrict__ err,
                                                         const int* __restrict__ skip) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_wait_and_trigger();
     if (skip && *skip) return;
     const int b = blockIdx.x;
     const int r0 = bstart[b], r1 = bstart[b + 1], nr = r1 - r0;
@@ -1055,7 +1057,7 @@ void psolve_dev(fvm_ctx* c, const double* r, double* z, const int* skip) {
     if (P->smem_stage[P->factored]) {
         size_t sm = P->smem_stage[P->factored];
         auto go = [&](auto kern, const auto* lu) {
-            fvm_launch(c, kern, P->nb, P->apply_threads, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_col.p, P->meta.p,
+            fvm_launch_pdl(c, kern, P->nb, P->apply_threads, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_col.p, P->meta.p,
                        P->meta_off.p, P->blk_lvl.p, P->blk_ulvl.p, lu, P->lu_row.p, r, z, P->status.p, skip);
         };
         if (P->factored) {
@@ -1067,12 +1069,12 @@ void psolve_dev(fvm_ctx* c, const double* r, double* z, const int* skip) {
         }
     } else if (P->factored) {
         size_t sm = sizeof(float) * P->maxb;
-        fvm_launch(c, k_ilu_apply<float>, P->nb, 128, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
+        fvm_launch_pdl(c, k_ilu_apply<float>, P->nb, 128, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
                                                  P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p, P->ulvl_rows.p,
                                                  P->blk_ulvl.p, P->lu32.p, P->lu_row.p, r, z, skip);
     } else {
         size_t sm = sizeof(double) * P->maxb;
-        fvm_launch(c, k_ilu_apply<double>, P->nb, 128, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
+        fvm_launch_pdl(c, k_ilu_apply<double>, P->nb, 128, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p,
                                                   P->lvl_rows.p, P->blk_lvl.p, P->ulvl_ptr.p, P->ulvl_rows.p,
                                                   P->blk_ulvl.p, P->lu64.p, P->lu_row.p, r, z, skip);
     }
