@@ -482,8 +482,6 @@ __global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __res
                                                         double* __restrict__ z, int* __restrict__ err,
                                                         const int* __restrict__ skip) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    pdl_wait_and_trigger();
-    if (skip && *skip) return;
     const int b = blockIdx.x;
     const int r0 = bstart[b], r1 = bstart[b + 1], nr = r1 - r0;
     const IluWindow w = ilu_window(lu_ptr[r0], lu_ptr[r1]);
@@ -506,9 +504,18 @@ __global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __res
     __syncthreads();
     // factor window and the block's metadata record (row pointers, pivot
     // positions, level lists) by three bulk copies; the right-hand side by
-    // the threads meanwhile
+    // the threads meanwhile.  The copies read only set-up data, so they are
+    // issued before the wait for the previous kernel (the factorisation has
+    // completed before any kernel that lets this launch start early); the
+    // right-hand side and the skip flag are read after it.
     const int mo = meta_off[b];
     ilu_stage_bulk(val, col, lu, lu_col, w, bar, rp, meta + mo, meta_off[b + 1] - mo);
+    pdl_wait_and_trigger();
+    if (skip && *skip) {
+        // a step queued after the stop: let the copies land (bounded), leave
+        tc05::mbar_wait(bar, 0);
+        return;
+    }
     for (int i = threadIdx.x; i < nr; i += blockDim.x) x[i] = (T)r[lu_row[r0 + i]];
     bool ok = tc05::mbar_wait(bar, 0);
     if (!ok) ok = tc05::mbar_wait(bar, 0);   // copies in flight get a second bounded chance
