@@ -354,6 +354,9 @@ __global__ void __launch_bounds__(kCgsThreads) k_arnoldi_cgs2(int N, ArnState* s
     __shared__ double red[(kCgsThreads / 32) * kCgsGroup];
     extern __shared__ double Ws[];   // this block's rows of W (the vector being orthogonalised)
     (void)W;
+    // launched as a programmatic dependent of the preconditioner apply, and
+    // lets the next step's node pass launch early in turn
+    pdl_wait_and_trigger();
     if (st->done) return;            // the device-driven loop has finished
     const int j = st->j, nv = j + 1, m = st->m;
     const int nblk = gridDim.x;
@@ -704,8 +707,24 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                     double* sgp = K->sigma.p;
                     void* args[] = {&Ni, &stp, &Ub, &ldv, &scp, &jvp, &ew, &Wp, &pp, &bp, &ep, &tp, &sgp,
                                     &H_d, &cs_d, &sn_d, &g_d};
-                    FVM_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi_cgs2<B>, dim3(K->coop_grid),
-                                                         dim3(kCgsThreads), args, K->coop_smem, s));
+                    // cooperative (grid barriers) and a programmatic dependent
+                    // of the apply: its blocks take their SM slots while the
+                    // apply finishes, then wait for it at entry
+                    cudaLaunchConfig_t cfg = {};
+                    cfg.gridDim = dim3(K->coop_grid);
+                    cfg.blockDim = dim3(kCgsThreads);
+                    cfg.dynamicSmemBytes = K->coop_smem;
+                    cfg.stream = s;
+                    cudaLaunchAttribute attr[2];
+                    attr[0].id = cudaLaunchAttributeCooperative;
+                    attr[0].val.cooperative = 1;
+                    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                    attr[1].val.programmaticStreamSerializationAllowed = 1;
+                    cfg.attrs = attr;
+                    cfg.numAttrs = 2;
+                    (void)args;
+                    FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_cgs2<B>, Ni, stp, Ub, ldv, scp, (const double*)jvp,
+                                                (const double*)ew, Wp, pp, bp, ep, tp, sgp, H_d, cs_d, sn_d, g_d));
                     c->launches++;
                     c->tm.end(TM_CGS, s);
                 }
