@@ -705,8 +705,6 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                     int* ep = K->err.p;
                     double* tp = K->t.p;
                     double* sgp = K->sigma.p;
-                    void* args[] = {&Ni, &stp, &Ub, &ldv, &scp, &jvp, &ew, &Wp, &pp, &bp, &ep, &tp, &sgp,
-                                    &H_d, &cs_d, &sn_d, &g_d};
                     // cooperative (grid barriers) and a programmatic dependent
                     // of the apply: its blocks take their SM slots while the
                     // apply finishes, then wait for it at entry
@@ -722,7 +720,6 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                     attr[1].val.programmaticStreamSerializationAllowed = 1;
                     cfg.attrs = attr;
                     cfg.numAttrs = 2;
-                    (void)args;
                     FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_cgs2<B>, Ni, stp, Ub, ldv, scp, (const double*)jvp,
                                                 (const double*)ew, Wp, pp, bp, ep, tp, sgp, H_d, cs_d, sn_d, g_d));
                     c->launches++;
