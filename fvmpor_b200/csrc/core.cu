@@ -41,8 +41,8 @@ constexpr int kDefaultChunk = 512;   // elements per chunk of the element pass
 struct NodeCopies {
     const int* part_ptr = nullptr;   // [N+1]
     const int* cpos = nullptr;       // [P] chunk-major position of each copy
-    double* ch_h = nullptr;          // [P]
-    double* ch_krw = nullptr;        // [P] (single zone)
+    double* ch_h = nullptr;          // [P] (several zones)
+    double* ch_hk = nullptr;         // [P][2] (head, krw) pairs (one zone): one 16-byte store per copy
 };
 
 __global__ void k_node(int N, const double* __restrict__ y, const double* __restrict__ yp,
@@ -79,8 +79,7 @@ __global__ void k_node(int N, const double* __restrict__ y, const double* __rest
         dsw = d * nz_w[i];
         for (int q = c0; q < c1; ++q) {
             const int cm = cp.cpos[q];
-            cp.ch_h[cm] = h;
-            cp.ch_krw[cm] = k;
+            reinterpret_cast<double2*>(cp.ch_hk)[cm] = make_double2(h, k);
         }
     } else {
         for (int q = c0; q < c1; ++q) cp.ch_h[cp.cpos[q]] = h;
@@ -135,8 +134,8 @@ struct ElemArgs {
     const double* eK;             // VAR 1: [estride] (kiso) or [3][estride]
     const int* ezone;
     const double* krw;            // [nz][N] (several zones)
-    const double* ch_h;           // [P] chunk-major head (written by the node pass)
-    const double* ch_krw;         // [P] chunk-major krw (single zone)
+    const double* ch_h;           // [P] chunk-major head (written by the node pass; several zones)
+    const double* ch_hk;          // [P][2] chunk-major (head, krw) pairs (one zone)
     const unsigned char* upw;     // [8*estride]
     double rho0;
     double* part;                 // [P] chunk-major partials
@@ -154,6 +153,8 @@ struct StageLayout {
     size_t h, krw, xyz, eloc, upw, ek, lc, lp, bytes;
     __host__ __device__ StageLayout(int CE, int npe, int nnmax, bool mz, bool rc, bool kiso) {
         const size_t nd = (size_t)nnmax * 8;
+        // one zone: (head, krw) pairs in [h, h + 2 nd); several zones: head
+        // only (krw is read per zone from the node-major array)
         h = 0;
         krw = h + nd;
         xyz = krw + (mz ? 0 : nd);
@@ -185,8 +186,8 @@ __device__ __forceinline__ void elem_issue(const ElemArgs& a, const StageLayout&
                      (VAR1 ? (uint32_t)nep * 8 * (a.kiso ? 1 : 3) : 0) + (uint32_t)nep * NPE * 2 + (uint32_t)nnp * 2;
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc05::smem_u32(bar)), "r"(bytes)
                  : "memory");
-    bulk_g2s(st + L.h, a.ch_h + sg.x, nnp * 8, bar);
-    if (!MZ) bulk_g2s(st + L.krw, a.ch_krw + sg.x, nnp * 8, bar);
+    if (MZ) bulk_g2s(st + L.h, a.ch_h + sg.x, nnp * 8, bar);
+    else bulk_g2s(st + L.h, a.ch_hk + 2 * (size_t)sg.x, nnp * 16, bar);
     if (VAR1)
         for (int d = 0; d < 3; ++d) bulk_g2s(st + L.xyz + (size_t)d * a.nnmax * 8, a.ch_xyz + d * a.P + sg.x, nnp * 8, bar);
     bulk_g2s(st + L.eloc, a.elocal + e0, nep * 8, bar);
@@ -243,7 +244,6 @@ __global__ void __launch_bounds__(kElemThreads) k_elem_chunk(ElemArgs a) {
         const int j0 = md.x, nn = md.y, e0 = md.z, ne = md.w;
         const unsigned char* st = smem_e + s * L.bytes;
         const double* sh = reinterpret_cast<const double*>(st + L.h);
-        const double* skr = reinterpret_cast<const double*>(st + L.krw);
         const double* sx = reinterpret_cast<const double*>(st + L.xyz);
         const ushort4* sel = reinterpret_cast<const ushort4*>(st + L.eloc);
         const uint2* sup = reinterpret_cast<const uint2*>(st + L.upw);
@@ -261,8 +261,14 @@ __global__ void __launch_bounds__(kElemThreads) k_elem_chunk(ElemArgs a) {
             const size_t zo = MZ ? (size_t)a.ezone[e] * a.N : 0;
 #pragma unroll
             for (int k = 0; k < NPE; ++k) {
-                hv[k] = sh[li[k]];
-                kr[k] = MZ ? a.krw[zo + a.ch_node[j0 + li[k]]] : skr[li[k]];
+                if (MZ) {
+                    hv[k] = sh[li[k]];
+                    kr[k] = a.krw[zo + a.ch_node[j0 + li[k]]];
+                } else {
+                    const double2 hk = reinterpret_cast<const double2*>(sh)[li[k]];
+                    hv[k] = hk.x;
+                    kr[k] = hk.y;
+                }
             }
             double q[NFE];
             if (VAR == 0) {
@@ -391,7 +397,7 @@ static NodeCopies node_copies(fvm_ctx* c) {
     cp.part_ptr = c->part_ptr.p;
     cp.cpos = c->ch_cpos.p;
     cp.ch_h = c->ch_h.p;
-    cp.ch_krw = c->ch_krw.p;
+    cp.ch_hk = c->ch_hk.p;
     return cp;
 }
 
@@ -444,7 +450,7 @@ static void launch_elem(fvm_ctx* c, const double* h, const int* skip = nullptr) 
     a.ch_seg = c->ch_seg.p; a.ch_node = c->ch_node.p;
     a.elocal = c->elocal.p; a.ch_lptr = c->ch_lptr.p; a.ch_lc = c->ch_lc.p;
     a.coef = c->coef.p; a.ch_xyz = c->ch_xyz.p; a.eK = c->eK.p; a.ezone = c->ezone.p;
-    a.krw = c->krw.p; a.ch_h = c->ch_h.p; a.ch_krw = c->ch_krw.p; a.upw = c->upw.p; a.rho0 = c->rho0;
+    a.krw = c->krw.p; a.ch_h = c->ch_h.p; a.ch_hk = c->ch_hk.p; a.upw = c->upw.p; a.rho0 = c->rho0;
     a.part = c->part.p; a.err = c->elem_err.p; a.P = c->ch_node.n;
     with_elem_kernel(c, [&](auto k) { fvm_launch_pdl(c, k, c->chunk_grid, kElemThreads, c->chunk_smem, c->stream, a); });
 }
@@ -528,7 +534,7 @@ static void build_chunks(fvm_ctx* c, int CE) {
         c->ch_xyz.upload(cx, s);
     }
     c->ch_h.alloc(P);
-    c->ch_krw.alloc(P);
+    c->ch_hk.alloc(2 * P);
     c->elocal.upload(elocal, s);
     c->ch_lptr.upload(lptr, s);
     c->ch_lc.upload(lc, s);

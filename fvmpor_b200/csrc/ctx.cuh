@@ -218,7 +218,8 @@ struct fvm_ctx {
     fvmb::DevBuf<int> ch_node;            // [P] distinct nodes per chunk, ascending
     fvmb::DevBuf<int> ch_cpos;            // [P] node-major copy slot -> chunk-major position
     fvmb::DevBuf<double> ch_xyz;          // [3][P] chunk-major coordinates (3D)
-    fvmb::DevBuf<double> ch_h, ch_krw;    // [P] chunk-major head / krw (node pass output)
+    fvmb::DevBuf<double> ch_h;            // [P] chunk-major head (several zones)
+    fvmb::DevBuf<double> ch_hk;           // [P][2] chunk-major (head, krw) pairs (one zone)
     fvmb::DevBuf<ushort4> elocal;         // [T] chunk-local corner ids
     fvmb::DevBuf<unsigned short> ch_lptr; // [P + nchunk] corner-list offsets
     fvmb::DevBuf<unsigned short> ch_lc;   // [T*npe] node-ordered corner lists
