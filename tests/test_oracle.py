@@ -235,6 +235,76 @@ def test_gmres_solves_the_newton_system(p2):
     assert np.sqrt(np.mean(((F0 - Jx) * ewt) ** 2)) < 0.05
 
 
+def _colour_order(rp, col, r0, r1):
+    """the rows r0..r1-1 of a block in the factor's colour order: greedy
+    colours in natural order (smallest colour not used by an earlier coupled
+    row of the block), then stable by colour"""
+    colour = {}
+    for i in range(r0, r1):
+        used = {colour[j] for j in col[rp[i]:rp[i + 1]] if r0 <= j < i}
+        c = 0
+        while c in used:
+            c += 1
+        colour[i] = c
+    return sorted(range(r0, r1), key=lambda i: (colour[i], i)), colour
+
+
+@pytest.mark.parametrize("nblocks", [1, 4, 9])
+def test_block_ilu_colour_order_matches_a_dense_restatement(p2, nblocks):
+    # The oracle's block ILU(0) factors each block with its rows in colour
+    # order.  Restate that here with dense arrays: per block, the permuted
+    # block matrix restricted to its pattern, IKJ elimination keeping only
+    # pattern entries, then the two triangular solves.
+    o = Oracle(p2)
+    y, yp = setup_state(p2, 7)
+    F0 = o.residual(0.0, y, yp)
+    ewt = 1.0 / (1e-6 * np.abs(y) + 1e-6)
+    assert o.psetup(0.0, 1e-2, 1e2, y, yp, F0, ewt, nblocks) == 0
+    rp, col, val, _ = o.jacobian()
+    N = p2.n_nodes
+    r = np.random.default_rng(8).standard_normal(N)
+    z = np.zeros(N)
+    bstart = [(N * b) // nblocks for b in range(nblocks + 1)]
+    max_colours = 0
+    for b in range(nblocks):
+        r0, r1 = bstart[b], bstart[b + 1]
+        order, colour = _colour_order(rp, col, r0, r1)
+        max_colours = max(max_colours, max(colour.values()) + 1)
+        n = r1 - r0
+        pos = {g: k for k, g in enumerate(order)}
+        A = np.zeros((n, n))
+        mask = np.zeros((n, n), bool)
+        for g in range(r0, r1):
+            for p in range(rp[g], rp[g + 1]):
+                j = col[p]
+                if r0 <= j < r1:
+                    A[pos[g], pos[j]] = val[p]
+                    mask[pos[g], pos[j]] = True
+        # rows of one colour are uncoupled
+        for g in range(r0, r1):
+            for j in col[rp[g]:rp[g + 1]]:
+                if r0 <= j < r1 and j != g:
+                    assert colour[j] != colour[g]
+        LU = A.copy()
+        for i in range(n):
+            for k in range(i):
+                if not mask[i, k]:
+                    continue
+                LU[i, k] /= LU[k, k]
+                for j in range(k + 1, n):
+                    if mask[i, j] and mask[k, j]:
+                        LU[i, j] -= LU[i, k] * LU[k, j]
+        x = r[order].copy()
+        for i in range(n):
+            x[i] -= sum(LU[i, k] * x[k] for k in range(i) if mask[i, k])
+        for i in reversed(range(n)):
+            x[i] = (x[i] - sum(LU[i, j] * x[j] for j in range(i + 1, n) if mask[i, j])) / LU[i, i]
+        z[order] = x
+    assert max_colours <= 8    # triangles: a proper greedy colouring of the couplings
+    zo = o.psolve(r)
+    assert np.abs(zo - z).max() <= 1e-10 * np.abs(z).max()
+
+
 def test_block_ilu_given_matrix_is_deterministic(p2):
     o = Oracle(p2)
     y, yp = setup_state(p2, 5)
