@@ -30,6 +30,7 @@
 #include "tc05.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <cfloat>
 #include <cmath>
 
@@ -136,7 +137,9 @@ __global__ void k_fd_node(int N, const double* __restrict__ y, const double* __r
 
 // per element: the npe x npe changes of its corner partials, one column
 // (perturbed node m) at a time, divided by d_m, into their slots
-template <int NPE, int NFE, bool RC, bool MZ>
+// Slots are FP64, or FP32 when the factor is FP32 (the factor rounds every
+// entry to FP32 anyway; the slots then move half the bytes).
+template <int NPE, int NFE, bool RC, bool MZ, class S>
 // (two blocks per SM: 128 registers, no spills; the unbounded build took
 // 130 and ran one block of 8 warps per SM)
 __global__ void __launch_bounds__(256, 2) k_fd_elem(int T, int N, const int4* __restrict__ en,
@@ -146,7 +149,7 @@ __global__ void __launch_bounds__(256, 2) k_fd_elem(int T, int N, const int4* __
                                                  const double* __restrict__ shift, const double* __restrict__ krwb,
                                                  const double* __restrict__ krwp,
                                                  const unsigned char* __restrict__ upw, double rho0,
-                                                 const int* __restrict__ epos, double* __restrict__ slots) {
+                                                 const int* __restrict__ epos, S* __restrict__ slots) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= T) return;
     const int4 nd = en[e];
@@ -216,14 +219,15 @@ __global__ void __launch_bounds__(256, 2) k_fd_elem(int T, int N, const int4* __
         }
         const double inv = 1.0 / dl[m];
 #pragma unroll
-        for (int k = 0; k < NPE; ++k) slots[epos[(size_t)e * NPE * NPE + m * NPE + k]] = dc[k] * inv;
+        for (int k = 0; k < NPE; ++k) slots[epos[(size_t)e * NPE * NPE + m * NPE + k]] = (S)(dc[k] * inv);
     }
 }
 
 // per nonzero (i, j): J_ij = (1/V_i) sum of the slots - [i == j] dstor_i / d_i;
 // Dirichlet rows h_D - h differentiate to the quotient of that expression
+template <class S>
 __global__ void k_fd_gather(int nnz, const int* __restrict__ rowof, const int* __restrict__ col,
-                            const int* __restrict__ jptr, const double* __restrict__ slots,
+                            const int* __restrict__ jptr, const S* __restrict__ slots,
                             const double* __restrict__ invV, const double* __restrict__ dstor,
                             const unsigned char* __restrict__ ntype, const double* __restrict__ hD,
                             const double* __restrict__ y, const double* __restrict__ shift,
@@ -237,7 +241,7 @@ __global__ void k_fd_gather(int nnz, const int* __restrict__ rowof, const int* _
     } else {
         double s = 0.0;
         const int p1 = jptr[q + 1];
-        for (int p = jptr[q]; p < p1; ++p) s += slots[p];
+        for (int p = jptr[q]; p < p1; ++p) s += (double)slots[p];
         v = s * invV[i];
         if (i == j) v = v - dstor[i] / shift[i];
     }
@@ -995,20 +999,26 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     {
         const int gb = grid_for(c->T, 256);
         const bool mz = c->nz > 1;
-        auto go = [&](auto kern) {
-            fvm_launch(c, kern, gb, 256, 0, s, c->T, N, c->enodes.p, c->coef.p, c->xyz.p, c->eK.p, c->kiso ? 1 : 0,
-                       c->estride, c->ezone.p, y, P->shift.p, P->krwb.p, P->krwp.p, c->upw.p, c->rho0, P->fd_epos.p,
-                       P->fd_slots.p);
+        auto run = [&](auto* slots) {
+            using S = std::remove_pointer_t<decltype(slots)>;
+            auto go = [&](auto kern) {
+                fvm_launch(c, kern, gb, 256, 0, s, c->T, N, c->enodes.p, c->coef.p, c->xyz.p, c->eK.p,
+                           c->kiso ? 1 : 0, c->estride, c->ezone.p, y, P->shift.p, P->krwb.p, P->krwp.p, c->upw.p,
+                           c->rho0, P->fd_epos.p, slots);
+            };
+            if (c->dim == 3) {
+                if (c->recompute) mz ? go(k_fd_elem<4, 6, true, true, S>) : go(k_fd_elem<4, 6, true, false, S>);
+                else mz ? go(k_fd_elem<4, 6, false, true, S>) : go(k_fd_elem<4, 6, false, false, S>);
+            } else {
+                mz ? go(k_fd_elem<3, 3, false, true, S>) : go(k_fd_elem<3, 3, false, false, S>);
+            }
+            fvm_launch(c, k_fd_gather<S>, grid_for(P->nnz, 256), 256, 0, s, P->nnz, P->rowof.p, P->col.p,
+                       P->fd_jptr.p, slots, c->invV.p, P->dstor.p, c->ntype.p, c->hD.p, y, P->shift.p, P->J.p);
         };
-        if (c->dim == 3) {
-            if (c->recompute) mz ? go(k_fd_elem<4, 6, true, true>) : go(k_fd_elem<4, 6, true, false>);
-            else mz ? go(k_fd_elem<4, 6, false, true>) : go(k_fd_elem<4, 6, false, false>);
-        } else {
-            mz ? go(k_fd_elem<3, 3, false, true>) : go(k_fd_elem<3, 3, false, false>);
-        }
+        // the FP64 slot buffer holds the FP32 slots in its first half
+        if (precision) run(reinterpret_cast<float*>(P->fd_slots.p));
+        else run(P->fd_slots.p);
     }
-    fvm_launch(c, k_fd_gather, grid_for(P->nnz, 256), 256, 0, s, P->nnz, P->rowof.p, P->col.p, P->fd_jptr.p,
-               P->fd_slots.p, c->invV.p, P->dstor.p, c->ntype.p, c->hD.p, y, P->shift.p, P->J.p);
     c->tm.end(TM_FD_JAC, s);
     FVM_CUDA(cudaMemsetAsync(P->status.p, 0, sizeof(int), s));
     size_t nlu = P->lu_src.n;
