@@ -57,3 +57,45 @@ def test_product_never_imports_oracle():
             if f.endswith((".py", ".cu", ".cpp", ".cuh", ".hpp")):
                 src = open(os.path.join(dirpath, f)).read()
                 assert "pyoracle" not in src and "oracle.cpp" not in src and "orc_" not in src, f
+
+
+# C struct of the header <-> its ctypes mirror in the package
+STRUCTS = {
+    "fvm_mesh": "Mesh", "fvm_zone": "Zone", "fvm_bc": "BC", "fvm_physics": "PhysicsDesc",
+    "fvm_problem": "ProblemStruct", "fvm_pmesh": "PmeshStruct", "fvm_step_record": "StepRecord",
+    "fvm_opts": "Opts", "fvm_stats": "Stats", "fvm_tune_result": "TuneResult",
+}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """every ctypes mirror has the size and field offsets that the C
+    compiler gives the header's struct (a field added on one side only
+    shifts everything after it)"""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fvmpor_b200.h"', "int main(void) {"]
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(fb, pyname)
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in cls._fields_:
+            lines.append(f'printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln:
+            s, f, v = ln.split()
+            got[(s, f)] = int(v)
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(fb, pyname)
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)
