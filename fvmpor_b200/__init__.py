@@ -153,6 +153,7 @@ def _declare(L):
     L.fvm_opts_default.argtypes = [C.POINTER(Opts)]
     L.fvm_integrate.argtypes = [_P, C.POINTER(Opts), _D, _D, _P, _P, C.POINTER(Stats)]
     L.fvm_integrate_host.argtypes = [_P, C.POINTER(Opts), _D, _D, _P, _P, C.POINTER(Stats)]
+    L.fvm_integrate_outputs.argtypes = [_P, C.POINTER(Opts), _D, _P, C.c_int, _P, _P, _P, C.POINTER(Stats)]
     L.fvm_problem_richards2d.argtypes = [_I, _I, _D, _D, _D, C.c_uint64, _D, _D, C.POINTER(ProblemStruct)]
     L.fvm_problem_richards3d.argtypes = [_I, _I, _I, _D, _D, _D, _D, C.c_uint64, _D, _D, _D, _D, _D,
                                          C.POINTER(ProblemStruct)]
@@ -511,7 +512,10 @@ class Preconditioner:
 def default_opts(**kw) -> Opts:
     o = Opts()
     lib().fvm_opts_default(C.byref(o))
+    names = {f for f, _ in Opts._fields_}
     for k, v in kw.items():
+        if k not in names:
+            raise TypeError(f"unknown integrator option {k!r}")
         setattr(o, k, v)
     return o
 
@@ -540,6 +544,24 @@ class Integrator:
         L.fvm_step_trace(self.ph._c, buf, n)
         dt = np.dtype([(k, np.float64 if t is C.c_double else np.int32) for k, t in StepRecord._fields_])
         return np.frombuffer(bytes(buf), dtype=dt, count=n).copy() if n > 0 else np.zeros(0, dt)
+
+    def integrate_outputs(self, t0, t_out, y0, y_out, yp_out=None):
+        """integrate from (t0, y0) through the ascending output times t_out
+        without shortening steps to meet them (IDAIntegrator::advance); the
+        heads at t_out[i] go to y_out[i] and their time derivatives to
+        yp_out[i] (float64 CUDA tensors [len(t_out), N]; yp_out optional),
+        interpolated from the step that reached each time"""
+        tv = np.ascontiguousarray(t_out, np.float64)
+        n = tv.size
+        if y_out.shape != (n, self.ph.problem.n_nodes) or (yp_out is not None and yp_out.shape != y_out.shape):
+            raise ValueError("y_out / yp_out must have shape (len(t_out), n_nodes)")
+        st = Stats()
+        r = lib().fvm_integrate_outputs(self.ph._c, C.byref(self.opts), t0, _ptr(y0), n, tv.ctypes.data,
+                                        _ptr(y_out), _ptr(yp_out) if yp_out is not None else None,
+                                        C.byref(st))
+        if r < 0:
+            raise _err("fvm_integrate_outputs", r)
+        return r, st.as_dict()
 
     def integrate_host(self, t0, t_end, y0: np.ndarray, y_end: np.ndarray):
         st = Stats()

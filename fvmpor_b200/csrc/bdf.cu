@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 
 namespace fvmb {
 
@@ -45,6 +46,22 @@ __global__ void k_predict(int N, int k, PhiPtrs ph, Coef7 gamma, double* __restr
     y[i] = s;
     yp[i] = sp;
     e[i] = 0.0;
+}
+
+// dense output: y = sum_{j<=k} c_j phi_j ; yp = sum_{1<=j<=k} d_j phi_j
+// (yp may be null)
+__global__ void k_interp(int N, int k, PhiPtrs ph, Coef7 c, Coef7 d, double* __restrict__ y,
+                         double* __restrict__ yp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double s = ph.p[0][i], sp = 0.0;
+    for (int j = 1; j <= k; ++j) {
+        const double v = ph.p[j][i];
+        s += c.v[j] * v;
+        sp += d.v[j] * v;
+    }
+    y[i] = s;
+    if (yp) yp[i] = sp;
 }
 
 __global__ void k_phi_scale(int N, int j0, int j1, PhiPtrs ph, Coef7 f) {
@@ -378,6 +395,13 @@ struct DeviceOps {
         fetch(4);
         for (int q = 0; q < 4; ++q) out[q] = std::sqrt(host[q] / N);
     }
+    // head and time derivative at tq from the last accepted step's
+    // interpolating polynomial (coefficients from the controller)
+    void interpolate(int k, const double* cf, const double* df, double* yo, double* ypo) {
+        Coef7 cc, dd;
+        for (int j = 0; j < kNPhi; ++j) { cc.v[j] = cf[j]; dd.v[j] = df[j]; }
+        fvm_launch(c, k_interp, g(), 256, 0, c->stream, N, k, ptrs(), cc, dd, yo, ypo);
+    }
     void phi_update(int k, int set_kp2) {
         if (pred || rec) {
             // the accepted corrector y against the predictor (training
@@ -440,8 +464,20 @@ struct DeviceOps {
     }
 };
 
+// requested output times of fvm_integrate_outputs and where their heads go
+struct OutputTimes {
+    int n = 0;
+    const double* t = nullptr;
+    double* y = nullptr;
+    double* yp = nullptr;
+    int done = 0;
+};
+
+// t_end is the last output time when out is given: the steps then run
+// without a stop time and each output is interpolated from the step that
+// reached it
 int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, const double* y0,
-                  double* y_end, fvm_stats* stats, Recorder* rec = nullptr) {
+                  double* y_end, fvm_stats* stats, Recorder* rec = nullptr, OutputTimes* out = nullptr) {
     const fvm_opts& o = *opts;
     if (o.max_order < 1 || o.max_order > 5) throw Error("integrate: max_order must be 1..5");
     if (!(o.rtol > 0) || !(o.atol > 0)) throw Error("integrate: tolerances must be positive");
@@ -468,13 +504,25 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
     double h0 = ops.start(t0, y0, t_end);
     ctl.start(t0, h0);
     int rc = 0;
-    while (ctl.t < t_end) {
+    const double tstop = out ? std::numeric_limits<double>::infinity() : t_end;
+    while (out ? out->done < out->n : ctl.t < t_end) {
         if (o.max_steps > 0 && ctl.st.nst >= o.max_steps) { rc = 1; break; }
-        rc = ctl.step(t_end);
+        rc = ctl.step(tstop);
         if (rc != 0) break;
-        if (t_end - ctl.t <= 1e-12 * std::max(1.0, std::fabs(t_end))) ctl.t = t_end;
+        if (out) {
+            while (out->done < out->n && out->t[out->done] <= ctl.t) {
+                double cf[kNPhi], df[kNPhi];
+                const int k = ctl.interp_coefs(out->t[out->done], cf, df);
+                const size_t off = (size_t)out->done * c->N;
+                ops.interpolate(k, cf, df, out->y + off, out->yp ? out->yp + off : nullptr);
+                ++out->done;
+            }
+        } else if (t_end - ctl.t <= 1e-12 * std::max(1.0, std::fabs(t_end))) {
+            ctl.t = t_end;
+        }
     }
-    FVM_CUDA(cudaMemcpyAsync(y_end, ops.phi[0].p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+    if (y_end)
+        FVM_CUDA(cudaMemcpyAsync(y_end, ops.phi[0].p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
     FVM_CUDA(cudaStreamSynchronize(c->stream));
     c->last_trace.swap(ctl.trace);
     if (stats) {
@@ -520,6 +568,34 @@ extern "C" int fvm_integrate(fvm_ctx* c, const fvm_opts* opts, double t0, double
         int rc = integrate_dev(c, opts, t0, t_end, y0, y_end, stats);
         FVM_CUDA(cudaGetLastError());
         if (rc < 0) set_error("fvm_integrate: step failure code " + std::to_string(rc));
+        return rc;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+extern "C" int fvm_integrate_outputs(fvm_ctx* c, const fvm_opts* opts, double t0, const double* y0, int n_out,
+                                     const double* t_out_host, double* y_out, double* yp_out, fvm_stats* stats) {
+    try {
+        if (!c || !opts || !y0 || !t_out_host || !y_out) throw Error("fvm_integrate_outputs: null argument");
+        if (n_out < 1) throw Error("fvm_integrate_outputs: n_out must be positive");
+        for (int i = 0; i < n_out; ++i) {
+            const double prev = i ? t_out_host[i - 1] : t0;
+            if (!std::isfinite(t_out_host[i]) || !(t_out_host[i] > prev))
+                throw Error("fvm_integrate_outputs: output times must be finite, ascending and after t0");
+        }
+        OutputTimes out;
+        out.n = n_out;
+        out.t = t_out_host;
+        out.y = y_out;
+        out.yp = yp_out;
+        int rc = integrate_dev(c, opts, t0, t_out_host[n_out - 1], y0, nullptr, stats, nullptr, &out);
+        FVM_CUDA(cudaGetLastError());
+        if (rc < 0) set_error("fvm_integrate_outputs: step failure code " + std::to_string(rc));
         return rc;
     } catch (const Error& ex) {
         set_error(ex.what());

@@ -114,7 +114,34 @@ template <class Ops> struct BdfController {
         for (int i = 1; i <= k; ++i) psi[i - 1] = psi[i] - h;
     }
 
-    // one accepted step (not past tstop); 0 ok, < 0 unrecoverable
+    // Dense output from the last accepted step (IDAGetDky orders 0 and 1, as
+    // IDAIntegrator::advance(next_time) reads it, ida_integrator.h:325-340).
+    // After the step's update phi_j are the modified divided differences at
+    // t over the nodes t, t - psi_0, ..., t - psi_{k-1} (k = kold, the order
+    // the step used), so the Newton form of the interpolating polynomial is,
+    // with delt = tq - t and psi_{-1} = 0,
+    //   y(tq)  = sum_{j<=k} c_j phi_j,  c_0 = 1, c_j = c_{j-1} g_j,
+    //   y'(tq) = sum_{j<=k} d_j phi_j,  d_0 = 0, d_j = d_{j-1} g_j + c_{j-1} / psi_{j-1},
+    //   g_j = (delt + psi_{j-2}) / psi_{j-1}.
+    // At tq = t this gives c = (1, 0, ...) exactly.  c and d get kMaxOrd + 2
+    // entries (zero past k); returns k.
+    int interp_coefs(double tq, double* c, double* d) const {
+        const int kk = std::max(kold, 1);
+        const double delt = tq - t;
+        for (int j = 0; j < kMaxOrd + 2; ++j) c[j] = d[j] = 0.0;
+        c[0] = 1.0;
+        double prev = 0.0;
+        for (int j = 1; j <= kk; ++j) {
+            const double gj = (delt + prev) / psi[j - 1];
+            d[j] = d[j - 1] * gj + c[j - 1] / psi[j - 1];
+            c[j] = c[j - 1] * gj;
+            prev = psi[j - 1];
+        }
+        return kk;
+    }
+
+    // one accepted step (not past tstop, which may be +infinity); 0 ok,
+    // < 0 unrecoverable
     int step(double tstop) {
         const double uround = 2.220446049250313e-16;
         const double epcon = 0.33;
@@ -313,7 +340,8 @@ template <class Ops> struct BdfController {
                 h *= 0.25;
                 if (ncf > 10) return -5;
             }
-            if (std::fabs(h) < 4.0 * uround * std::max(std::fabs(t), std::fabs(tstop))) return -6;
+            const double tref = std::isfinite(tstop) ? std::max(std::fabs(t), std::fabs(tstop)) : std::fabs(t);
+            if (std::fabs(h) < 4.0 * uround * tref) return -6;
         }
     }
 };

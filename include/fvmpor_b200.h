@@ -329,6 +329,21 @@ int fvm_integrate(fvm_ctx* ctx, const fvm_opts* opts, double t0,
                   double t_end, const double* y0, double* y_end,
                   fvm_stats* stats);
 
+/* Integrate from (t0, y0) through the n_out output times t_out_host
+ * (ascending, all after t0) as IDAIntegrator::advance(next_time) does
+ * (ida_integrator.h:325-340): whole BDF steps with no stop time, none
+ * shortened to land on an output time, then the head and its time
+ * derivative at each output time from the interpolating polynomial of the
+ * step that reached it (IDAGetDky orders 0 and 1).  y_out and yp_out are
+ * device buffers of n_out * N doubles, output i at offset i * N; yp_out may
+ * be NULL.  The run ends with the step that passes the last output time
+ * (stats->t).  Returns 0 on success, 1 when opts->max_steps ended the run
+ * first (outputs after stats->t are then not written), < 0 on failure. */
+int fvm_integrate_outputs(fvm_ctx* ctx, const fvm_opts* opts, double t0,
+                          const double* y0, int n_out,
+                          const double* t_out_host, double* y_out,
+                          double* yp_out, fvm_stats* stats);
+
 /* ------------------------------------------------------------------ */
 /* Learned Newton initial iterate (no counterpart in the reference:     */
 /* IDAS always starts Newton from its BDF predictor).  A per-node MLP    */

@@ -44,6 +44,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <set>
 #include <stdexcept>
@@ -1139,8 +1140,13 @@ int orc_gmres(orc_ctx* c, double cj, const double* y, const double* yp, const do
     return reinterpret_cast<Oracle*>(c)->gmres(cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, rn, &njv, &nps);
 }
 
-int orc_integrate(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, double t_end,
-                  const double* y0, double* y_end, fvm_stats* stats) {
+// The time loop of fvm_integrate (t_end a stop time) and, with n_out > 0,
+// of fvm_integrate_outputs: steps with no stop time, each output time's head
+// y_out[i N ..] and derivative yp_out[i N ..] interpolated from the step that
+// reached it (IDAIntegrator::advance(next_time), ida_integrator.h:325-340).
+static int orc_run(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, double t_end,
+                   const double* y0, double* y_end, fvm_stats* stats, int n_out, const double* t_out,
+                   double* y_out, double* yp_out) {
     Oracle* o = reinterpret_cast<Oracle*>(c);
     const int N = o->N;
     CpuOps ops(*o, *opts, nblocks);
@@ -1166,14 +1172,30 @@ int orc_integrate(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, doub
     double h0 = fvmb::bdf_first_step(t0, t_end, ops.wrms(yp0), opts->h0, opts->hmax);
     for (int i = 0; i < N; ++i) { ops.phi[0][i] = y0[i]; ops.phi[1][i] = h0 * yp0[i]; ops.yp[i] = yp0[i]; }
     ctl.start(t0, h0);
-    int rc = 0;
-    while (ctl.t < t_end) {
+    int rc = 0, done = 0;
+    const double tstop = n_out > 0 ? std::numeric_limits<double>::infinity() : t_end;
+    while (n_out > 0 ? done < n_out : ctl.t < t_end) {
         if (opts->max_steps > 0 && ctl.st.nst >= opts->max_steps) { rc = 1; break; }
-        rc = ctl.step(t_end);
+        rc = ctl.step(tstop);
         if (rc != 0) break;
-        if (t_end - ctl.t <= 1e-12 * std::max(1.0, std::fabs(t_end))) ctl.t = t_end;
+        if (n_out > 0) {
+            for (; done < n_out && t_out[done] <= ctl.t; ++done) {
+                double cf[7], df[7];
+                const int k = ctl.interp_coefs(t_out[done], cf, df);
+                double* yo = y_out + (size_t)done * N;
+                double* ypo = yp_out ? yp_out + (size_t)done * N : nullptr;
+                for (int i = 0; i < N; ++i) {
+                    double s = ops.phi[0][i], sp = 0.0;
+                    for (int j = 1; j <= k; ++j) { s += cf[j] * ops.phi[j][i]; sp += df[j] * ops.phi[j][i]; }
+                    yo[i] = s;
+                    if (ypo) ypo[i] = sp;
+                }
+            }
+        } else if (t_end - ctl.t <= 1e-12 * std::max(1.0, std::fabs(t_end))) {
+            ctl.t = t_end;
+        }
     }
-    std::copy(ops.phi[0].begin(), ops.phi[0].end(), y_end);
+    if (y_end) std::copy(ops.phi[0].begin(), ops.phi[0].end(), y_end);
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
         stats->nst = ctl.st.nst; stats->nre = o->n_res - nre0; stats->nni = ctl.st.nni;
@@ -1182,6 +1204,20 @@ int orc_integrate(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, doub
         stats->last_order = ctl.st.last_order; stats->last_h = ctl.st.last_h; stats->t = ctl.t;
     }
     return rc;
+}
+
+int orc_integrate(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, double t_end,
+                  const double* y0, double* y_end, fvm_stats* stats) {
+    return orc_run(c, opts, nblocks, t0, t_end, y0, y_end, stats, 0, nullptr, nullptr, nullptr);
+}
+
+// fvm_integrate_outputs restated; the output times are ascending and after t0
+int orc_integrate_outputs(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, const double* y0,
+                          int n_out, const double* t_out, double* y_out, double* yp_out, fvm_stats* stats) {
+    if (n_out < 1) return -1;
+    for (int i = 0; i < n_out; ++i)
+        if (!std::isfinite(t_out[i]) || !(t_out[i] > (i ? t_out[i - 1] : t0))) return -1;
+    return orc_run(c, opts, nblocks, t0, t_out[n_out - 1], y0, nullptr, stats, n_out, t_out, y_out, yp_out);
 }
 
 int orc_threads(void) { return omp_get_max_threads(); }

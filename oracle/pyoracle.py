@@ -46,6 +46,7 @@ def lib():
         L.orc_psolve.argtypes = [P, P, P]
         L.orc_gmres.argtypes = [P, D, P, P, P, P, P, P, I, I, D, P, P]
         L.orc_integrate.argtypes = [P, P, I, D, D, P, P, P]
+        L.orc_integrate_outputs.argtypes = [P, P, I, D, P, I, P, P, P, P]
         L.orc_threads.restype = I
         _lib = L
     return _lib
@@ -144,6 +145,18 @@ class Oracle:
         r = lib().orc_integrate(self._c, C.addressof(opts), nblocks, t0, t_end,
                                 _p(np.ascontiguousarray(y0, np.float64)), _p(y_end), C.addressof(st))
         return r, y_end, st.as_dict()
+
+    def integrate_outputs(self, opts, nblocks, t0, y0, t_out):
+        from fvmpor_b200 import Stats
+
+        tv = np.ascontiguousarray(t_out, np.float64)
+        Y = np.zeros((tv.size, self.N))
+        YP = np.zeros((tv.size, self.N))
+        st = Stats()
+        r = lib().orc_integrate_outputs(self._c, C.addressof(opts), nblocks, t0,
+                                        _p(np.ascontiguousarray(y0, np.float64)), tv.size, _p(tv), _p(Y),
+                                        _p(YP), C.addressof(st))
+        return r, Y, YP, st.as_dict()
 
     @staticmethod
     def threads():

@@ -330,3 +330,62 @@ def test_integrate_host_buffers(cuda):
     yd = torch.empty_like(y0)
     rc2, st2 = integ.integrate(0.0, 600.0, y0, yd)
     assert np.array_equal(yd.cpu().numpy(), yend)
+
+
+def test_dense_output_matches_oracle(cuda):
+    """fvm_integrate_outputs (whole steps, heads interpolated at the output
+    times, IDAIntegrator::advance(next_time)) against the oracle's
+    restatement: same tolerance as the stop-time runs"""
+    p = fb.make_problem("richards2d", nx=21, ny=11)
+    ph = fb.Physics(p)
+    orc = Oracle(p)
+    y0 = torch.empty(p.n_nodes, dtype=torch.float64, device=cuda)
+    ph.initial_head(y0)
+    tout = [600.0, 1800.0, 3600.0]
+    integ = fb.Integrator(ph, krylov_dim=20, max_order=5)
+    Y = torch.empty(len(tout), p.n_nodes, dtype=torch.float64, device=cuda)
+    YP = torch.empty_like(Y)
+    rc, st = integ.integrate_outputs(0.0, tout, y0, Y, YP)
+    assert rc == 0 and st["t"] >= tout[-1], st
+    nb = fb.Preconditioner(ph).info()["nblocks"]
+    rc_o, Yo, YPo, st_o = orc.integrate_outputs(fb.default_opts(krylov_dim=20, max_order=5), nb, 0.0,
+                                                y0.cpu().numpy(), tout)
+    assert rc_o == 0, st_o
+    Yg, YPg = Y.cpu().numpy(), YP.cpu().numpy()
+    span = np.abs(Yo).max()
+    assert np.abs(Yg - Yo).max() < 1e-4 * span, (np.abs(Yg - Yo).max(), st, st_o)
+    assert np.abs(YPg - YPo).max() < 1e-2 * np.abs(YPo).max(), np.abs(YPg - YPo).max()
+    # a stop-time run to the last output time agrees to the same tolerance
+    yend = torch.empty_like(y0)
+    rc, _ = integ.integrate(0.0, tout[-1], y0, yend)
+    assert rc == 0
+    assert np.abs(Yg[-1] - yend.cpu().numpy()).max() < 1e-4 * span
+
+
+def test_dense_output_at_a_step_time_is_the_state(cuda):
+    p = fb.make_problem("richards2d", nx=21, ny=11)
+    ph = fb.Physics(p)
+    y0 = torch.empty(p.n_nodes, dtype=torch.float64, device=cuda)
+    ph.initial_head(y0)
+    # a fixed first step makes the step sequence independent of the end time
+    yk = torch.empty_like(y0)
+    rc, stk = fb.Integrator(ph, krylov_dim=20, h0=1.0, max_steps=12).integrate(0.0, 1e9, y0, yk)
+    assert rc == 1 and stk["nst"] == 12
+    tk, hk = stk["t"], stk["last_h"]
+    integ = fb.Integrator(ph, krylov_dim=20, h0=1.0)
+    d = 1e-4 * hk
+    tout = [tk - d, tk, 3600.0]
+    Y = torch.empty(3, p.n_nodes, dtype=torch.float64, device=cuda)
+    YP = torch.empty_like(Y)
+    rc, st = integ.integrate_outputs(0.0, tout, y0, Y, YP)
+    assert rc == 0
+    assert torch.equal(Y[1], yk)
+    fd = (Y[1] - Y[0]) / d
+    assert (fd - YP[1]).abs().max().item() <= 1e-3 * YP[1].abs().max().item() + 1e-12
+    # more output times leave the integration unchanged (yp_out optional)
+    Y2 = torch.empty(1, p.n_nodes, dtype=torch.float64, device=cuda)
+    rc, st2 = integ.integrate_outputs(0.0, [3600.0], y0, Y2)
+    assert rc == 0 and torch.equal(Y2[0], Y[2])
+    assert (st2["nst"], st2["nli"]) == (st["nst"], st["nli"])
+    with pytest.raises(RuntimeError):
+        integ.integrate_outputs(0.0, [3600.0, 3600.0], y0, torch.empty_like(Y[:2]))

@@ -371,3 +371,45 @@ def test_mlp_oracle_bf16_rounding():
     assert r[2] == 1.0078125      # above halfway rounds up
     assert r[3] == 1.015625       # halfway between 1.0078125 (odd) and 1.015625 (even)
     assert abs(r[4] + 3.140625) < 1e-6
+
+
+def test_oracle_dense_output():
+    """fvm_integrate_outputs restated: whole steps with no stop time and the
+    heads at the output times from the interpolating polynomial of the step
+    that reached them (IDAIntegrator::advance(next_time),
+    ida_integrator.h:325-340)."""
+    p = fb.make_problem("richards2d", nx=21, ny=11)
+    o = Oracle(p)
+    a = p.arrays()
+    y0 = p.water_table - a["coords"][:, 1]
+    y0[a["node_tag"] == 2] = 0.0
+    T = 3600.0
+    # a fixed first step makes the step sequence independent of the end time
+    opts = fb.default_opts(krylov_dim=20, max_order=5, h0=1.0)
+    optk = fb.default_opts(krylov_dim=20, max_order=5, h0=1.0, max_steps=12)
+    rc, yk, stk = o.integrate(optk, 1, 0.0, 1e9, y0)
+    assert rc == 1 and stk["nst"] == 12
+    tk, hk = stk["t"], stk["last_h"]
+    assert 0.0 < tk < T and hk > 0.0
+    d = 1e-4 * hk
+    rc, Y, YP, st = o.integrate_outputs(opts, 1, 0.0, y0, [tk - d, tk, T])
+    assert rc == 0, st
+    assert st["t"] >= T
+    # at an accepted step's time the interpolant is the step's state, bit for bit
+    assert np.array_equal(Y[1], yk)
+    # the derivative output is the interpolant's slope
+    fd = (Y[1] - Y[0]) / d
+    assert np.abs(fd - YP[1]).max() <= 1e-3 * np.abs(YP[1]).max() + 1e-12
+    # asking for more output times does not change the integration
+    rc, Y2, YP2, st2 = o.integrate_outputs(opts, 1, 0.0, y0, [T])
+    assert rc == 0
+    assert np.array_equal(Y2[0], Y[2]) and np.array_equal(YP2[0], YP[2])
+    assert (st2["nst"], st2["nni"], st2["nli"]) == (st["nst"], st["nni"], st["nli"])
+    # against the run that stops at T: two step sequences, each within the
+    # 1e-6 local error tolerance
+    rc, yT, stT = o.integrate(opts, 1, 0.0, T, y0)
+    assert rc == 0
+    assert np.abs(Y[2] - yT).max() < 1e-4 * np.abs(yT).max()
+    # the bad output times are rejected
+    assert o.integrate_outputs(opts, 1, 0.0, y0, [T, T])[0] < 0
+    assert o.integrate_outputs(opts, 1, 10.0, y0, [5.0])[0] < 0
