@@ -199,6 +199,47 @@ def test_cassion_oracle_matches_reference_run(cass_path, eem):
         assert mx < MAX_DIFF_M and rms < RMS_DIFF_M, (k, mx, rms)
 
 
+def test_cassion_oracle_dense_output_matches_reference_run(cass_path, eem):
+    """one continuous run through the stored output times, heads interpolated
+    at each as the reference's advance(next_time) does (no restart at the
+    output times: 739 steps against 969 with restarts)"""
+    from oracle.pyoracle import Oracle
+
+    zones, bcs, h0 = fb.cassion_physics()
+    p = fb.Problem.from_pmesh(cass_path, zones, bcs)
+    o = Oracle(p)
+    opts = fb.default_opts(krylov_dim=30, max_order=5, rtol=1e-6, atol=1e-6)
+    rc, Y, YP, st = o.integrate_outputs(opts, 1, 0.0, np.full(p.n_nodes, h0), eem["t"][1:12])
+    assert rc == 0 and st["t"] >= eem["t"][11]
+    for k in range(1, 12):
+        mx, rms = _compare(Y[k - 1], eem["head"][k])
+        assert mx < MAX_DIFF_M and rms < RMS_DIFF_M, (k, mx, rms)
+
+
+@pytest.mark.gpu
+def test_cassion_device_dense_output_matches_reference_run_and_oracle(cass_path, eem):
+    import torch
+
+    from oracle.pyoracle import Oracle
+
+    zones, bcs, h0 = fb.cassion_physics()
+    p = fb.Problem.from_pmesh(cass_path, zones, bcs)
+    ph = fb.Physics(p)
+    tout = eem["t"][1:12]
+    y0 = torch.full((p.n_nodes,), h0, dtype=torch.float64, device="cuda")
+    Y = torch.empty(len(tout), p.n_nodes, dtype=torch.float64, device="cuda")
+    rc, st = fb.Integrator(ph, krylov_dim=30, max_order=5).integrate_outputs(0.0, tout, y0, Y)
+    assert rc == 0
+    opts = fb.default_opts(krylov_dim=30, max_order=5)
+    rc, Yo, _, _ = Oracle(p).integrate_outputs(opts, 1, 0.0, np.full(p.n_nodes, h0), tout)
+    assert rc == 0
+    Yg = Y.cpu().numpy()
+    for k in range(1, 12):
+        mx, rms = _compare(Yg[k - 1], eem["head"][k])
+        assert mx < MAX_DIFF_M and rms < RMS_DIFF_M, (k, mx, rms)
+        assert np.abs(Yg[k - 1] - Yo[k - 1]).max() < 2e-3, (k, np.abs(Yg[k - 1] - Yo[k - 1]).max())
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", [0, 1])
 def test_cassion_device_matches_reference_run_and_oracle(cass_path, eem, precision):
