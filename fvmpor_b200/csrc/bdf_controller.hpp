@@ -78,6 +78,21 @@ struct BdfOptions {
     int psetup_age = 1;
 };
 
+// c_j, d_j (j <= k) of the interpolating polynomial in Newton form over the
+// nodes t, t - psi_0, ..., t - psi_{k-1}, at t + delt; n entries, zero past k
+// (the recurrences are given at BdfController::interp_coefs)
+inline void bdf_interp_coefs(const double* psi, int k, double delt, int n, double* c, double* d) {
+    for (int j = 0; j < n; ++j) c[j] = d[j] = 0.0;
+    c[0] = 1.0;
+    double prev = 0.0;
+    for (int j = 1; j <= k; ++j) {
+        const double gj = (delt + prev) / psi[j - 1];
+        d[j] = d[j - 1] * gj + c[j - 1] / psi[j - 1];
+        c[j] = c[j - 1] * gj;
+        prev = psi[j - 1];
+    }
+}
+
 template <class Ops> struct BdfController {
     static constexpr int kMaxOrd = 5;
     Ops& ops;
@@ -127,16 +142,7 @@ template <class Ops> struct BdfController {
     // entries (zero past k); returns k.
     int interp_coefs(double tq, double* c, double* d) const {
         const int kk = std::max(kold, 1);
-        const double delt = tq - t;
-        for (int j = 0; j < kMaxOrd + 2; ++j) c[j] = d[j] = 0.0;
-        c[0] = 1.0;
-        double prev = 0.0;
-        for (int j = 1; j <= kk; ++j) {
-            const double gj = (delt + prev) / psi[j - 1];
-            d[j] = d[j - 1] * gj + c[j - 1] / psi[j - 1];
-            c[j] = c[j - 1] * gj;
-            prev = psi[j - 1];
-        }
+        bdf_interp_coefs(psi, kk, tq - t, kMaxOrd + 2, c, d);
         return kk;
     }
 

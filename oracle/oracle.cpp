@@ -1211,6 +1211,13 @@ int orc_integrate(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, doub
     return orc_run(c, opts, nblocks, t0, t_end, y0, y_end, stats, 0, nullptr, nullptr, nullptr);
 }
 
+// the dense-output coefficients of the controller, for a known-answer test
+int orc_interp_coefs(const double* psi, int k, double delt, double* c, double* d) {
+    if (k < 1 || k > 6) return -1;
+    fvmb::bdf_interp_coefs(psi, k, delt, 7, c, d);
+    return 0;
+}
+
 // fvm_integrate_outputs restated; the output times are ascending and after t0
 int orc_integrate_outputs(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, const double* y0,
                           int n_out, const double* t_out, double* y_out, double* yp_out, fvm_stats* stats) {

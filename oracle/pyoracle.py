@@ -47,6 +47,7 @@ def lib():
         L.orc_gmres.argtypes = [P, D, P, P, P, P, P, P, I, I, D, P, P]
         L.orc_integrate.argtypes = [P, P, I, D, D, P, P, P]
         L.orc_integrate_outputs.argtypes = [P, P, I, D, P, I, P, P, P, P]
+        L.orc_interp_coefs.argtypes = [P, I, D, P, P]
         L.orc_threads.restype = I
         _lib = L
     return _lib

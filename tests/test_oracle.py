@@ -413,3 +413,40 @@ def test_oracle_dense_output():
     # the bad output times are rejected
     assert o.integrate_outputs(opts, 1, 0.0, y0, [T, T])[0] < 0
     assert o.integrate_outputs(opts, 1, 10.0, y0, [5.0])[0] < 0
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5])
+def test_dense_output_coefficients_reproduce_polynomials(k):
+    """c_j, d_j of the dense output against a degree-k polynomial: with
+    phi_j = psi_0 ... psi_{j-1} p[x_0, ..., x_j] over the nodes x_0 = t,
+    x_i = t - psi_{i-1}, sum c_j phi_j = p(t + delt) and sum d_j phi_j =
+    p'(t + delt)"""
+    import ctypes as C
+
+    from oracle.pyoracle import lib
+
+    rng = np.random.default_rng(k)
+    t = 7.0
+    steps = rng.uniform(0.3, 2.0, k)
+    psi = np.cumsum(steps)
+    x = np.concatenate([[t], t - psi])
+    coef = rng.standard_normal(k + 1)
+    P = np.polynomial.Polynomial(coef)
+    dd = P(x).astype(np.float64)
+    phi = np.zeros(k + 1)
+    phi[0] = dd[0]
+    for j in range(1, k + 1):   # divided differences p[x_0..x_j]
+        dd = (dd[:-1] - dd[1:]) / (x[: len(dd) - 1] - x[j:])
+        phi[j] = np.prod(psi[:j]) * dd[0]
+    for delt in (0.0, -0.25 * steps[0], -steps[0], 0.4 * steps[0]):
+        c, d = np.zeros(7), np.zeros(7)
+        ps = np.zeros(7)
+        ps[:k] = psi
+        assert lib().orc_interp_coefs(ps.ctypes.data, k, delt, c.ctypes.data, d.ctypes.data) == 0
+        assert np.all(c[k + 1:] == 0) and np.all(d[k + 1:] == 0)
+        y, yp = c[: k + 1] @ phi, d[: k + 1] @ phi
+        scale = np.abs(coef).sum() * (1 + abs(t) + psi[-1]) ** k
+        assert abs(y - P(t + delt)) < 1e-13 * scale, (delt, y, P(t + delt))
+        assert abs(yp - P.deriv()(t + delt)) < 1e-12 * scale, (delt, yp, P.deriv()(t + delt))
+        if delt == 0.0:
+            assert c[0] == 1.0 and np.all(c[1:] == 0.0)
