@@ -4,8 +4,8 @@
 // with hand-written forward and backward kernels and Adam.
 //
 // The reference has no counterpart (its Newton iterate is IDAS's BDF
-// predictor); north_star asks for one, judged by the FP64 nonlinear
-// residual: on every step the network's iterate y_pred + w * MLP(x) is kept
+// predictor).  The network's iterate is judged by the FP64 nonlinear
+// residual: on every step where it is tried, y_pred + w * MLP(x) is kept
 // only if its residual norm is below the BDF predictor's, otherwise the
 // plain BDF extrapolation is used.
 //

@@ -1,8 +1,8 @@
 """ctypes loader for the FP64 CPU oracle (oracle/oracle.cpp).
 
 TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py, as the checker (or the timed CPU baseline) —
-never by the product.
+CPU-baseline leg of bench.py, as the FP64 answer results are compared against
+(or the timed CPU baseline) — never by the product.
 """
 from __future__ import annotations
 
