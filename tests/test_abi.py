@@ -51,6 +51,22 @@ def test_create_reports_errors_without_crashing():
     assert b"null" in L.fvm_last_error()
 
 
+def test_integrate_entry_points_reject_null_arguments():
+    # argument checks come before any device work, so they run without a GPU
+    import ctypes as C
+
+    L = fb.lib()
+    o = fb.default_opts()
+    st = fb.Stats()
+    t = (C.c_double * 2)(1.0, 2.0)
+    assert L.fvm_integrate(None, C.byref(o), 0.0, 1.0, None, None, C.byref(st)) < 0
+    assert b"null" in L.fvm_last_error()
+    assert L.fvm_integrate_outputs(None, C.byref(o), 0.0, None, 2, t, None, None, C.byref(st)) < 0
+    assert b"null" in L.fvm_last_error()
+    assert L.fvm_integrate_host(None, C.byref(o), 0.0, 1.0, None, None, C.byref(st)) < 0
+    assert b"null" in L.fvm_last_error()
+
+
 def test_product_never_imports_oracle():
     for dirpath, _, files in os.walk(os.path.join(ROOT, "fvmpor_b200")):
         for f in files:
