@@ -33,6 +33,7 @@ struct Krylov {
     DevBuf<int> err;          // 3 = a grid barrier timed out
     int coop_grid = 0;        // blocks of the cooperative launch, 0 = three-pass path
     size_t coop_smem = 0;     // dynamic shared memory of the fused kernel
+    int coop_threads = 0;     // its block size: one thread per row quad of a block, 128..512
     DevBuf<ArnState> st;      // device-driven Arnoldi state
     DevBuf<double> ls;        // H [(m+1) x m], cs [m], sn [m], g [m+1]
     double* host = nullptr;   // pinned
