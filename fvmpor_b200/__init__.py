@@ -160,6 +160,8 @@ def _declare(L):
     L.fvm_problem_free.argtypes = [C.POINTER(ProblemStruct)]
     L.fvm_problem_ensemble2d.argtypes = [_I, _I, _I, C.c_uint64, C.POINTER(ProblemStruct), _P]
     L.fvm_set_members.argtypes = [_P, _I, _P]
+    L.fvm_integrate_replay.argtypes = [_P, C.POINTER(Opts), _D, _P, _D, C.c_long, C.POINTER(StepRecord), _D,
+                                       C.c_int, _P, C.POINTER(Stats)]
     L.fvm_step_trace.restype = C.c_long
     L.fvm_step_trace.argtypes = [_P, C.POINTER(StepRecord), C.c_long]
     L.fvm_pmesh_read.argtypes = [C.c_char_p, _I, C.POINTER(PmeshStruct)]
@@ -544,6 +546,23 @@ class Integrator:
         L.fvm_step_trace(self.ph._c, buf, n)
         dt = np.dtype([(k, np.float64 if t is C.c_double else np.int32) for k, t in StepRecord._fields_])
         return np.frombuffer(bytes(buf), dtype=dt, count=n).copy() if n > 0 else np.zeros(0, dt)
+
+    def replay(self, t0, y0, h0, steps, y_end, newton_tol=1e-5, max_newton=10):
+        """replay the accepted steps ``steps`` (a trace record array, or any
+        array with fields h and order) from (t0, y0) with every corrector
+        solved to ||delta||_wrms <= newton_tol (fvm_integrate_replay);
+        returns (rc, stats), rc 1 when some corrector stopped at max_newton"""
+        n = len(steps)
+        buf = (StepRecord * n)()
+        for i in range(n):
+            buf[i].h = float(steps["h"][i])
+            buf[i].order = int(steps["order"][i])
+        st = Stats()
+        r = lib().fvm_integrate_replay(self.ph._c, C.byref(self.opts), t0, _ptr(y0), h0, n, buf, newton_tol,
+                                       max_newton, _ptr(y_end), C.byref(st))
+        if r < 0:
+            raise _err("fvm_integrate_replay", r)
+        return r, st.as_dict()
 
     def integrate_outputs(self, t0, t_out, y0, y_out, yp_out=None):
         """integrate from (t0, y0) through the ascending output times t_out

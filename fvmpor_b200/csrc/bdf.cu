@@ -544,6 +544,62 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
     return rc;
 }
 
+// Replay of a given sequence of accepted steps with tight correctors
+// (fvm_integrate_replay): the controller's own coefficients and predictor,
+// the step sizes and orders forced, no error test
+int replay_dev(fvm_ctx* c, const fvm_opts* opts, double t0, const double* y0, double h0, long n,
+               const fvm_step_record* steps, double newton_tol, int max_newton, double* y_end, fvm_stats* stats) {
+    fvm_opts o = *opts;
+    if (o.max_order < 1 || o.max_order > 5) throw Error("replay: max_order must be 1..5");
+    if (!(o.rtol > 0) || !(o.atol > 0)) throw Error("replay: tolerances must be positive");
+    if (!(h0 > 0) || !std::isfinite(h0)) throw Error("replay: h0 must be positive");
+    if (!(newton_tol > 0) || max_newton < 1) throw Error("replay: newton_tol must be positive, max_newton >= 1");
+    for (long i = 0; i < n; ++i) {
+        const int kk = steps[i].order;
+        // the order rises by at most one per step, so history exists for it
+        if (!(steps[i].h > 0) || !std::isfinite(steps[i].h) || kk < 1 || kk > o.max_order ||
+            kk > (i ? steps[i - 1].order + 1 : 1))
+            throw Error("replay: step " + std::to_string(i) + " has a bad size or order");
+    }
+    o.h0 = h0;      // the first-step rule returns the given h0
+    o.hmax = 0.0;
+    o.use_predictor = 0;
+    c->last_trace.clear();
+    DeviceOps ops(c, o);
+    ops.enable_learning(nullptr, nullptr);
+    BdfOptions bo;
+    bo.rtol = o.rtol;
+    bo.atol = o.atol;
+    bo.max_order = o.max_order;
+    BdfController<DeviceOps> ctl(ops, bo);
+    const long nre0 = c->n_residuals;
+    const double hs = ops.start(t0, y0, t0 + h0);
+    ctl.start(t0, hs);
+    int rc = 0;
+    for (long i = 0; i < n; ++i) {
+        const int r = bdf_replay_step(ctl, steps[i].h, steps[i].order, newton_tol, max_newton);
+        if (r < 0) { rc = r; break; }
+        if (r == 1) rc = 1;
+    }
+    if (y_end)
+        FVM_CUDA(cudaMemcpyAsync(y_end, ops.phi[0].p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    c->last_trace.swap(ctl.trace);
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->nst = ctl.st.nst;
+        stats->nre = c->n_residuals - nre0;
+        stats->nni = ctl.st.nni;
+        stats->nli = ctl.st.nli;
+        stats->npe = ctl.st.npe;
+        stats->nps = ctl.st.nps;
+        stats->last_order = ctl.st.last_order;
+        stats->last_h = ctl.st.last_h;
+        stats->t = ctl.t;
+    }
+    return rc;
+}
+
 } // namespace fvmb
 
 using namespace fvmb;
@@ -645,6 +701,25 @@ extern "C" int fvm_integrate_host(fvm_ctx* c, const fvm_opts* opts, double t0, d
         FVM_CUDA(cudaMemcpyAsync(y_end_host, b.p, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
         FVM_CUDA(cudaStreamSynchronize(c->stream));
         if (rc < 0) set_error("fvm_integrate_host: step failure code " + std::to_string(rc));
+        return rc;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+extern "C" int fvm_integrate_replay(fvm_ctx* c, const fvm_opts* opts, double t0, const double* y0, double h0,
+                                    long n_steps, const fvm_step_record* steps, double newton_tol, int max_newton,
+                                    double* y_end, fvm_stats* stats) {
+    try {
+        if (!c || !opts || !y0 || !steps || !y_end) throw Error("fvm_integrate_replay: null argument");
+        if (n_steps < 1) throw Error("fvm_integrate_replay: n_steps must be positive");
+        int rc = replay_dev(c, opts, t0, y0, h0, n_steps, steps, newton_tol, max_newton, y_end, stats);
+        FVM_CUDA(cudaGetLastError());
+        if (rc < 0) set_error("fvm_integrate_replay: step failure code " + std::to_string(rc));
         return rc;
     } catch (const Error& ex) {
         set_error(ex.what());

@@ -146,6 +146,26 @@ template <class Ops> struct BdfController {
         return kk;
     }
 
+    // psi, alpha, beta, sigma, gamma of the step about to be tried with
+    // (h, k); recomputed unless the last k + 1 steps had this h and k
+    void update_coefs() {
+        if (h != hold || k != kold) ns = 0;
+        ns = std::min(ns + 1, kold + 2);
+        if (k + 1 < ns) return;
+        beta[0] = 1.0; alpha[0] = 1.0; gamma[0] = 0.0; sigma[0] = 1.0;
+        double temp1 = h;
+        for (int i = 1; i <= k; ++i) {
+            double temp2 = psi[i - 1];
+            psi[i - 1] = temp1;
+            beta[i] = beta[i - 1] * psi[i - 1] / temp2;
+            temp1 = temp2 + h;
+            alpha[i] = h / temp1;
+            sigma[i] = i * sigma[i - 1] * alpha[i];
+            gamma[i] = gamma[i - 1] + alpha[i - 1] / h;
+        }
+        psi[k] = temp1;
+    }
+
     // one accepted step (not past tstop, which may be +infinity); 0 ok,
     // < 0 unrecoverable
     int step(double tstop) {
@@ -158,22 +178,7 @@ template <class Ops> struct BdfController {
         ops.ewt_from_phi0(o.rtol, o.atol);
         ops.begin_step();
         for (;;) {
-            if (h != hold || k != kold) ns = 0;
-            ns = std::min(ns + 1, kold + 2);
-            if (k + 1 >= ns) {
-                beta[0] = 1.0; alpha[0] = 1.0; gamma[0] = 0.0; sigma[0] = 1.0;
-                double temp1 = h;
-                for (int i = 1; i <= k; ++i) {
-                    double temp2 = psi[i - 1];
-                    psi[i - 1] = temp1;
-                    beta[i] = beta[i - 1] * psi[i - 1] / temp2;
-                    temp1 = temp2 + h;
-                    alpha[i] = h / temp1;
-                    sigma[i] = i * sigma[i - 1] * alpha[i];
-                    gamma[i] = gamma[i - 1] + alpha[i - 1] / h;
-                }
-                psi[k] = temp1;
-            }
+            update_coefs();
             double alphas = 0.0, alpha0 = 0.0;
             for (int i = 1; i <= k; ++i) { alphas -= 1.0 / i; alpha0 -= alpha[i - 1]; }
             cj = -alphas / h;
@@ -351,6 +356,64 @@ template <class Ops> struct BdfController {
         }
     }
 };
+
+// One step of a replayed sequence: the step size and order are given (from a
+// trace of accepted steps), the coefficients and predictor are the
+// controller's own, and the corrector is solved to ||delta||_wrms <=
+// newton_tol with GMRES at 0.05 newton_tol, one preconditioner set-up at
+// the predictor.  No error test and no step-size or order choice.  Returns
+// 0 when Newton reached newton_tol within max_newton updates, 1 when not
+// (the step is still taken), < 0 on failure.
+template <class Ops> int bdf_replay_step(BdfController<Ops>& c, double hh, int kk, double newton_tol,
+                                         int max_newton) {
+    Ops& ops = c.ops;
+    c.h = hh;
+    c.k = kk;
+    ops.ewt_from_phi0(c.o.rtol, c.o.atol);
+    ops.begin_step();
+    c.update_coefs();
+    const int k = c.k;
+    const double h = c.h;
+    double alphas = 0.0;
+    for (int i = 1; i <= k; ++i) alphas -= 1.0 / i;
+    c.cj = -alphas / h;
+    if (k >= c.ns) ops.phi_scale(c.ns, k, c.beta);
+    const double tnew = c.t + h;
+    ops.predict(k, c.gamma, h);
+    ops.set_time(tnew);
+    const long nni0 = c.st.nni, nli0 = c.st.nli;
+    bool conv = false;
+    for (int m = 0; m < max_newton; ++m) {
+        ops.residual();
+        if (m == 0) {
+            if (ops.psetup(c.cj, h)) return -3;
+            c.st.npe++;
+        }
+        int its = 0;
+        double rn = 0.0;
+        long nps = 0, njv = 0;
+        int lr = ops.gmres(c.cj, 0.05 * newton_tol, &its, &rn, &nps, &njv);
+        c.st.nli += its; c.st.nps += nps; c.st.njv += njv; c.st.nni++;
+        if (lr == 2) return -7;
+        const double d = ops.newton_update(c.cj);
+        if (!std::isfinite(d)) return -7;
+        if (d <= newton_tol) { conv = true; break; }
+    }
+    c.kold = k;
+    c.hold = h;
+    c.t = tnew;
+    c.cj_last = c.cj;
+    c.st.nst++;
+    fvm_step_record rec = {};
+    rec.t = c.t; rec.h = h; rec.order = k; rec.attempts = 1;
+    rec.nni = (int)(c.st.nni - nni0); rec.nli = (int)(c.st.nli - nli0); rec.npe = 1;
+    rec.wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - c.wall0).count();
+    c.trace.push_back(rec);
+    ops.phi_update(k, k + 1 < c.kMaxOrd + 2 ? 1 : 0);
+    c.st.last_order = k;
+    c.st.last_h = h;
+    return conv ? 0 : 1;
+}
 
 // DASSL's first step: 1e-3 of the interval, limited by 0.5 / ||y'0||_wrms
 inline double bdf_first_step(double t0, double tout, double ypnorm, double h0, double hmax) {

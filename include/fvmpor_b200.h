@@ -344,6 +344,25 @@ int fvm_integrate_outputs(fvm_ctx* ctx, const fvm_opts* opts, double t0,
                           const double* t_out_host, double* y_out,
                           double* yp_out, fvm_stats* stats);
 
+/* Replays a given sequence of accepted steps: step i has size steps[i].h
+ * and order steps[i].order (the other fields are ignored), from (t0, y0),
+ * with the history started as the adaptive integrator starts it (phi_1 =
+ * h0 y'0, y'0 from the initial residual).  No error test and no step-size or
+ * order choice: each corrector is solved until ||delta||_wrms <= newton_tol
+ * (error weights from opts->rtol, opts->atol), at most max_newton updates,
+ * with GMRES(opts->krylov_dim) at 0.05 newton_tol in opts->precision.  Run
+ * on the trace of an adaptive integration (fvm_step_trace), it removes the
+ * step-size decisions from a comparison of two implementations, so that
+ * their states agree to the corrector tolerance rather than to rtol.  The
+ * orders may rise by at most one per step.  y0, y_end are device pointers.
+ * Returns 0, 1 when some corrector stopped at max_newton (the run still
+ * completes), < 0 on failure.  No counterpart in the reference: IDAS has no
+ * replay mode (the step loop it replaces is ida_integrator.h:296-321). */
+int fvm_integrate_replay(fvm_ctx* ctx, const fvm_opts* opts, double t0,
+                         const double* y0, double h0, long n_steps,
+                         const fvm_step_record* steps, double newton_tol,
+                         int max_newton, double* y_end, fvm_stats* stats);
+
 /* ------------------------------------------------------------------ */
 /* Learned Newton initial iterate (no counterpart in the reference:     */
 /* IDAS always starts Newton from its BDF predictor).  A per-node MLP    */

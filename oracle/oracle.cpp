@@ -31,9 +31,12 @@
 //   ILU(0)     decomp/ILU.c:12-115, :133-223
 //   GMRES      decomp/gmres.c:26-201, :412-511 (modified Gram-Schmidt), left
 //              preconditioned and ewt-scaled as IDAS SPGMR runs it
-// The BDF controller is the shared template of the product
-// (fvmpor_b200/csrc/bdf_controller.hpp), so oracle and GPU integrations
-// differ only in the kernels.
+// The adaptive time loop (orc_integrate) instantiates the product's BDF
+// controller template (fvmpor_b200/csrc/bdf_controller.hpp), so oracle and GPU
+// adaptive runs differ only in the kernels.  The step-sequence replay
+// (orc_replay) does NOT use it: it restates the fixed-leading-coefficient BDF
+// step independently, as Lagrange interpolation through the stored solution
+// values, so a replay comparison also checks the controller's formulas.
 #include "../include/fvmpor_b200.h"
 #include "../fvmpor_b200/csrc/bdf_controller.hpp"
 
@@ -146,6 +149,16 @@ struct Oracle {
     // work
     std::vector<double> h, hp, gx, gy, gz, phi_vec, dSw_vec, ahh, krw_f, qdotn, Mflux;
     long n_res = 0;
+    // time split of the integrations and replays (seconds): Newton residuals
+    // (with the begin-step evaluation), J*v, finite-difference Jacobian, ILU
+    // factor, preconditioner apply, Krylov orthogonalisation and least
+    // squares, whole run; and their work counters: Newton residuals, J*v
+    // products, set-ups, applies, Krylov iterations, Newton iterations,
+    // steps (the reference prints the same split, examples/fvmporMinlin/
+    // fvmpor_ODE.cpp:233-245)
+    double tm[7] = {};
+    long cnt[7] = {};
+    std::vector<fvm_step_record> last_trace;
     // preconditioner
     bool pat_built = false;
     std::vector<int> jrow, jcol, colour;
@@ -168,6 +181,18 @@ struct Oracle {
     void psetup(double t, double cj, double hh, const double* y, const double* yp, const double* F0,
                 const double* ewt, int nb);
     int ilu_factor();
+    // psetup + ilu_factor with the time split booked
+    int timed_psetup(double t, double cj, double hh, const double* y, const double* yp, const double* F0,
+                     const double* ewt, int nb) {
+        const double a = omp_get_wtime();
+        psetup(t, cj, hh, y, yp, F0, ewt, nb);
+        const double b = omp_get_wtime();
+        const int r = ilu_factor();
+        tm[2] += b - a;
+        tm[3] += omp_get_wtime() - b;
+        cnt[2]++;
+        return r;
+    }
     void psolve(const double* r, double* z) const;
     int gmres(double cj, const double* y, const double* yp, const double* F0, const double* ewt,
               const double* b, double* x, int m, int max_restarts, double tol, int* iters,
@@ -844,12 +869,30 @@ int Oracle::gmres(double cj, const double* y, const double* yp, const double* F0
         for (int i = 0; i < N; ++i) { double q = v[i] * ewt[i]; s += q * q; }
         return std::sqrt(s / N);
     };
+    const double g0 = omp_get_wtime();
+    double t_jv = 0.0, t_ps = 0.0;
     auto jtimes = [&](const std::vector<double>& v, std::vector<double>& out) {
+        const double a = omp_get_wtime();
         double nv = wrms_of(v);
         double sigma = nv > 0 ? 1.0 / nv : 1.0;
         jv(0.0, cj, y, yp, F0, v.data(), sigma, out.data());
         (*njv)++;
+        t_jv += omp_get_wtime() - a;
     };
+    auto precond = [&](const double* r, double* z) {
+        const double a = omp_get_wtime();
+        psolve(r, z);
+        t_ps += omp_get_wtime() - a;
+    };
+    struct Book {   // books the time split when the solve returns
+        Oracle* o; const double& g0; double& t_jv; double& t_ps; long* njv; long* nps; long njv0, nps0; int* its;
+        ~Book() {
+            const double all = omp_get_wtime() - g0;
+            o->tm[1] += t_jv; o->tm[4] += t_ps; o->tm[5] += all - t_jv - t_ps;
+            o->cnt[1] += *njv - njv0; o->cnt[3] += *nps - nps0; o->cnt[4] += *its;
+        }
+    } book{this, g0, t_jv, t_ps, njv, nps, *njv, *nps, iters};
+    *iters = 0;
     int total = 0;
     double rnorm = 0.0;
     bool have_x = false;
@@ -857,7 +900,7 @@ int Oracle::gmres(double cj, const double* y, const double* yp, const double* F0
     for (int cycle = 0; cycle <= max_restarts; ++cycle) {
         if (have_x) jtimes(xv, Jz);
         for (int i = 0; i < N; ++i) t[i] = have_x ? b[i] - Jz[i] : b[i];
-        psolve(t.data(), z.data());
+        precond(t.data(), z.data());
         (*nps)++;
         double beta = 0.0;
         for (int i = 0; i < N; ++i) {
@@ -876,7 +919,7 @@ int Oracle::gmres(double cj, const double* y, const double* yp, const double* F0
         for (; j < m; ++j) {
             for (int i = 0; i < N; ++i) t[i] = V[j][i] / ewt[i];
             jtimes(t, Jz);
-            psolve(Jz.data(), z.data());
+            precond(Jz.data(), z.data());
             (*nps)++;
             for (int i = 0; i < N; ++i) w[i] = ewt[i] * z[i];
             std::vector<double> hcol(j + 2);
@@ -953,7 +996,12 @@ struct CpuOps {
     void ewt_from_phi0(double rtol, double atol) {
         for (int i = 0; i < N; ++i) ewt[i] = 1.0 / (rtol * std::fabs(phi[0][i]) + atol);
     }
-    void begin_step() { o.begin_step(tcur, phi[0].data(), yp.data()); }
+    void begin_step() {
+        const double a = omp_get_wtime();
+        o.begin_step(tcur, phi[0].data(), yp.data());
+        o.tm[0] += omp_get_wtime() - a;
+        o.cnt[0]++;
+    }
     void phi_scale(int j0, int j1, const double* f) {
         for (int j = j0; j <= j1; ++j)
             for (int i = 0; i < N; ++i) phi[j][i] *= f[j];
@@ -966,11 +1014,13 @@ struct CpuOps {
         }
     }
     double wrms_y() { return wrms(y); }
-    void residual() { o.residual(tcur, y.data(), yp.data(), F.data()); }
-    int psetup(double cj, double h) {
-        o.psetup(tcur, cj, h, y.data(), yp.data(), F.data(), ewt.data(), nblocks);
-        return o.ilu_factor();
+    void residual() {
+        const double a = omp_get_wtime();
+        o.residual(tcur, y.data(), yp.data(), F.data());
+        o.tm[0] += omp_get_wtime() - a;
+        o.cnt[0]++;
     }
+    int psetup(double cj, double h) { return o.timed_psetup(tcur, cj, h, y.data(), yp.data(), F.data(), ewt.data(), nblocks); }
     int gmres(double cj, double tol, int* its, double* rn, long* nps, long* njv) {
         return o.gmres(cj, y.data(), yp.data(), F.data(), ewt.data(), F.data(), x.data(), opt.krylov_dim,
                        opt.max_restarts, tol, its, rn, njv, nps);
@@ -1149,6 +1199,7 @@ static int orc_run(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, dou
                    double* y_out, double* yp_out) {
     Oracle* o = reinterpret_cast<Oracle*>(c);
     const int N = o->N;
+    const double wall0 = omp_get_wtime();
     CpuOps ops(*o, *opts, nblocks);
     fvmb::BdfOptions bo;
     bo.rtol = opts->rtol;
@@ -1196,6 +1247,10 @@ static int orc_run(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, dou
         }
     }
     if (y_end) std::copy(ops.phi[0].begin(), ops.phi[0].end(), y_end);
+    o->last_trace.swap(ctl.trace);
+    o->cnt[5] += ctl.st.nni;
+    o->cnt[6] += ctl.st.nst;
+    o->tm[6] += omp_get_wtime() - wall0;
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
         stats->nst = ctl.st.nst; stats->nre = o->n_res - nre0; stats->nni = ctl.st.nni;
@@ -1228,5 +1283,210 @@ int orc_integrate_outputs(orc_ctx* c, const fvm_opts* opts, int nblocks, double 
 }
 
 int orc_threads(void) { return omp_get_max_threads(); }
+
+// The same replay driven by the product's controller template
+// (fvmb::bdf_replay_step: modified divided differences) with the oracle's
+// kernels.  Against orc_replay this compares the controller's predictor and
+// corrector formulas with the independent Lagrange-form restatement, on
+// identical kernels.
+int orc_replay_controller(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, const double* y0, double h0,
+                          long n, const fvm_step_record* steps, double newton_tol, int max_newton, double* y_end,
+                          fvm_stats* stats) {
+    Oracle* o = reinterpret_cast<Oracle*>(c);
+    if (!opts || !y0 || !steps || n < 1 || !(h0 > 0) || !(newton_tol > 0) || max_newton < 1) return -1;
+    const int N = o->N;
+    CpuOps ops(*o, *opts, nblocks);
+    fvmb::BdfOptions bo;
+    bo.rtol = opts->rtol;
+    bo.atol = opts->atol;
+    bo.max_order = opts->max_order;
+    fvmb::BdfController<CpuOps> ctl(ops, bo);
+    std::fill(o->w_front.begin(), o->w_front.end(), 0.5);
+    std::fill(o->w_back.begin(), o->w_back.end(), 0.5);
+    std::vector<double> zero(N, 0.0), F(N), yp0(N, 0.0);
+    o->residual(t0, y0, zero.data(), F.data());
+    for (int i = 0; i < N; ++i)
+        if (!o->is_dirichlet[i] && o->ahh[i] != 0.0) yp0[i] = F[i] / o->ahh[i];
+    for (int i = 0; i < N; ++i) { ops.phi[0][i] = y0[i]; ops.phi[1][i] = h0 * yp0[i]; ops.yp[i] = yp0[i]; }
+    ctl.start(t0, h0);
+    int rc = 0;
+    for (long s = 0; s < n; ++s) {
+        const int r = fvmb::bdf_replay_step(ctl, steps[s].h, steps[s].order, newton_tol, max_newton);
+        if (r < 0) return r;
+        if (r == 1) rc = 1;
+    }
+    if (y_end) std::copy(ops.phi[0].begin(), ops.phi[0].end(), y_end);
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->nst = ctl.st.nst; stats->nni = ctl.st.nni; stats->nli = ctl.st.nli; stats->npe = ctl.st.npe;
+        stats->nps = ctl.st.nps; stats->t = ctl.t;
+    }
+    return rc;
+}
+
+// initial head: the Dirichlet value on Dirichlet rows, water_table minus the
+// elevation elsewhere (set_initial_conditions, examples/fvmporMinlin/vs.h:8-32)
+int orc_initial_head(orc_ctx* c, double water_table, double* y) {
+    Oracle* o = reinterpret_cast<Oracle*>(c);
+    for (int i = 0; i < o->N; ++i) y[i] = water_table - (o->dim == 2 ? o->X[i].y : o->X[i].z);
+    for (size_t d = 0; d < o->dirichlet_nodes.size(); ++d) y[o->dirichlet_nodes[d]] = o->h_dirichlet[d];
+    return 0;
+}
+
+// copies up to cap records of the last adaptive integration; returns the count
+long orc_step_trace(orc_ctx* c, fvm_step_record* out, long cap) {
+    Oracle* o = reinterpret_cast<Oracle*>(c);
+    const long n = (long)o->last_trace.size();
+    if (out && cap > 0) std::copy(o->last_trace.begin(), o->last_trace.begin() + std::min(n, cap), out);
+    return n;
+}
+
+// time split and work counters since creation or the last reset (reset != 0
+// zeroes them after reading); either pointer may be NULL
+int orc_timers(orc_ctx* c, double* tm, long* cnt, int reset) {
+    Oracle* o = reinterpret_cast<Oracle*>(c);
+    if (tm) std::copy(o->tm, o->tm + 7, tm);
+    if (cnt) std::copy(o->cnt, o->cnt + 7, cnt);
+    if (reset) {
+        std::fill(o->tm, o->tm + 7, 0.0);
+        std::fill(o->cnt, o->cnt + 7, 0L);
+    }
+    return 0;
+}
+
+// Replay of a given sequence of accepted BDF steps (step sizes and orders),
+// with each corrector solved to a tight tolerance.
+//
+// This is an independent restatement of the fixed-leading-coefficient BDF
+// step of DASSL / IDA (Brenan, Campbell & Petzold 1996, ch. 5; Hindmarsh et
+// al., ACM TOMS 31(3), 2005) that the reference's IDAIntegrator drives
+// (include/fvm/integrators/ida_integrator.h:296-321).  It does not use the
+// modified divided differences of the adaptive controller: the predictor of
+// a step of order k is the polynomial through the k + 1 newest solution
+// values, evaluated in Lagrange form,
+//   y_pred = sum_i l_i(t) Y_i,   y'_pred = sum_i l_i'(t) Y_i,
+// and the corrector solves G(y) = F(t, y, y'_pred + cj (y - y_pred)) = 0 with
+// cj = (1 + 1/2 + ... + 1/k) / h.  Before the first step the history holds
+// y0 and the point (t0 - h0, y0 - h0 y'0), the line through y0 with slope
+// y'0 that the divided-difference form starts from (phi_1 = h0 y'0).
+// y'0 = F(t0, y0, 0) / ahh on free rows (fvmpor_ODE_impl.cpp:34-58).  The
+// upwind directions are frozen at the start of every step from the newest
+// solution (fvmpor_ODE_impl.cpp:118-141).  Newton: one preconditioner set-up
+// at the predictor, then updates until ||delta||_wrms <= newton_tol (error
+// weights 1/(rtol |y_n| + atol)), GMRES solved to 0.05 newton_tol.  Returns 0
+// on success, 1 if some step's Newton iteration did not reach newton_tol
+// within max_newton updates (the state is still advanced), < 0 on bad input.
+int orc_replay(orc_ctx* c, const fvm_opts* opts, int nblocks, double t0, const double* y0, double h0, long n,
+               const fvm_step_record* steps, double newton_tol, int max_newton, double* y_end, fvm_stats* stats) {
+    Oracle* o = reinterpret_cast<Oracle*>(c);
+    if (!opts || !y0 || !steps || n < 1 || !(h0 > 0) || !(newton_tol > 0) || max_newton < 1) return -1;
+    const int N = o->N;
+    const double wall0 = omp_get_wtime();
+    std::fill(o->w_front.begin(), o->w_front.end(), 0.5);
+    std::fill(o->w_back.begin(), o->w_back.end(), 0.5);
+    std::vector<double> zero(N, 0.0), F(N), yp(N, 0.0), y(N), x(N), ewt(N);
+    o->residual(t0, y0, zero.data(), F.data());
+    for (int i = 0; i < N; ++i)
+        if (!o->is_dirichlet[i] && o->ahh[i] != 0.0) yp[i] = F[i] / o->ahh[i];
+    // history, newest first: (time, solution)
+    std::vector<double> Th;
+    std::vector<std::vector<double>> Yh;
+    Th.push_back(t0);
+    Yh.emplace_back(y0, y0 + N);
+    Th.push_back(t0 - h0);
+    Yh.emplace_back(N);
+    for (int i = 0; i < N; ++i) Yh[1][i] = y0[i] - h0 * yp[i];
+    double t = t0;
+    long nni = 0, nli = 0, npe = 0, nps = 0, nre0 = o->n_res;
+    int rc = 0;
+    for (long s = 0; s < n; ++s) {
+        const double h = steps[s].h;
+        const int k = steps[s].order;
+        if (!(h > 0) || k < 1 || k > 5 || (size_t)k + 1 > Th.size()) return -2;
+        const double tn = t + h;
+        // Lagrange weights over the k + 1 newest nodes and their derivatives
+        double l[6], dl[6];
+        for (int i = 0; i <= k; ++i) {
+            double prod = 1.0, dsum = 0.0;
+            for (int j = 0; j <= k; ++j) {
+                if (j == i) continue;
+                prod *= (tn - Th[j]) / (Th[i] - Th[j]);
+            }
+            for (int m = 0; m <= k; ++m) {
+                if (m == i) continue;
+                double term = 1.0 / (Th[i] - Th[m]);
+                for (int j = 0; j <= k; ++j)
+                    if (j != i && j != m) term *= (tn - Th[j]) / (Th[i] - Th[j]);
+                dsum += term;
+            }
+            l[i] = prod;
+            dl[i] = dsum;
+        }
+        const std::vector<double>& yn = Yh[0];
+        for (int i = 0; i < N; ++i) ewt[i] = 1.0 / (opts->rtol * std::fabs(yn[i]) + opts->atol);
+        {
+            const double a = omp_get_wtime();
+            o->begin_step(t, yn.data(), yp.data());
+            o->tm[0] += omp_get_wtime() - a;
+            o->cnt[0]++;
+        }
+        double alphas = 0.0;
+        for (int j = 1; j <= k; ++j) alphas += 1.0 / j;
+        const double cj = alphas / h;
+        std::vector<double> ypred(N), yppred(N);
+        for (int i = 0; i < N; ++i) {
+            double s0 = 0.0, s1 = 0.0;
+            for (int q = 0; q <= k; ++q) { s0 += l[q] * Yh[q][i]; s1 += dl[q] * Yh[q][i]; }
+            ypred[i] = s0;
+            yppred[i] = s1;
+        }
+        y = ypred;
+        yp = yppred;
+        bool conv = false;
+        for (int m = 0; m < max_newton; ++m) {
+            {
+                const double a = omp_get_wtime();
+                o->residual(tn, y.data(), yp.data(), F.data());
+                o->tm[0] += omp_get_wtime() - a;
+                o->cnt[0]++;
+            }
+            if (m == 0) {
+                if (o->timed_psetup(tn, cj, h, y.data(), yp.data(), F.data(), ewt.data(), nblocks)) return -3;
+                npe++;
+            }
+            int its = 0;
+            double rn = 0.0;
+            long njv = 0, np = 0;
+            o->gmres(cj, y.data(), yp.data(), F.data(), ewt.data(), F.data(), x.data(), opts->krylov_dim,
+                     opts->max_restarts, 0.05 * newton_tol, &its, &rn, &njv, &np);
+            nli += its;
+            nps += np;
+            nni++;
+            double d2 = 0.0;
+            for (int i = 0; i < N; ++i) {
+                y[i] -= x[i];
+                yp[i] -= cj * x[i];
+                const double q = x[i] * ewt[i];
+                d2 += q * q;
+            }
+            if (std::sqrt(d2 / N) <= newton_tol) { conv = true; break; }
+        }
+        if (!conv) rc = 1;
+        Th.insert(Th.begin(), tn);
+        Yh.insert(Yh.begin(), y);
+        if (Th.size() > 7) { Th.pop_back(); Yh.pop_back(); }
+        t = tn;
+    }
+    if (y_end) std::copy(Yh[0].begin(), Yh[0].end(), y_end);
+    o->cnt[5] += nni;
+    o->cnt[6] += n;
+    o->tm[6] += omp_get_wtime() - wall0;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->nst = n; stats->nre = o->n_res - nre0; stats->nni = nni; stats->nli = nli; stats->npe = npe;
+        stats->nps = nps; stats->last_order = steps[n - 1].order; stats->last_h = steps[n - 1].h; stats->t = t;
+    }
+    return rc;
+}
 
 }  // extern "C"
