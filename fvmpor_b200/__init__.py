@@ -109,7 +109,7 @@ class Opts(C.Structure):
                 ("krylov_dim", C.c_int), ("max_restarts", C.c_int), ("precision", C.c_int),
                 ("use_predictor", C.c_int), ("h0", C.c_double), ("hmax", C.c_double),
                 ("max_steps", C.c_long), ("eps_lin", C.c_double), ("cj_refresh", C.c_double),
-                ("psetup_age", C.c_int)]
+                ("psetup_age", C.c_int), ("krylov_operator", C.c_int)]
 
 
 class Stats(C.Structure):

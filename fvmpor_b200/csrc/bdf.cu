@@ -367,7 +367,7 @@ struct DeviceOps {
     int gmres(double cj, double tol, int* its, double* rn, long* nps, long* njv) {
         GmresCounters gc;
         int r = gmres_dev(c, cj, y.p, yp.p, F.p, ewt.p, F.p, x.p, o.krylov_dim, o.max_restarts,
-                          o.precision, tol, its, rn, &gc);
+                          o.precision, tol, its, rn, &gc, o.krylov_operator);
         *nps = gc.nps;
         *njv = gc.njv;
         return r;

@@ -52,14 +52,19 @@ void fvmb_destroy_krylov_impl(Krylov* K);
 double reduce_sumsq(fvm_ctx* c, const double* x, const double* w);
 double reduce_dot(fvm_ctx* c, const double* x, const double* y);
 
+// op 0: J v by the residual's difference quotient; 1: by the assembled
+// Jacobian of the last set-up (jacobian_apply)
 int gmres_dev(fvm_ctx* c, double cj, const double* y, const double* yp, const double* F0,
               const double* ewt, const double* b, double* x, int m, int max_restarts,
-              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt);
+              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt, int op = 0);
 
 // preconditioner (precond.cu)
 void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* yp,
                 const double* F0, const double* ewt, int precision);
 void psolve_dev(fvm_ctx* c, const double* r, double* z, const int* skip = nullptr);
+// y = J(cj) x with the assembled difference-quotient Jacobian of the last
+// set-up (the Krylov operator of fvm_opts.krylov_operator = 1)
+void jacobian_apply(fvm_ctx* c, double cj, const double* x, double* y, const int* skip = nullptr);
 bool ilu_ready(fvm_ctx* c);
 int ilu_status(fvm_ctx* c);   // 0 ok, 1 zero pivot in the last factorisation
 

@@ -630,7 +630,7 @@ template <class B>
 static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const double* yp,
                       const double* F0, const double* ewt, const double* b, double* x, int m,
                       int max_restarts, double tol, int* iters, double* res_norm,
-                      GmresCounters* cnt) {
+                      GmresCounters* cnt, int op) {
     cudaStream_t s = c->stream;
     const int N = c->N;
     B* U = reinterpret_cast<B*>(K->U);
@@ -644,7 +644,8 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
     for (int cycle = 0; cycle <= max_restarts; ++cycle) {
         // preconditioned residual of the current iterate: z = P^-1 (b - J x)
         if (have_x) {
-            jv_dev(c, K, cj, y, yp, F0, x, ewt, K->Jv.p);
+            if (op) jacobian_apply(c, cj, x, K->Jv.p);
+            else jv_dev(c, K, cj, y, yp, F0, x, ewt, K->Jv.p);
             if (cnt) cnt->njv++;
             fvm_launch(c, k_sub, grid_for(N, 256), 256, 0, s, N, b, K->Jv.p, K->t.p);
             psolve_dev(c, K->t.p, K->z.p);
@@ -699,7 +700,8 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                     pt.v = K->t.p;
                     pt.sigma_dev = K->sigma.p;
                     pt.skip = skip;
-                    launch_residual(c, y, yp, pt, F0, K->Jv.p);
+                    if (op) jacobian_apply(c, cj, K->t.p, K->Jv.p, skip);
+                    else launch_residual(c, y, yp, pt, F0, K->Jv.p);
                     psolve_dev(c, K->Jv.p, K->z.p, skip);
                     c->tm.begin(TM_CGS, s);
                     int Ni = N;
@@ -752,7 +754,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
             }
             j = hst->j;
             total += j;
-            c->n_residuals -= queued - j;   // evaluations queued after the stop were skipped
+            if (!op) c->n_residuals -= queued - j;   // evaluations queued after the stop were skipped
             if (cnt) { cnt->njv += j; cnt->nps += j; }
             if (hst->done == 3) { *iters = total; *res_norm = rnorm; return 2; }
             rnorm = hst->rnorm;
@@ -767,7 +769,8 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         for (; K->coop_grid == 0 && j < m; ++j) {
             // w = D P^-1 J D^-1 V_j (left preconditioning, scaled by D = ewt)
             fvm_launch(c, k_unscale<B>, grid_for(N, 256), 256, 0, s, N, U + ld * j, K->scale.p, j, ewt, K->t.p);
-            jv_dev(c, K, cj, y, yp, F0, K->t.p, ewt, K->Jv.p);
+            if (op) jacobian_apply(c, cj, K->t.p, K->Jv.p);
+            else jv_dev(c, K, cj, y, yp, F0, K->t.p, ewt, K->Jv.p);
             if (cnt) cnt->njv++;
             psolve_dev(c, K->Jv.p, K->z.p);
             if (cnt) cnt->nps++;
@@ -843,12 +846,12 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
 
 int gmres_dev(fvm_ctx* c, double cj, const double* y, const double* yp, const double* F0,
               const double* ewt, const double* b, double* x, int m, int max_restarts,
-              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt) {
+              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt, int op) {
     if (m < 1 || m > 60) throw Error("gmres: krylov dimension must be in [1, 60]");
     Krylov* K = krylov_get(c, m, precision);
     if (precision)
-        return gmres_impl<float>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt);
-    return gmres_impl<double>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt);
+        return gmres_impl<float>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op);
+    return gmres_impl<double>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op);
 }
 
 } // namespace fvmb

@@ -20,8 +20,9 @@ constexpr int kNoAllocThreads = 256;
 constexpr int kNoAllocChunk = 2048;    // elements per block (8 per thread)
 constexpr long kNoAllocMaxN = (long)kNoAllocBlocks * kNoAllocChunk;   // 8,388,608
 
-// [0, kNoAllocBlocks): per-block partial sums; [kNoAllocBlocks]: counter.
-// Every GPU that loads the library holds this 32 KiB until exit.
+// [0, kNoAllocBlocks): per-block partial sums; [kNoAllocBlocks]: counter;
+// [kNoAllocBlocks + 8]: the finished sum.  4,128 doubles (33,024 bytes),
+// which every GPU that loads the library holds until exit.
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocBlocks + 32];
 
 // per-block sums of (x w)^2 into scratch[block]; the last block to finish
@@ -45,7 +46,9 @@ __global__ void k_wrms_noalloc_finish(long n, const double* scratch, double* __r
     *result = sqrt(scratch[kNoAllocBlocks + 8] / (double)n);
 }
 
-// per-device address of the static scratch, looked up once per device
+// per-device address of the static scratch, looked up once per device and
+// kept for the life of the process (a cudaDeviceReset may reload the module
+// elsewhere; the header tells callers not to call again after one)
 static std::mutex g_noalloc_mutex;
 static double* g_noalloc_ptr[64] = {};
 

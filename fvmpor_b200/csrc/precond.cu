@@ -48,6 +48,12 @@ struct BlockILU {
     DevBuf<int> fd_jptr;      // [nnz+1] slots of each nonzero
     DevBuf<double> fd_slots;  // [T*npe*npe]
     DevBuf<double> krwb, krwp, dstor;
+    // assembled-operator Krylov products (fvm_opts.krylov_operator = 1):
+    // device row pointers of J, the storage coefficient ahh(h + d) behind
+    // the cj term of J's diagonal, and the cj of the current set-up
+    DevBuf<int> rowptr;
+    DevBuf<double> ahhp;
+    double cj_setup = 0.0;
     int nb = 0, maxb = 0;
     DevBuf<int> bstart, lu_ptr, lu_src, lu_diag;
     DevBuf<int> lu_row;       // global row of each factor position (colour order inside the blocks)
@@ -112,7 +118,7 @@ __global__ void k_fd_node(int N, const double* __restrict__ y, const double* __r
                           const double* __restrict__ shift, const ZoneDev* __restrict__ zones, int nz,
                           const int* __restrict__ nz_ptr, const int* __restrict__ nz_zone,
                           const double* __restrict__ nz_w, double rho0, double* __restrict__ krwb,
-                          double* __restrict__ krwp, double* __restrict__ dstor) {
+                          double* __restrict__ krwp, double* __restrict__ dstor, double* __restrict__ ahhp_out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const double h = y[i], d = shift[i];
@@ -133,6 +139,29 @@ __global__ void k_fd_node(int N, const double* __restrict__ y, const double* __r
     }
     const double ahh = (phi * dsw) * rho0, ahhp = (phi * dswp) * rho0;
     dstor[i] = (yp[i] + cj * d) * ahhp - yp[i] * ahh;
+    ahhp_out[i] = ahhp;
+}
+
+// y = J x for the assembled difference-quotient Jacobian of the last
+// set-up, shifted to another cj: the cj term of J enters only the diagonal
+// of free rows, as -cj ahh(h + d) (the quotient of the storage term
+// y' ahh(h), k_fd_node), so J(cj) = J(cj_setup) - (cj - cj_setup) ahh(h + d)
+// on those rows.  Four lanes per row, rows in node order.
+__global__ void k_jac_apply(int N, const int* __restrict__ rowptr, const int* __restrict__ col,
+                            const double* __restrict__ J, const double* __restrict__ ahhp,
+                            const unsigned char* __restrict__ ntype, double dcj, const double* __restrict__ x,
+                            double* __restrict__ y, const int* __restrict__ skip) {
+    pdl_wait_and_trigger();
+    if (skip && *skip) return;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = g >> 2, lane = g & 3;
+    if (i >= N) return;
+    const int p0 = rowptr[i], p1 = rowptr[i + 1];
+    double acc = 0.0;
+    for (int p = p0 + lane; p < p1; p += 4) acc += J[p] * x[col[p]];
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    if (lane == 0) y[i] = ntype[i] ? acc : acc - dcj * ahhp[i] * x[i];
 }
 
 // per element: the npe x npe changes of its corner partials, one column
@@ -957,6 +986,8 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
     P->krwb.alloc((size_t)c->nz * N);
     P->krwp.alloc((size_t)c->nz * N);
     P->dstor.alloc(N);
+    P->ahhp.alloc(N);
+    P->rowptr.upload(P->h_rowptr, s);
     P->bstart.upload(bstart, s);
     P->lu_ptr.upload(lu_ptr, s);
     // 8 padding entries so every block's widened copy window stays inside
@@ -995,7 +1026,8 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     (void)F0;   // the element-wise quotients difference each element's own partials
     fvm_launch(c, k_shift, grid_for(N, 256), 256, 0, s, N, y, yp, ewt, h, std::sqrt(DBL_EPSILON), P->shift.p);
     fvm_launch(c, k_fd_node, grid_for(N, 256), 256, 0, s, N, y, yp, cj, P->shift.p, c->zones.p, c->nz, c->nz_ptr.p,
-               c->nz_zone.p, c->nz_w.p, c->rho0, P->krwb.p, P->krwp.p, P->dstor.p);
+               c->nz_zone.p, c->nz_w.p, c->rho0, P->krwb.p, P->krwp.p, P->dstor.p, P->ahhp.p);
+    P->cj_setup = cj;
     {
         const int gb = grid_for(c->T, 256);
         const bool mz = c->nz > 1;
@@ -1052,6 +1084,13 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     c->tm.end(TM_ILU_FACTOR, s);
     FVM_CUDA(cudaMemcpyAsync(P->h_status, P->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     P->factored = precision;
+}
+
+void jacobian_apply(fvm_ctx* c, double cj, const double* x, double* y, const int* skip) {
+    BlockILU* P = c->ilu;
+    if (!P || P->factored < 0) throw Error("jacobian_apply: preconditioner not set up");
+    fvm_launch_pdl(c, k_jac_apply, grid_for(4L * c->N, 256), 256, 0, c->stream, c->N, P->rowptr.p, P->col.p,
+                   P->J.p, P->ahhp.p, c->ntype.p, cj - P->cj_setup, x, y, skip);
 }
 
 int ilu_status(fvm_ctx* c) {

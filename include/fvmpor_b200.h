@@ -208,12 +208,16 @@ int fvm_profile_read(fvm_ctx* ctx, double* ms, long* counts);
  * call cudaMalloc (a host integrator that owns all device memory through its
  * own pool and calls the norm inside its step loop, where an allocation
  * would stall the device or is forbidden).  No counterpart in the
- * reference.  The reduction scratch is a static 32 KiB __device__ array
- * that every GPU loading the library keeps until exit, which bounds n to
- * fvm_wrms_noalloc_max_n() = 8,388,608; larger n is rejected (status < 0,
- * message in fvm_last_error()).  The first call on a device looks the
- * array's address up with cudaGetSymbolAddress, so make that first call
- * before any stream capture.  x, ewt (may be NULL = 1) and result are
+ * reference.  The reduction scratch is a static __device__ array of 4,128
+ * doubles (33,024 bytes: partial sums for 4,096 blocks plus a 256-byte
+ * counter and result tail) that every GPU loading the library keeps until
+ * exit, which bounds n to fvm_wrms_noalloc_max_n() = 8,388,608; larger n is
+ * rejected (status < 0, message in fvm_last_error()).  The first call on a
+ * device looks the array's address up with cudaGetSymbolAddress and keeps
+ * it for the life of the process, so make that first call before any
+ * stream capture, and do not call this entry point again after a
+ * cudaDeviceReset of that device (the module, and with it the array, may
+ * then be loaded at another address).  x, ewt (may be NULL = 1) and result are
  * device pointers; the work is queued on `stream` (a cudaStream_t, NULL for
  * the legacy default stream) and *result is valid once that stream reaches
  * it.  All calls share the one scratch array: calls that overlap on the GPU
@@ -281,6 +285,13 @@ typedef struct {
                                 (0 = 1.05)                               */
     int psetup_age;          /* ... or after this many steps (0 = 1:
                                 every step)                              */
+    int krylov_operator;     /* 0: J v as the difference quotient of the
+                                residual (Jacobian-free, IDAS SPGMR's
+                                product); 1: J v as the product with the
+                                preconditioner set-up's assembled
+                                difference-quotient Jacobian, shifted
+                                exactly to the current cj (the residual,
+                                Newton update and tests stay FP64)        */
 } fvm_opts;
 
 typedef struct {

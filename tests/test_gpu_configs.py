@@ -125,7 +125,6 @@ def plane(cuda):
 def test_plane_one_day_adaptive_and_replay(plane, cuda):
     p, ph, orc, y0 = plane
     day = 86400.0
-    nb = fb.Preconditioner(ph).info()["nblocks"]
     ends, traces = {}, {}
     for prec in (0, 1):
         integ = fb.Integrator(ph, krylov_dim=30, max_order=5, precision=prec)
@@ -133,6 +132,7 @@ def test_plane_one_day_adaptive_and_replay(plane, cuda):
         rc, st = integ.integrate(0.0, day, y0, ye)
         assert rc == 0 and abs(st["t"] - day) < 1e-6, st
         ends[prec], traces[prec] = ye.cpu().numpy(), integ.trace()
+    nb = fb.Preconditioner(ph).info()["nblocks"]   # the partition the runs used
     y0h = y0.cpu().numpy()
     rc, yo, st_o = orc.integrate(fb.default_opts(krylov_dim=30, max_order=5), nb, 0.0, day, y0h)
     assert rc == 0, st_o
