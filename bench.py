@@ -5,14 +5,18 @@ Newton tolerance from rtol = atol = 1e-6) on B200.
 
 One step = one complete 30-day integration from the hydrostatic initial
 state (variable-order BDF, Newton-GMRES(40), block-ILU(0)).  The headline
-``value`` is the learned + mixed-precision path (the per-node MLP proposes
-the Newton initial iterate, kept only when its FP64 residual beats the BDF
-predictor's; FP32 block-ILU(0) factor/apply and FP32 Krylov basis; FP64
-residual, Newton update, least squares and stopping test) with the state
-resident in HBM.  The MLP is trained before the timed region on a plain
-FP64 trajectory of a different Ks realisation.  The plain FP64 path and the
-FP32 path without the learned iterate are timed the same way and reported
-beside it.  ``e2e`` is the same metric through
+``value`` is the learned + mixed-precision path: the per-node MLP proposes
+the Newton initial iterate (kept only when its FP64 residual beats the BDF
+predictor's); the block-ILU(0) factor and apply, the Krylov basis and the
+Krylov operator -- the preconditioner set-up's assembled difference-quotient
+Jacobian, applied in one fused persistent launch per GMRES cycle -- run in
+FP32; the residual, Newton update, least squares and stopping tests stay
+FP64.  The state is resident in HBM.  The MLP is trained before the timed
+region on a plain FP64 trajectory of a different Ks realisation.  The plain
+FP64 path (the reference's Jacobian-free method: J v as the difference
+quotient of the FP64 residual), the FP32 Jacobian-free path and the FP32
+assembled path without the learned iterate are timed the same way and
+reported beside it.  ``e2e`` is the same metric through
 fvm_integrate_host (host buffers, H2D of y0 and D2H of the final head inside
 the timed region).
 
@@ -360,9 +364,13 @@ def main():
     yend = torch.empty_like(y0)
     P, train_info = train_predictor(fb, torch, dev, 1001 + rank, horizon)
     fb.Predictor(ph).set_params(P)
-    learned = fb.Integrator(ph, krylov_dim=40, max_restarts=5, precision=1, max_order=5, use_predictor=1)
-    mixed = fb.Integrator(ph, krylov_dim=40, max_restarts=5, precision=1, max_order=5)
-    plain = fb.Integrator(ph, krylov_dim=40, max_restarts=5, precision=0, max_order=5)
+    common = dict(krylov_dim=40, max_restarts=5, max_order=5)
+    # headline: learned iterate + FP32 factor, basis and assembled Krylov
+    # operator (one fused launch per GMRES cycle)
+    learned = fb.Integrator(ph, precision=1, krylov_operator=1, use_predictor=1, **common)
+    assembled = fb.Integrator(ph, precision=1, krylov_operator=1, **common)
+    fp32_dq = fb.Integrator(ph, precision=1, **common)
+    plain = fb.Integrator(ph, precision=0, **common)
 
     def timed(integ, k, host=False, profile=False):
         y0h = y0.cpu().numpy()
@@ -399,40 +407,65 @@ def main():
     with ClockSampler(local) as clk:
         ms_learn, st_learn, cnt = timed(learned, args.steps)
     y_learn = yend.clone()
+    trace_learn = learned.trace()
     # per-kernel CUDA-event profile on one more run outside the timed region
     # (the events themselves slow the run down)
     _, _, prof = timed(learned, 1, profile=True)
+    st_prof = learned.trace()   # the trace belongs to the context: read it before the next run
     # the comparison paths are timed run by run, alternating, and reported as
     # the median run (each run is a whole 30-day integration; alternating
     # keeps a slow spell of the shared host from landing on one path only)
     k_extra = max(2, args.steps // 2)
-    mixed.integrate(0.0, horizon, y0, yend)   # warm the FP32 and FP64 factor/basis buffers
-    plain.integrate(0.0, horizon, y0, yend)
-    runs_mixed, runs_plain = [], []
+    others = {"fp32_assembled_without_learned": assembled, "fp32_jacobian_free": fp32_dq, "plain_fp64": plain}
+    for integ in others.values():
+        integ.integrate(0.0, horizon, y0, yend)   # warm the FP32 and FP64 factor/basis buffers
+    runs = {k: [] for k in others}
+    st_o = {}
     with ClockSampler(local) as clk_cmp:
         for _ in range(k_extra):
-            ms, st_mixed, _ = timed(mixed, 1)
-            runs_mixed.append(ms)
-            ms, st_plain, _ = timed(plain, 1)
-            runs_plain.append(ms)
-    y_plain = yend.clone()
-    ms_mixed = float(np.median(runs_mixed)) * k_extra
-    ms_plain = float(np.median(runs_plain)) * k_extra
+            for name, integ in others.items():
+                ms, st_o[name], _ = timed(integ, 1)
+                runs[name].append(ms)
+    y_plain = yend.clone()   # plain FP64 ran last
     ms_e2e, _, _ = timed(learned, k_extra, host=True)
     value = job_throughput(horizon * args.steps, ws, ms_learn / 1e3)
-    mixed_value = job_throughput(horizon * k_extra, ws, ms_mixed / 1e3)
-    plain_value = job_throughput(horizon * k_extra, ws, ms_plain / 1e3)
     e2e_value = job_throughput(horizon * k_extra, ws, ms_e2e / 1e3)
     head_diff = float((y_learn - y_plain).abs().max() / y_plain.abs().max())
+    cmp = {}
+    for name in others:
+        med = float(np.median(runs[name]))
+        cmp[name] = {"value": job_throughput(horizon, ws, med / 1e3), "ms_per_step": med, "runs": k_extra,
+                     "ms_each_run": runs[name],
+                     "stats": {k: st_o[name][0][k] for k in ("nst", "nni", "nli", "npe", "nre")}}
+    plain_value = cmp["plain_fp64"]["value"]
+    cmp["plain_fp64"]["ratio_headline_over_plain"] = value / plain_value
+    cmp["fp32_assembled_without_learned"]["clocks_comparison_runs"] = clk_cmp.summary()
 
-    # roofline of the residual evaluation (node pass + element pass + gather):
-    # algorithmic bytes 36 B/node + 270 B/tet per evaluation
-    alg_bytes = 36.0 * N + 270.0 * T
-    n_eval = prof["element"][1]
-    chain_ms = (prof["node"][0] + prof["element"][0] + prof["gather"][0]) / max(n_eval, 1)
-    achieved = alg_bytes / (chain_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
-    launches_per_run = None
+    # roofline of the dominant kernel, the fused Arnoldi cycle: algorithmic
+    # bytes of Arnoldi step j (nv = j + 1 basis vectors) are the assembled
+    # operator (FP32 value + 4-byte column per non-zero), per node the
+    # direction and the cj coefficient (4 B each), ewt (8 B), four passes
+    # over the FP32 basis (16 nv B) and the new basis vector and direction
+    # (8 B); the factor stays in shared memory for the whole cycle.  Per
+    # launch = per cycle; the time is the kernel's CUDA-event total over its
+    # launches of the profiled run.
+    nnz = fb.Preconditioner(ph).info()["nnz"]
+    nv_sum, n_ar = 0.0, 0
+    for nli_s, nni_s in zip(st_prof["nli"], st_prof["nni"]):
+        per = nli_s / max(int(nni_s), 1)   # Krylov iterations of each Newton solve of the step
+        nv_sum += max(int(nni_s), 1) * per * (per + 1) / 2.0
+        n_ar += int(nli_s)
+    bytes_steps = n_ar * (8.0 * nnz + 24.0 * N) + 16.0 * N * nv_sum
+    launches_k = max(int(prof["gram_schmidt"][1]), 1)
+    fused_ms = prof["gram_schmidt"][0]
+    achieved = bytes_steps / launches_k / (fused_ms / launches_k * 1e-3) / 1e9
+    # residual evaluation chain (node pass + element pass + gather):
+    # algorithmic bytes 36 B/node + 270 B/tet per evaluation
+    alg_res = 36.0 * N + 270.0 * T
+    n_eval = max(prof["element"][1], 1)
+    chain_ms = (prof["node"][0] + prof["element"][0] + prof["gather"][0]) / n_eval
+    achieved_res = alg_res / (chain_ms * 1e-3) / 1e9
     st0 = st_learn[0]
     clocks = clk.summary()
     line = {
@@ -442,25 +475,28 @@ def main():
         "data": "synthetic (seeded 3D jittered Kuhn mesh, lognormal Ks by FFT)",
         "config": {"workload": f"richards3d {N} nodes / {T} tets, {args.days:g}-day run per step",
                    "path": "learned Newton iterate (per-node MLP, BF16 weights / FP32 accumulation on tcgen05) + "
-                           "FP32 block-ILU(0) + FP32 GMRES(40) basis, FP64 residual/Newton/LSQ",
+                           "FP32 block-ILU(0), FP32 GMRES(40) basis and FP32 assembled Krylov operator (the "
+                           "set-up's difference-quotient Jacobian, one fused launch per GMRES cycle); FP64 "
+                           "residual, Newton update, least squares and tests",
                    "rtol": 1e-6, "atol": 1e-6, "l2": "inputs larger than L2 (331 MB per residual)",
                    "parallelism": f"replicas x{ws}"},
-        "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain / k_extra, "runs": k_extra,
-                       "ms_each_run": runs_plain,
-                       "ratio_learned_fp32_over_plain": value / plain_value,
-                       "stats": {k: st_plain[0][k] for k in ("nst", "nni", "nli", "npe", "nre")}},
-        "fp32_without_learned": {"value": mixed_value, "ms_per_step": ms_mixed / k_extra, "runs": k_extra,
-                                 "ms_each_run": runs_mixed, "clocks_fp32_and_fp64_runs": clk_cmp.summary(),
-                                 "stats": {k: st_mixed[0][k] for k in ("nst", "nni", "nli", "npe", "nre")}},
+        "comparison_paths": cmp,
         "learned_predictor": dict(train_info, accepted_steps=st0["npred"]),
         "final_head_rel_diff_vs_plain_fp64": head_diff,
         "stats": {k: st0[k] for k in ("nst", "nni", "nli", "npe", "nps", "nre", "ncfn", "netf", "npred",
                                       "last_order")},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": CHAIN_DRAM_BYTES,
-                     "kernel": "residual evaluation (node pass + element pass + node gather)",
-                     "algorithmic_bytes_per_launch": alg_bytes, "avg_ms": chain_ms,
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "k_arnoldi_fused (one GMRES cycle: assembled operator, block-ILU(0) sweeps, CGS2, "
+                               "Givens)",
+                     "algorithmic_bytes_per_launch": bytes_steps / launches_k,
+                     "avg_ms": fused_ms / launches_k, "arnoldi_steps_per_launch": n_ar / launches_k,
                      "peak_kind": peak_kind},
+        "roofline_residual": {"bound": "hbm", "achieved": achieved_res, "peak": peak, "unit": "GB/s",
+                              "frac": achieved_res / peak, "traffic": CHAIN_DRAM_BYTES,
+                              "kernel": "residual evaluation (node pass + element pass + node gather)",
+                              "algorithmic_bytes_per_launch": alg_res, "avg_ms": chain_ms,
+                              "peak_kind": peak_kind},
         "kernel_ms": {k: {"total_ms": v[0], "launches": v[1], "avg_us": 1e3 * v[0] / max(v[1], 1)}
                       for k, v in prof.items()},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N},
@@ -477,8 +513,9 @@ def main():
         # error of the final heads against the FP64 CPU oracle: the first
         # steps of the headline run replayed with tight correctors
         line["error_vs_oracle"] = error_vs_oracle(
-            fb, torch, ph, y0, learned.trace(), args.replay_steps,
-            {"plain_fp64": dict(precision=0), "mixed_fp32": dict(precision=1)})
+            fb, torch, ph, y0, trace_learn, args.replay_steps,
+            {"plain_fp64": dict(precision=0), "fp32_jacobian_free": dict(precision=1),
+             "fp32_assembled": dict(precision=1, krylov_operator=1)})
         v, total, unit, wall, threads = cpu_baseline_sample()
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": "FP64 oracle unit costs on the 214,221-node mesh (2 bounded samples, "

@@ -1,0 +1,532 @@
+// One GMRES cycle in one persistent cooperative launch, for the assembled
+// Krylov operator (fvm_opts.krylov_operator = 1) with the FP32 block-ILU(0)
+// factor and FP32 basis.
+//
+// The Arnoldi step of decomp/gmres.c:412-511 (left-preconditioned and scaled
+// by D = diag(ewt), as IDAS SPGMR runs it, ida_integrator.h:248-254) is
+//   w = D P^-1 J D^-1 V_j,  CGS2 against V_0..V_j,  Givens update
+// (linalg_dense.c:128-173).  With J assembled (the preconditioner set-up's
+// difference-quotient Jacobian, shifted exactly to the current cj), every
+// part of a step is local to the rows of one ILU block except the operator's
+// reads of the direction at neighbouring nodes and the orthogonalisation's
+// dot products.  So one CTA owns one ILU block for the whole cycle:
+//   - its factor window and metadata are brought into shared memory ONCE per
+//     cycle by bulk copies (the staged apply reloads them on every apply);
+//   - per step it gathers the direction at its own and its halo nodes into
+//     shared memory, forms its rows of J t from there (rows in factor order,
+//     one warp per 32 rows, entry-major slices with 16-bit local columns)
+//     straight into the shared-memory vector the triangular sweeps work on,
+//     runs both sweeps there, scales by ewt, and
+//     orthogonalises its rows (CGS2 in three passes over the basis, row quads,
+//     fixed-order reductions through per-block partials);
+//   - every block computes the Hessenberg column, the rotations and the
+//     stopping test from the same reduced numbers, so all take the same
+//     decision without another barrier; block 0 writes them out for the
+//     host's back substitution.
+// Two bounded grid barriers per step (after each dot pass).  The next
+// direction is published block by block: a block raises its flag once its
+// rows are written, and a block starting the next step waits (bounded) only
+// for the flags of the blocks its operator rows reach, plus its two
+// neighbours in node order.  Nothing returns to the host until the cycle
+// ends.  Replaces, for this operator, the five launches per step of the
+// difference-quotient path (node pass, element pass, gather, apply, CGS2).
+#include "cgs.cuh"
+#include "ilu.cuh"
+#include "krylov.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace fvmb {
+
+struct FusedArgs {
+    int N, m, nr_max, nh_max;
+    size_t stage_max;          // shared bytes of the largest block's staged factor
+    ArnState* st;
+    float* U;
+    size_t ld;
+    double* scale;
+    float* tdir;               // D^-1 V_j, FP32, node order (read at neighbours)
+    const double* ewt;
+    const int* slptr;          // [slices + 1] first entry of each slice
+    const int* blksl;          // [nb + 1] first slice of each block
+    const unsigned short* op_lcol;   // entry -> index in the block's node list
+    const unsigned short* op_self;   // [N], factor order: the row's own index there
+    const int* halo_ptr;       // [nb + 1] the block's node list: its rows and halo
+    const int* halo_node;
+    const int* nbr_ptr;        // [nb + 1] blocks whose flags a block waits for
+    const int* nbr;
+    unsigned* flags;           // [nb] last step whose direction rows a block wrote
+    const float* op_val;
+    const float* op_dg;        // [N], factor order: ahh(h + d) on free rows, else 0
+    float dcj;                 // cj - cj of the set-up
+    const int* bstart;
+    const int* lu_ptr;
+    const unsigned short* lu_col;
+    const unsigned short* meta;
+    const int* meta_off;
+    const int* blk_lvl;
+    const int* blk_ulvl;
+    const float* lu;
+    const int* lu_row;
+    const double* beta2;       // ||D P^-1 r||^2 of the cycle's start
+    double* partial;
+    unsigned* bar;
+    int* err;
+    double* H;
+    double* cs;
+    double* sn;
+    double* g;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// barrier among `count` threads (whole warps) of the block on barrier `id`
+__device__ __forceinline__ void named_barrier(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// at most 384 threads (one per row quad of a 1,536-row block; larger blocks
+// loop), so a thread may hold up to 170 registers
+constexpr int kFusedThreads = 384;
+
+template <int KM>
+__global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a) {
+    __shared__ double ca[64], cb[64], coef[64], sc[64], rc[64], rs[64], gs[64];
+    __shared__ int s_done;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int b = blockIdx.x, nblk = gridDim.x;
+    const int r0 = a.bstart[b], r1 = a.bstart[b + 1], nr = r1 - r0;
+    const IluWindow w = ilu_window(a.lu_ptr[r0], a.lu_ptr[r1]);
+    const int la = a.blk_lvl[b], nl = a.blk_lvl[b + 1] - la;
+    const int ua = a.blk_ulvl[b], nu = a.blk_ulvl[b + 1] - ua;
+    // staged factor (the layout of k_ilu_apply_smem), then the inverse of
+    // the block's row order and its rows of W
+    float* x = reinterpret_cast<float*>(smem_raw);
+    float* val = reinterpret_cast<float*>(smem_raw + round16(sizeof(float) * nr));
+    unsigned short* col = reinterpret_cast<unsigned short*>(val + w.wn);
+    unsigned short* rp = col + w.wn;
+    unsigned short* dg = rp + nr + 1;
+    unsigned short* lrow = dg + nr;
+    unsigned short* urow = lrow + nr;
+    unsigned short* lptr = urow + nr;
+    unsigned short* uptr = lptr + nl + 1;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + ilu_stage_bytes(nr, w.wn, nl + nu + 2, sizeof(float)) - 16);
+    unsigned short* inv = reinterpret_cast<unsigned short*>(smem_raw + a.stage_max);
+    double* Ws = reinterpret_cast<double*>(smem_raw + a.stage_max + round16(2 * (size_t)a.nr_max));
+    float* tl = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(Ws) + 8 * (size_t)a.nr_max);
+    if (threadIdx.x == 0) {
+        tc05::mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    __syncthreads();
+    const int mo = a.meta_off[b];
+    ilu_stage_bulk(val, col, a.lu, a.lu_col, w, mbar, rp, a.meta + mo, a.meta_off[b + 1] - mo);
+    for (int q = threadIdx.x; q < nr; q += blockDim.x) inv[a.lu_row[r0 + q] - r0] = (unsigned short)q;
+    const int m = a.m;
+    const double tol = a.st->tol, sqrtN = a.st->sqrtN;
+    // the cycle's initial residual norm (||D P^-1 r||, left by the host's
+    // launches in a.beta2) decides whether any step is needed
+    const double beta = sqrt(*a.beta2);
+    const double rn0 = beta / sqrtN;
+    for (int i = threadIdx.x; i <= m; i += blockDim.x) gs[i] = i == 0 ? beta : 0.0;
+    if (threadIdx.x == 0) sc[0] = a.scale[0];
+    if (!isfinite(beta) || rn0 <= tol) {
+        if (b == 0 && threadIdx.x == 0) {
+            a.st->rnorm = rn0;
+            a.st->j = 0;
+            a.st->done = isfinite(beta) ? 1 : 3;
+        }
+        tc05::mbar_wait(mbar, 0);   // the factor copies land before the block leaves
+        return;
+    }
+    bool ok = tc05::mbar_wait(mbar, 0);
+    if (!ok) ok = tc05::mbar_wait(mbar, 0);   // copies in flight get a second bounded chance
+    if (!__syncthreads_and(ok ? 1 : 0) && threadIdx.x == 0) atomicExch(a.err, 2);   // all blocks stop at the next barrier
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int sl0 = a.blksl[b], nsl = a.blksl[b + 1] - sl0;
+    // vector-major partials: pa[v * nblk + b]
+    double* pa = a.partial;
+    double* pb = a.partial + (size_t)nblk * 64;
+    // the block reads only basis rows that were complete before its last
+    // barrier (its own rows; the other rows of its edge quads are masked
+    // out and belong to blocks it waits for), so the read-only path is safe
+    const BasisRows<float, false> UR{a.U, a.ld};
+    const int q0 = r0 & ~3;
+    const int h0 = a.halo_ptr[b], nh = a.halo_ptr[b + 1] - h0;
+    const int nb0 = a.nbr_ptr[b], nb1 = a.nbr_ptr[b + 1];
+    // step 0's direction was written before the launch
+    for (int k = threadIdx.x; k < nh; k += blockDim.x) tl[k] = __ldcg(a.tdir + a.halo_node[h0 + k]);
+    __syncthreads();
+    for (int j = 0;; ++j) {
+        const int nv = j + 1;
+        // operator: x = J(cj) t for the block's rows, in factor order; a
+        // warp takes two slices at a time, eight entries of each in flight
+        for (int sl = warp; sl < nsl; sl += 2 * nw) {
+            const int slb = sl + nw < nsl ? sl + nw : sl;
+            const int ea = a.slptr[sl0 + sl] + lane, ea1 = a.slptr[sl0 + sl + 1];
+            const int eb = a.slptr[sl0 + slb] + lane, eb1 = slb != sl ? a.slptr[sl0 + slb + 1] : eb;
+            float acc_a = 0.f, acc_b = 0.f;
+            for (int k = 0; ea + 32 * k < ea1 || eb + 32 * k < eb1; k += 8) {
+                float va[8], vb[8];
+                unsigned short ca_[8], cb_[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const int e = ea + 32 * (k + t), f = eb + 32 * (k + t);
+                    // streamed once per step through L2 only, so that L1
+                    // keeps the block's basis rows between the passes
+                    va[t] = e < ea1 ? __ldcg(a.op_val + e) : 0.f;
+                    ca_[t] = e < ea1 ? __ldcg(a.op_lcol + e) : (unsigned short)0;
+                    vb[t] = f < eb1 ? __ldcg(a.op_val + f) : 0.f;
+                    cb_[t] = f < eb1 ? __ldcg(a.op_lcol + f) : (unsigned short)0;
+                }
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    acc_a = fmaf(va[t], tl[ca_[t]], acc_a);
+                    acc_b = fmaf(vb[t], tl[cb_[t]], acc_b);
+                }
+            }
+            const int qa = 32 * sl + lane, qb = 32 * slb + lane;
+            if (qa < nr) x[qa] = fmaf(-a.dcj * a.op_dg[r0 + qa], tl[a.op_self[r0 + qa]], acc_a);
+            if (slb != sl && qb < nr) x[qb] = fmaf(-a.dcj * a.op_dg[r0 + qb], tl[a.op_self[r0 + qb]], acc_b);
+        }
+        __syncthreads();
+        // preconditioner: both triangular sweeps in shared memory
+        ilu_sweep<float, KM, false>(x, val, col, rp, dg, lrow, lptr, 1, nl);
+        ilu_sweep<float, KM, true>(x, val, col, rp, dg, urow, uptr, 0, nu);
+        for (int k = threadIdx.x; k < nr; k += blockDim.x) Ws[k] = a.ewt[r0 + k] * (double)x[inv[k]];
+        __syncthreads();
+        // pass 1: a = U^T W
+        block_dots_by_warp(a.U, a.ld, Ws, r0, r1, nv, false, ca);
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
+        if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
+        block_reduce_all_vmajor(pa, nv, nblk, ca);
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = ca[i] * sc[i] * sc[i];
+        __syncthreads();
+        // pass 2: W' = W - U diag(s^2) a; b = U^T W', ||W'||^2
+        for (int r = q0 + 4 * threadIdx.x; r < r1; r += 4 * blockDim.x) {
+            double acc[4];
+            quad_combine(UR, coef, nv, r, acc);
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (r + e >= r0 && r + e < r1) Ws[r + e - r0] -= acc[e];
+        }
+        __syncthreads();
+        block_dots_by_warp(a.U, a.ld, Ws, r0, r1, nv, true, cb);
+        for (int i = threadIdx.x; i <= nv; i += blockDim.x) pb[(size_t)i * nblk + b] = cb[i];
+        if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
+        block_reduce_all_vmajor(pb, nv + 1, nblk, cb);
+        double nrm2 = cb[nv];
+        for (int i = 0; i < nv; ++i) {
+            const double c = sc[i] * cb[i];
+            nrm2 -= c * c;
+        }
+        nrm2 = nrm2 > 0.0 ? nrm2 : 0.0;
+        const double snv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = cb[i] * sc[i] * sc[i];
+        __syncthreads();
+        // pass 3: the new basis vector (unnormalised, scale snv) and the
+        // next direction D^-1 V_{j+1}
+        float* Un = a.U + a.ld * nv;
+        for (int r = q0 + 4 * threadIdx.x; r < r1; r += 4 * blockDim.x) {
+            double acc[4];
+            quad_combine(UR, coef, nv, r, acc);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int k = r + e;
+                if (k >= r0 && k < r1) {
+                    const float u = (float)(Ws[k - r0] - acc[e]);
+                    Un[k] = u;
+                    a.tdir[k] = (float)(snv * (double)u / a.ewt[k]);
+                }
+            }
+        }
+        // publish this block's rows of the next direction
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release_gpu(a.flags + b, (unsigned)nv);
+        }
+        // Hessenberg column, rotations and stopping test, the same in every
+        // block (the same reduced numbers, the same operations), on thread
+        // 0 while the other warps wait for the next direction's rows this
+        // block reads (bounded) and gather them into shared memory
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) ca[i] = sc[i] * (ca[i] + cb[i]);
+        __syncthreads();
+        if (warp > 0) {
+            if (warp == 1) {
+                for (int k = nb0 + lane; k < nb1; k += 32) {
+                    const unsigned* f = a.flags + a.nbr[k];
+                    long it = 0;
+                    while (ld_acquire_gpu(f) < (unsigned)nv) {
+                        if (++it > (1l << 26)) { atomicExch(a.err, 3); break; }
+                    }
+                }
+            }
+            named_barrier(1, blockDim.x - 32);
+            for (int k = threadIdx.x - 32; k < nh; k += blockDim.x - 32)
+                tl[k] = __ldcg(a.tdir + a.halo_node[h0 + k]);
+        } else if (threadIdx.x == 0) {
+            double* hc = ca;
+            const double hn = sqrt(nrm2);
+            hc[nv] = hn;
+            int done = 0;
+            if (!isfinite(hn) || !isfinite(hc[j])) {
+                done = 3;
+            } else {
+                double cur = hc[0];
+                for (int i = 0; i < j; ++i) {
+                    const double nx = hc[i + 1];
+                    hc[i] = rc[i] * cur + rs[i] * nx;
+                    cur = -rs[i] * cur + rc[i] * nx;
+                }
+                hc[j] = cur;
+                const double den = hypot(hc[j], hc[j + 1]);
+                double cj_, sj_;
+                if (den == 0.0) { cj_ = 1.0; sj_ = 0.0; }
+                else { cj_ = hc[j] / den; sj_ = hc[j + 1] / den; }
+                rc[j] = cj_;
+                rs[j] = sj_;
+                hc[j] = den;
+                const double gj = gs[j];
+                gs[j + 1] = -sj_ * gj;
+                gs[j] = cj_ * gj;
+                sc[nv] = snv;
+                const double rn = fabs(gs[j + 1]) / sqrtN;
+                if (rn <= tol || hn == 0.0) done = 1;
+                else if (j + 1 == m) done = 2;
+                if (b == 0) {
+                    for (int i = 0; i <= j; ++i) a.H[(size_t)i * m + j] = hc[i];
+                    a.cs[j] = cj_;
+                    a.sn[j] = sj_;
+                    a.g[j] = gs[j];
+                    a.g[j + 1] = gs[j + 1];
+                    a.scale[nv] = snv;
+                    a.st->rnorm = rn;
+                    a.st->j = j + 1;
+                }
+            }
+            if (b == 0) a.st->done = done;
+            s_done = done;
+        }
+        __syncthreads();
+        if (s_done) return;
+    }
+}
+
+// t = s_0 U_0 / ewt in FP32 (the cycle's first direction)
+__global__ void k_first_dir(int N, const float* __restrict__ U0, const double* __restrict__ scale,
+                            const double* __restrict__ ewt, float* __restrict__ t) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < N) t[k] = (float)(scale[0] * (double)U0[k] / ewt[k]);
+}
+
+// values of the operator's slices from the set-up's Jacobian (FP64 CSR) and
+// the cj coefficient of its diagonal, in factor order
+__global__ void k_op_refresh(long ne, const int* __restrict__ src, const double* __restrict__ J, float* __restrict__ v,
+                             int N, const int* __restrict__ lu_row, const double* __restrict__ ahhp,
+                             const unsigned char* __restrict__ ntype, float* __restrict__ dgq) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ne) {
+        const int p = src[t];
+        v[t] = p >= 0 ? (float)J[p] : 0.f;
+    }
+    if (t < N) {
+        const int row = lu_row[t];
+        dgq[t] = ntype[row] ? 0.f : (float)ahhp[row];
+    }
+}
+
+// Host side: the slice layout (once per pattern), the launch checks, and the
+// per-set-up refresh.  Returns false when the fused cycle cannot run on this
+// context (FP32 staged factor does not fit, or the blocks cannot all be
+// resident at once); the caller then uses the separate kernels.
+bool fused_prepare(fvm_ctx* c, int m) {
+    BlockILU* P = c->ilu;
+    if (!P || !P->built || P->factored != 1 || m + 2 > 64) return false;
+    cudaStream_t s = c->stream;
+    if (!P->op_built) {
+        P->op_built = true;
+        P->fused_ok = false;
+        const int nb = P->nb;
+        if (!P->smem_stage[1]) return false;
+        std::vector<int> slptr(1, 0), blksl(1, 0), opcol, opsrc;
+        std::vector<int> halo_ptr(1, 0), halo_node, nbr_ptr(1, 0), nbr;
+        std::vector<unsigned short> lcol, self(c->N);
+        std::vector<int> where(c->N, -1);
+        int nr_max = 0, nh_max = 0;
+        for (int b = 0; b < nb; ++b) {
+            const int r0 = P->h_bstart[b], r1 = P->h_bstart[b + 1];
+            nr_max = std::max(nr_max, r1 - r0);
+            const size_t ebase = opcol.size();
+            for (int q0 = r0; q0 < r1; q0 += 32) {
+                const int n = std::min(32, r1 - q0);
+                int width = 0;
+                for (int l = 0; l < n; ++l) {
+                    const int row = P->h_lu_row[q0 + l];
+                    width = std::max(width, P->h_rowptr[row + 1] - P->h_rowptr[row]);
+                }
+                const size_t base = opcol.size();
+                opcol.resize(base + 32 * (size_t)width);
+                opsrc.resize(base + 32 * (size_t)width);
+                for (int l = 0; l < 32; ++l) {
+                    const int row = l < n ? P->h_lu_row[q0 + l] : P->h_lu_row[q0];
+                    const int p0 = P->h_rowptr[row], len = l < n ? P->h_rowptr[row + 1] - p0 : 0;
+                    for (int k = 0; k < width; ++k) {
+                        opcol[base + 32 * (size_t)k + l] = k < len ? P->h_col[p0 + k] : row;
+                        opsrc[base + 32 * (size_t)k + l] = k < len ? p0 + k : -1;
+                    }
+                }
+                if (opcol.size() >= (size_t)INT32_MAX) return false;
+                slptr.push_back((int)opcol.size());
+            }
+            blksl.push_back((int)slptr.size() - 1);
+            // the block's node list (its operator columns, sorted), local
+            // column indices, and the blocks owning those nodes
+            std::vector<int> nodes(opcol.begin() + ebase, opcol.end());
+            std::sort(nodes.begin(), nodes.end());
+            nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+            if (nodes.size() >= 65535) return false;
+            nh_max = std::max(nh_max, (int)nodes.size());
+            for (size_t k = 0; k < nodes.size(); ++k) where[nodes[k]] = (int)k;
+            for (size_t e = ebase; e < opcol.size(); ++e) lcol.push_back((unsigned short)where[opcol[e]]);
+            for (int q = r0; q < r1; ++q) self[q] = (unsigned short)where[P->h_lu_row[q]];
+            std::vector<int> nbs;
+            if (b > 0) nbs.push_back(b - 1);
+            if (b + 1 < nb) nbs.push_back(b + 1);
+            for (int v : nodes) {
+                const int ob = (int)(std::upper_bound(P->h_bstart.begin(), P->h_bstart.end(), v) - P->h_bstart.begin()) - 1;
+                if (ob != b) nbs.push_back(ob);
+            }
+            std::sort(nbs.begin(), nbs.end());
+            nbs.erase(std::unique(nbs.begin(), nbs.end()), nbs.end());
+            nbr.insert(nbr.end(), nbs.begin(), nbs.end());
+            nbr_ptr.push_back((int)nbr.size());
+            halo_node.insert(halo_node.end(), nodes.begin(), nodes.end());
+            halo_ptr.push_back((int)halo_node.size());
+            for (int v : nodes) where[v] = -1;
+        }
+        P->op_slptr.upload(slptr, s);
+        P->op_blksl.upload(blksl, s);
+        P->op_lcol.upload(lcol, s);
+        P->op_self.upload(self, s);
+        P->op_src.upload(opsrc, s);
+        P->halo_ptr.upload(halo_ptr, s);
+        P->halo_node.upload(halo_node, s);
+        P->nbr_ptr.upload(nbr_ptr, s);
+        P->nbr.upload(nbr, s);
+        P->flags.alloc(nb);
+        P->op_val.alloc(opcol.size());
+        P->op_dg.alloc(c->N);
+        P->fused_nrmax = nr_max;
+        P->fused_nhmax = nh_max;
+        P->fused_stage = round16(P->smem_stage[1]);
+        P->fused_smem = P->fused_stage + round16(2 * (size_t)nr_max) + 8 * (size_t)nr_max + 4 * (size_t)nh_max;
+        // one thread per row quad of the largest block, whole warps
+        P->fused_threads = std::min(kFusedThreads, std::max(128, ((nr_max + 3) / 4 + 1 + 31) / 32 * 32));
+        if (P->fused_smem > kMaxDynSmem) return false;
+        const void* kfn = P->lanes == 8 ? (const void*)k_arnoldi_fused<8> : (const void*)k_arnoldi_fused<4>;
+        raise_smem_limit(kfn, P->fused_smem);
+        // the smallest shared-memory carveout that holds the block's
+        // shared data (dynamic + static, about 1 KB reserved), so that the
+        // rest of the SM's 256 KB stays L1 for the block's basis rows
+        {
+            cudaFuncAttributes fa;
+            FVM_CUDA(cudaFuncGetAttributes(&fa, kfn));
+            const double need = (double)(P->fused_smem + fa.sharedSizeBytes + 1024);
+            const int pct = std::min(100, (int)std::ceil(100.0 * need / (228.0 * 1024.0)));
+            FVM_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        }
+        int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+        FVM_CUDA(cudaGetDevice(&dev));
+        FVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        FVM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, P->fused_threads, P->fused_smem));
+        P->fused_ok = coop && per_sm > 0 && nb <= per_sm * nsm;
+    }
+    if (!P->fused_ok) return false;
+    if (P->op_setup_id != P->setup_id) {
+        const long ne = (long)P->op_val.n;
+        const long nt = std::max(ne, (long)c->N);
+        fvm_launch(c, k_op_refresh, grid_for(nt, 256), 256, 0, s, ne, P->op_src.p, P->J.p, P->op_val.p, c->N,
+                   P->lu_row.p, P->ahhp.p, c->ntype.p, P->op_dg.p);
+        P->op_setup_id = P->setup_id;
+    }
+    return true;
+}
+
+// one cycle: the Arnoldi state (j = 0), g[0] and U_0 with its scale are in
+// place; runs until convergence, a full basis or a breakdown
+void fused_cycle(fvm_ctx* c, Krylov* K, double cj, const double* ewt, double* H_d, double* cs_d, double* sn_d,
+                 double* g_d) {
+    BlockILU* P = c->ilu;
+    cudaStream_t s = c->stream;
+    float* U = reinterpret_cast<float*>(K->U);
+    if (K->tdir.n < (size_t)c->N) K->tdir.alloc(c->N);
+    fvm_launch(c, k_first_dir, grid_for(c->N, 256), 256, 0, s, c->N, U, K->scale.p, ewt, K->tdir.p);
+    FusedArgs a;
+    a.N = c->N;
+    a.m = K->m;
+    a.nr_max = P->fused_nrmax;
+    a.nh_max = P->fused_nhmax;
+    a.stage_max = P->fused_stage;
+    a.st = K->st.p;
+    a.U = U;
+    a.ld = K->ld;
+    a.scale = K->scale.p;
+    a.tdir = K->tdir.p;
+    a.ewt = ewt;
+    a.slptr = P->op_slptr.p;
+    a.blksl = P->op_blksl.p;
+    a.op_lcol = P->op_lcol.p;
+    a.op_self = P->op_self.p;
+    a.halo_ptr = P->halo_ptr.p;
+    a.halo_node = P->halo_node.p;
+    a.nbr_ptr = P->nbr_ptr.p;
+    a.nbr = P->nbr.p;
+    a.flags = P->flags.p;
+    a.op_val = P->op_val.p;
+    a.op_dg = P->op_dg.p;
+    a.dcj = (float)(cj - P->cj_setup);
+    a.bstart = P->bstart.p;
+    a.lu_ptr = P->lu_ptr.p;
+    a.lu_col = P->lu_col.p;
+    a.meta = P->meta.p;
+    a.meta_off = P->meta_off.p;
+    a.blk_lvl = P->blk_lvl.p;
+    a.blk_ulvl = P->blk_ulvl.p;
+    a.lu = P->lu32.p;
+    a.lu_row = P->lu_row.p;
+    a.beta2 = K->res.p;
+    a.partial = K->partial.p;
+    a.bar = K->bar.p;
+    a.err = K->err.p;
+    a.H = H_d;
+    a.cs = cs_d;
+    a.sn = sn_d;
+    a.g = g_d;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(P->nb);
+    cfg.blockDim = dim3(P->fused_threads);
+    cfg.dynamicSmemBytes = P->fused_smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    P->flags.zero(s);
+    c->tm.begin(TM_CGS, s);
+    if (P->lanes == 8) FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_fused<8>, a));
+    else FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_fused<4>, a));
+    c->tm.end(TM_CGS, s);
+    c->launches++;
+}
+
+} // namespace fvmb

@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -29,6 +30,18 @@ namespace fvmb {
 
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+void raise_smem_limit(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limit;
+    int dev = 0;
+    FVM_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = limit[{dev, func}];
+    if (bytes <= cur) return;
+    FVM_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+}
 
 constexpr int kBlock = 256;
 constexpr int kDefaultChunk = 512;   // elements per chunk of the element pass
@@ -437,7 +450,7 @@ static size_t chunk_smem_bytes(const fvm_ctx* c, int CE, int nnmax) {
 
 static void set_chunk_attrs(fvm_ctx* c) {
     with_elem_kernel(c, [&](auto k) {
-        FVM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->chunk_smem));
+        raise_smem_limit(k, c->chunk_smem);
     });
 }
 

@@ -305,4 +305,14 @@ void reset_upwind(fvm_ctx* c);
 
 inline int grid_for(long n, int block) { return (int)((n + block - 1) / block); }
 
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`.  The limit belongs to the kernel function for the whole
+// process, not to a context, so it is only ever raised: a context built for
+// a smaller mesh must not lower the limit that another live context's
+// launches need.
+void raise_smem_limit(const void* func, size_t bytes);
+template <typename... KArgs> inline void raise_smem_limit(void (*k)(KArgs...), size_t bytes) {
+    raise_smem_limit(reinterpret_cast<const void*>(k), bytes);
+}
+
 } // namespace fvmb

@@ -35,8 +35,10 @@ struct Krylov {
     size_t coop_smem = 0;     // dynamic shared memory of the fused kernel
     int coop_threads = 0;     // its block size: one thread per row quad of a block, 128..512
     DevBuf<ArnState> st;      // device-driven Arnoldi state
+    DevBuf<float> tdir;       // FP32 direction of the fused cycle (arnoldi_fused.cu)
     DevBuf<double> ls;        // H [(m+1) x m], cs [m], sn [m], g [m+1]
     double* host = nullptr;   // pinned
+    double* host_ls = nullptr;   // pinned: H and g of a fused cycle
 };
 
 struct GmresCounters {
@@ -65,6 +67,13 @@ void psolve_dev(fvm_ctx* c, const double* r, double* z, const int* skip = nullpt
 // y = J(cj) x with the assembled difference-quotient Jacobian of the last
 // set-up (the Krylov operator of fvm_opts.krylov_operator = 1)
 void jacobian_apply(fvm_ctx* c, double cj, const double* x, double* y, const int* skip = nullptr);
+// fused Arnoldi cycle of the assembled operator (arnoldi_fused.cu):
+// fused_prepare refreshes the operator after a set-up and tells whether the
+// cycle can run (FP32 factor staged in shared memory, every block resident);
+// fused_cycle runs one cycle from the state gmres has put in place
+bool fused_prepare(fvm_ctx* c, int m);
+void fused_cycle(fvm_ctx* c, Krylov* K, double cj, const double* ewt, double* H_d, double* cs_d, double* sn_d,
+                 double* g_d);
 bool ilu_ready(fvm_ctx* c);
 int ilu_status(fvm_ctx* c);   // 0 ok, 1 zero pivot in the last factorisation
 

@@ -21,6 +21,7 @@
 // bitwise reproducible.  The Hessenberg matrix, Givens rotations and the
 // stopping test run in FP64 on the host from j+2 numbers copied back per
 // step.
+#include "cgs.cuh"
 #include "ctx.cuh"
 #include "krylov.cuh"
 #include "reduce.cuh"
@@ -156,170 +157,6 @@ __global__ void k_cgs_pass3(int N, int nv, B* __restrict__ U, size_t ld,
         if (threadIdx.x == 0) partial[blockIdx.x] = t;
     }
     last_block_reduce(partial, 1, counter, out);
-}
-
-// ---- fused Arnoldi orthogonalisation (one cooperative launch per step)
-// Grid barrier of a cooperative launch: arrival counter plus generation
-// word.  The wait is bounded; if it runs out the kernel records error 3 and
-// every block leaves at its next barrier.
-__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, int* err) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* vg = gen;
-        const unsigned g = *vg;
-        __threadfence();
-        if (atomicAdd(count, 1u) == gridDim.x - 1) {
-            *count = 0u;
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
-            long it = 0;
-            while (*vg == g) {
-                if (++it > (1l << 26)) { atomicExch(err, 3); break; }
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return *(volatile int*)err == 0;
-}
-
-// out[v] = sum over blocks b (ascending, lane-strided, fixed shuffle tree) of
-// partial[b * nv + v] -- the order of last_block_reduce, so every block gets
-// the same bits; written to shared memory.  The partials were written by
-// other blocks before the grid barrier: they are read through L2 (ld.cg,
-// never a stale L1 line), a warp taking 4 vectors and each lane 5 blocks at
-// a time so that 20 loads per lane are in flight.
-__device__ __forceinline__ void block_reduce_all(const double* partial, int nv, int nblk, double* out) {
-    constexpr int kQ = 4, kI = 5;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int v0 = warp; v0 < nv; v0 += kQ * nw) {
-        double s[kQ];
-#pragma unroll
-        for (int q = 0; q < kQ; ++q) s[q] = 0.0;
-        for (int b0 = 0; b0 < nblk; b0 += 32 * kI) {
-            double x[kI][kQ];
-#pragma unroll
-            for (int i = 0; i < kI; ++i) {
-                const int b = b0 + lane + 32 * i;
-#pragma unroll
-                for (int q = 0; q < kQ; ++q) {
-                    const int v = v0 + q * nw;
-                    x[i][q] = (b < nblk && v < nv) ? __ldcg(partial + (size_t)b * nv + v) : 0.0;
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < kI; ++i)
-#pragma unroll
-                for (int q = 0; q < kQ; ++q) s[q] += x[i][q];
-        }
-#pragma unroll
-        for (int q = 0; q < kQ; ++q) {
-            const double t = warp_sum(s[q]);
-            const int v = v0 + q * nw;
-            if (lane == 0 && v < nv) out[v] = t;
-        }
-    }
-    __syncthreads();
-}
-
-constexpr int kCgsThreads = 512;
-constexpr int kCgsGroup = 8;   // basis vectors whose loads are in flight together
-
-// rows per block of the fused orthogonalisation: ceil(N / nblk) rounded up
-// to 4, so every block's rows start on a 4-row (16-byte FP32 / 32-byte
-// FP64) boundary and each thread owns whole quads of rows
-__host__ __device__ inline int cgs_chunk(int N, int nblk) {
-    const int c = (N + nblk - 1) / nblk;
-    return (c + 3) & ~3;
-}
-
-// four consecutive basis values starting at a 4-aligned row (the basis
-// allocation is padded to a multiple of 64 rows and zeroed, so a quad that
-// straddles row N reads zeros)
-__device__ __forceinline__ void ld4(const float* p, double v[4]) {
-    const float4 q = __ldg(reinterpret_cast<const float4*>(p));
-    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
-}
-__device__ __forceinline__ void ld4(const double* p, double v[4]) {
-    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
-    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-}
-// the basis, read by row quads through the read-only path (the block's
-// rows of the vectors stay in L1 between the three passes)
-template <class B>
-struct BasisRows {
-    const B* U;
-    size_t ld;
-    __device__ __forceinline__ void quad(int i, int r, double v[4]) const { ld4(U + ld * i + r, v); }
-};
-
-// block-local dot products <U_i, W> over rows [k0, k1) for i < nv, with the
-// block's W rows in shared memory (Wl[k - k0]).  Each thread owns quads of
-// rows; the vectors are taken kCgsGroup at a time so that many loads are in
-// flight per thread.  Per vector: the thread's quads in row order, then the
-// warp's lanes by a fixed shuffle tree, then the warps in warp order.  Row
-// nv of the output (when with_norm) is sum W^2.  out[i] is valid in every
-// thread after the call.  red holds kCgsGroup doubles per warp.
-template <class B>
-__device__ __forceinline__ void block_dots(const BasisRows<B>& U, const double* __restrict__ Wl, int k0, int k1,
-                                           int nv, bool with_norm, double* red, double* out) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int nvec = nv + (with_norm ? 1 : 0);
-    for (int i0 = 0; i0 < nvec; i0 += kCgsGroup) {
-        double acc[kCgsGroup];
-#pragma unroll
-        for (int q = 0; q < kCgsGroup; ++q) acc[q] = 0.0;
-        for (int r = k0 + 4 * threadIdx.x; r < k1; r += 4 * blockDim.x) {
-            double w[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) w[e] = r + e < k1 ? Wl[r + e - k0] : 0.0;
-#pragma unroll
-            for (int q = 0; q < kCgsGroup; ++q) {
-                const int i = i0 + q;
-                if (i < nv) {
-                    double u[4];
-                    U.quad(i, r, u);
-                    acc[q] += u[0] * w[0] + u[1] * w[1] + u[2] * w[2] + u[3] * w[3];
-                } else if (i == nv && with_norm) {
-                    acc[q] += w[0] * w[0] + w[1] * w[1] + w[2] * w[2] + w[3] * w[3];
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kCgsGroup; ++q) acc[q] = warp_sum(acc[q]);
-        if (lane == 0) {
-#pragma unroll
-            for (int q = 0; q < kCgsGroup; ++q) red[warp * kCgsGroup + q] = acc[q];
-        }
-        __syncthreads();
-        if (threadIdx.x < kCgsGroup && i0 + threadIdx.x < nvec) {
-            double t = 0.0;
-            for (int w2 = 0; w2 < nw; ++w2) t += red[w2 * kCgsGroup + threadIdx.x];
-            out[i0 + threadIdx.x] = t;
-        }
-        __syncthreads();
-    }
-}
-
-// acc[e] = sum_i coef[i] U_i[r + e], e < 4, vectors kCgsGroup at a time
-template <class B>
-__device__ __forceinline__ void quad_combine(const BasisRows<B>& U, const double* coef, int nv, int r,
-                                             double acc[4]) {
-    acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
-    for (int i0 = 0; i0 < nv; i0 += kCgsGroup) {
-#pragma unroll
-        for (int q = 0; q < kCgsGroup; ++q) {
-            const int i = i0 + q;
-            if (i < nv) {
-                double u[4];
-                U.quad(i, r, u);
-                const double c = coef[i];
-                acc[0] += c * u[0]; acc[1] += c * u[1]; acc[2] += c * u[2]; acc[3] += c * u[3];
-            }
-        }
-    }
 }
 
 // One Arnoldi step of the device-driven GMRES in one cooperative launch:
@@ -581,6 +418,7 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
     // results of the three passes, the m+1 basis scales, a status word and
     // the device-driven Arnoldi state
     FVM_CUDA(cudaMallocHost(&K->host, sizeof(double) * (4 * (m + 2) + 8) + sizeof(ArnState)));
+    FVM_CUDA(cudaMallocHost(&K->host_ls, sizeof(double) * ((size_t)(m + 1) * m + m + 1)));
     c->kry[precision] = K;
     return c->kry_last = K;
 }
@@ -589,6 +427,7 @@ void fvmb_destroy_krylov_impl(Krylov* K) {
     if (!K) return;
     if (K->U) cudaFree(K->U);
     if (K->host) cudaFreeHost(K->host);
+    if (K->host_ls) cudaFreeHost(K->host_ls);
     delete K;
 }
 
@@ -656,17 +495,61 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         fvm_launch(c, k_init_residual<B>, kRedBlocks, kRedThreads, 0, s, N, K->z.p, nullptr, ewt, U,
                                                               K->partial.p, K->counter.p, K->res.p);
         fvm_launch(c, k_set_scale, 1, 1, 0, s, K->res.p, K->scale.p, 0);
-        FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-        FVM_CUDA(cudaStreamSynchronize(s));
-        double beta = std::sqrt(K->host[0]);
-        rnorm = beta / sqrtN;
-        if (!std::isfinite(beta)) { *iters = total; *res_norm = rnorm; return 2; }
-        if (rnorm <= tol) { *iters = total; *res_norm = rnorm; return 0; }
+        // the assembled operator with the FP32 factor and basis: the whole
+        // cycle in one persistent launch (arnoldi_fused.cu), which also takes
+        // the initial norm from K->res and decides there whether any step is
+        // needed, so the host waits once per cycle
+        const bool fused = op && sizeof(B) == sizeof(float) && K->coop_grid > 0 && fused_prepare(c, m);
         std::fill(g.begin(), g.end(), 0.0);
-        g[0] = beta;
+        if (!fused) {
+            FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaStreamSynchronize(s));
+            const double beta = std::sqrt(K->host[0]);
+            rnorm = beta / sqrtN;
+            if (!std::isfinite(beta)) { *iters = total; *res_norm = rnorm; return 2; }
+            if (rnorm <= tol) { *iters = total; *res_norm = rnorm; return 0; }
+            g[0] = beta;
+        }
         int j = 0;
         bool conv = false;
-        if (K->coop_grid > 0) {
+        if (fused) {
+            ArnState* hst = reinterpret_cast<ArnState*>(K->host + 4 * (m + 2) + 8);
+            *hst = ArnState{0, 0, m, 0, tol, sqrtN, 0.0};
+            FVM_CUDA(cudaMemcpyAsync(K->st.p, hst, sizeof(ArnState), cudaMemcpyHostToDevice, s));
+            double* H_d = K->ls.p;
+            double* cs_d = H_d + (size_t)(m + 1) * m;
+            double* sn_d = cs_d + m;
+            double* g_d = sn_d + m;
+            fused_cycle(c, K, cj, ewt, H_d, cs_d, sn_d, g_d);
+            // state, status, least-squares data and scales in one wait
+            int* herr = reinterpret_cast<int*>(K->host + 4 * (m + 2) + 7);
+            double* hls = K->host_ls;
+            FVM_CUDA(cudaMemcpyAsync(hst, K->st.p, sizeof(ArnState), cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaMemcpyAsync(herr, K->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaMemcpyAsync(hls, H_d, sizeof(double) * ((size_t)(m + 1) * m), cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaMemcpyAsync(hls + (size_t)(m + 1) * m, g_d, sizeof(double) * (m + 1), cudaMemcpyDeviceToHost,
+                                     s));
+            FVM_CUDA(cudaMemcpyAsync(K->host + 3 * (m + 2), K->scale.p, sizeof(double) * (m + 1),
+                                     cudaMemcpyDeviceToHost, s));
+            FVM_CUDA(cudaStreamSynchronize(s));
+            if (*herr != 0) {
+                // a grid barrier, a flag wait or the factor copy gave up
+                K->err.zero(s);
+                K->bar.zero(s);
+                *iters = total + hst->j;
+                *res_norm = hst->rnorm;
+                return 2;
+            }
+            j = hst->j;
+            total += j;
+            if (cnt) { cnt->njv += j; cnt->nps += j; }
+            rnorm = hst->rnorm;
+            if (hst->done == 3) { *iters = total; *res_norm = rnorm; return 2; }
+            if (j == 0) { *iters = total; *res_norm = rnorm; return 0; }   // already within tol
+            conv = hst->done == 1;
+            std::copy(hls, hls + (size_t)(m + 1) * m, H.begin());
+            std::copy(hls + (size_t)(m + 1) * m, hls + (size_t)(m + 1) * m + m + 1, g.begin());
+        } else if (K->coop_grid > 0) {
             // Device-driven Arnoldi: each step is J*v, the preconditioner,
             // the fused CGS2 and the Givens update, all reading the step
             // index and the stop flag from device memory; steps are queued
@@ -680,13 +563,13 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
             double* sn_d = cs_d + m;
             double* g_d = sn_d + m;
             FVM_CUDA(cudaMemcpyAsync(g_d, g.data(), sizeof(double) * (m + 1), cudaMemcpyHostToDevice, s));
+            const int* skip = &K->st.p->done;
+            int queued = 0;
             // first direction and its increment
             fvm_launch(c, k_unscale<B>, grid_for(N, 256), 256, 0, s, N, U, K->scale.p, 0, ewt, K->t.p);
             fvm_launch(c, k_sumsq, kRedBlocks, kRedThreads, 0, s, N, K->t.p, ewt, K->partial.p, K->counter.p,
                        K->res.p);
             fvm_launch(c, k_sigma_from_sumsq, 1, 1, 0, s, K->res.p, N, K->sigma.p);
-            const int* skip = &K->st.p->done;
-            int queued = 0;
             for (;;) {
                 // 2 steps, then 8 per host look: steps queued after the stop
                 // cost little (every kernel of the chain returns at once), a

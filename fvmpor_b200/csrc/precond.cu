@@ -26,6 +26,7 @@
 // levels, for both the factorisation and the triangular solves
 // (decomp/ILU.c:133-223).
 #include "ctx.cuh"
+#include "ilu.cuh"
 #include "krylov.cuh"
 #include "tc05.cuh"
 
@@ -35,56 +36,6 @@
 #include <cmath>
 
 namespace fvmb {
-
-struct BlockILU {
-    bool built = false;
-    int nnz = 0, ncol = 0;
-    std::vector<int> h_rowptr, h_col, h_colour;
-    DevBuf<int> rowof, col;
-    DevBuf<double> J;
-    DevBuf<double> shift;
-    // element-wise finite-difference Jacobian
-    DevBuf<int> fd_epos;      // [T*npe*npe] slot of (element, perturbed node, corner)
-    DevBuf<int> fd_jptr;      // [nnz+1] slots of each nonzero
-    DevBuf<double> fd_slots;  // [T*npe*npe]
-    DevBuf<double> krwb, krwp, dstor;
-    // assembled-operator Krylov products (fvm_opts.krylov_operator = 1):
-    // device row pointers of J, the storage coefficient ahh(h + d) behind
-    // the cj term of J's diagonal, and the cj of the current set-up
-    DevBuf<int> rowptr;
-    DevBuf<double> ahhp;
-    double cj_setup = 0.0;
-    int nb = 0, maxb = 0;
-    DevBuf<int> bstart, lu_ptr, lu_src, lu_diag;
-    DevBuf<int> lu_row;       // global row of each factor position (colour order inside the blocks)
-    // ILU(0) elimination schedule of the shared-memory factorisation, one
-    // contiguous segment per level (upd[seg_ptr[g] .. seg_ptr[g+1]) for the
-    // global level g): the offset of each row's list in the segment, then
-    // per row and per L entry in column order a count word followed by that
-    // many (target | source << 16) window positions
-    DevBuf<int> seg_ptr;
-    DevBuf<unsigned> upd;
-    int scr_words[2] = {0, 0};   // shared-memory schedule scratch of the factorisation (words), by precision
-    DevBuf<unsigned short> lu_col;
-    DevBuf<int> lvl_ptr, lvl_rows, blk_lvl, ulvl_ptr, ulvl_rows, blk_ulvl;
-    DevBuf<unsigned short> meta;   // per-block metadata records of the staged apply
-    DevBuf<int> meta_off;
-    DevBuf<double> lu64;
-    DevBuf<float> lu32;
-    int factored = -1;        // precision of the current factor, -1 none
-    DevBuf<int> status;
-    int* h_status = nullptr;  // pinned
-    int nlevels_max = 0;
-    size_t smem_stage[2] = {0, 0};   // staged apply: shared bytes for FP64 / FP32, 0 = not possible
-    int lanes = 4;                   // row entries prefetched per thread in the staged sweeps
-    int apply_threads = 128;         // CTA of the staged apply: 128, or 256 when a level is wider
-};
-
-// largest dynamic shared-memory carve-out a CTA may request on sm_100
-constexpr size_t kMaxDynSmem = 227 * 1024;
-// threads of a staged triangular-solve CTA: levels hold a few dozen rows,
-// so a small CTA keeps the per-level barrier cheap
-constexpr int kIluThreads = 256;   // largest CTA of the staged apply
 
 // ------------------------------------------------------------------ kernels
 __global__ void k_shift(int N, const double* __restrict__ y, const double* __restrict__ yp,
@@ -362,143 +313,6 @@ __global__ void __launch_bounds__(128) k_ilu_apply(const int* __restrict__ bstar
         __syncthreads();
     }
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) z[lu_row[i]] = (double)x[i - r0];
-}
-
-// Staged variant: the CTA first brings its block's factor into shared
-// memory, then runs the level loops entirely there, so each level costs a
-// few shared-memory latencies and a barrier instead of a dependent chain of
-// L2/HBM loads.  The block's entries are one contiguous range of the factor
-// arrays; the copy window is that range widened to 8-entry (16-byte)
-// boundaries and moved by two 1D TMA bulk copies (cp.async.bulk, completion
-// counted on an mbarrier, bounded wait), while the threads fill the row
-// pointers, pivot positions, level lists and right-hand side alongside.
-// Shared layout: x[T nrows, 16-B padded] | val[T window] | col[u16 window] |
-// rp[u16 nrows+1] | dg[u16 nrows] | lrow[u16 nrows] | urow[u16 nrows] |
-// lptr[u16 nl+1] | uptr[u16 nu+1] | mbarrier (8-B aligned)
-struct IluWindow {
-    int base, wn;   // first entry of the copy window (multiple of 8), window length
-};
-__device__ __forceinline__ IluWindow ilu_window(int e0, int e1) {
-    IluWindow w;
-    w.base = e0 & ~7;
-    w.wn = ((e1 + 7) & ~7) - w.base;
-    return w;
-}
-__host__ __device__ __forceinline__ size_t round16(size_t b) { return (b + 15) & ~(size_t)15; }
-
-// u16 words of a block's metadata record: rp (nr+1) | dg (nr) | lrow (nr) |
-// urow (nr) | lptr (nl+1) | uptr (nu+1), padded to 16 bytes
-__host__ __device__ __forceinline__ size_t ilu_meta_words(size_t nr, size_t nlev) {
-    return (4 * nr + 1 + nlev + 7) & ~(size_t)7;
-}
-
-// shared bytes of the staged kernels for one block (host and device agree);
-// nlev = nl + 1 + nu + 1 level offsets of the two sweeps
-__host__ __device__ __forceinline__ size_t ilu_stage_bytes(size_t nr, size_t wn, size_t nlev, size_t sz) {
-    return round16(round16(nr * sz) + wn * (sz + 2) + ilu_meta_words(nr, nlev) * 2) + 16;
-}
-
-template <class T>
-__device__ __forceinline__ void ilu_stage_bulk(T* val, unsigned short* col, const T* lu,
-                                               const unsigned short* lu_col, IluWindow w, uint64_t* bar,
-                                               unsigned short* meta_dst = nullptr,
-                                               const unsigned short* meta_src = nullptr, int meta_words = 0) {
-    if (threadIdx.x == 0) {
-        uint32_t b = tc05::smem_u32(bar);
-        uint32_t bytes = (uint32_t)(w.wn * (sizeof(T) + sizeof(unsigned short)) + meta_words * 2);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes));
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                         tc05::smem_u32(val)),
-                     "l"(lu + w.base), "r"((uint32_t)(w.wn * sizeof(T))), "r"(b)
-                     : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                         tc05::smem_u32(col)),
-                     "l"(lu_col + w.base), "r"((uint32_t)(w.wn * sizeof(unsigned short))), "r"(b)
-                     : "memory");
-        if (meta_words)
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                             tc05::smem_u32(meta_dst)),
-                         "l"(meta_src), "r"((uint32_t)(meta_words * 2)), "r"(b)
-                         : "memory");
-    }
-}
-
-// One triangular sweep over the levels [l0, nlv): rows of a level are
-// independent, one thread per row.  UPPER: x_i = (x_i - sum_{p>diag}) *
-// inverse pivot; else x_i = x_i - sum_{p<diag} (unit lower triangle).  A
-// thread's row of level l+1 -- its index, range, first KM entries and pivot,
-// none of which depend on x -- is fetched while level l is computed, so after
-// each barrier only the x loads (independent of each other) and the
-// accumulation remain on the critical path.
-template <class T, int KM, bool UPPER> struct IluRow {
-    int li, p0, p1;
-    T v[KM];
-    unsigned short c[KM];
-    T piv;
-};
-
-template <class T, int KM, bool UPPER>
-__device__ __forceinline__ void ilu_fetch(IluRow<T, KM, UPPER>& R, int l, int nlv, const T* val,
-                                          const unsigned short* col, const unsigned short* rp,
-                                          const unsigned short* dg, const unsigned short* rows,
-                                          const unsigned short* lptr) {
-    R.li = -1;
-#pragma unroll
-    for (int k = 0; k < KM; ++k) R.c[k] = 0;
-    if (l >= nlv) return;
-    const int q = lptr[l] + threadIdx.x;
-    if (q >= lptr[l + 1]) return;
-    R.li = rows[q];
-    const int d = dg[R.li];
-    R.p0 = UPPER ? d + 1 : rp[R.li];
-    R.p1 = UPPER ? rp[R.li + 1] : d;
-#pragma unroll
-    for (int k = 0; k < KM; ++k) {
-        const int p = R.p0 + k < R.p1 ? R.p0 + k : 0;   // unused slots read entry 0
-        R.v[k] = val[p];
-        R.c[k] = col[p];
-    }
-    R.piv = UPPER ? val[d] : (T)1;
-}
-
-template <class T, int KM, bool UPPER>
-__device__ __forceinline__ void ilu_sweep(T* x, const T* val, const unsigned short* col, const unsigned short* rp,
-                                          const unsigned short* dg, const unsigned short* rows,
-                                          const unsigned short* lptr, int l0, int nlv) {
-    IluRow<T, KM, UPPER> cur, nxt;
-    ilu_fetch(cur, l0, nlv, val, col, rp, dg, rows, lptr);
-    for (int l = l0; l < nlv; ++l) {
-        // issue this level's x loads first (threads without a row read entry
-        // 0 and store nothing), then fetch the next level's row while they
-        // are in flight, then accumulate
-        const bool act = cur.li >= 0;
-        const int li = act ? cur.li : 0;
-        T xv[KM];
-#pragma unroll
-        for (int k = 0; k < KM; ++k) xv[k] = x[cur.c[k]];
-        const T xi = x[li];
-        const int q0 = lptr[l], q1 = lptr[l + 1];
-        ilu_fetch(nxt, l + 1, nlv, val, col, rp, dg, rows, lptr);
-        if (act) {
-            T acc = (T)0;
-#pragma unroll
-            for (int k = 0; k < KM; ++k)
-                if (cur.p0 + k < cur.p1) acc += cur.v[k] * xv[k];
-            for (int p = cur.p0 + KM; p < cur.p1; ++p) acc += val[p] * x[col[p]];
-            x[li] = UPPER ? (xi - acc) * cur.piv : xi - acc;
-        }
-        // rows of a level wider than the CTA
-        for (int q = q0 + threadIdx.x + blockDim.x; q < q1; q += blockDim.x) {
-            const int lj = rows[q];
-            const int d = dg[lj];
-            const int p0 = UPPER ? d + 1 : rp[lj], p1 = UPPER ? rp[lj + 1] : d;
-            T acc = (T)0;
-            for (int p = p0; p < p1; ++p) acc += val[p] * x[col[p]];
-            x[lj] = UPPER ? (x[lj] - acc) * val[d] : x[lj] - acc;
-        }
-        __syncthreads();
-        cur = nxt;
-    }
 }
 
 template <class T, int KM>
@@ -959,20 +773,14 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
         for (size_t g = 0; g + 1 < ulvl_ptr.size(); ++g) widest = std::max(widest, ulvl_ptr[g + 1] - ulvl_ptr[g]);
         P->apply_threads = widest > 128 ? 256 : 128;
         if (P->smem_stage[0]) {
-            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)P->smem_stage[0]));
-            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)P->smem_stage[0]));
-            FVM_CUDA(cudaFuncSetAttribute(k_ilu_factor_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)(round16(P->smem_stage[0]) + 8 * (size_t)P->scr_words[0])));
+            raise_smem_limit(k_ilu_apply_smem<double, 4>, (size_t)P->smem_stage[0]);
+            raise_smem_limit(k_ilu_apply_smem<double, 8>, (size_t)P->smem_stage[0]);
+            raise_smem_limit(k_ilu_factor_smem<double>, (size_t)(round16(P->smem_stage[0]) + 8 * (size_t)P->scr_words[0]));
         }
         if (P->smem_stage[1]) {
-            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)P->smem_stage[1]));
-            FVM_CUDA(cudaFuncSetAttribute(k_ilu_apply_smem<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)P->smem_stage[1]));
-            FVM_CUDA(cudaFuncSetAttribute(k_ilu_factor_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)(round16(P->smem_stage[1]) + 8 * (size_t)P->scr_words[1])));
+            raise_smem_limit(k_ilu_apply_smem<float, 4>, (size_t)P->smem_stage[1]);
+            raise_smem_limit(k_ilu_apply_smem<float, 8>, (size_t)P->smem_stage[1]);
+            raise_smem_limit(k_ilu_factor_smem<float>, (size_t)(round16(P->smem_stage[1]) + 8 * (size_t)P->scr_words[1]));
         }
     }
     cudaStream_t s = c->stream;
@@ -989,6 +797,8 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
     P->ahhp.alloc(N);
     P->rowptr.upload(P->h_rowptr, s);
     P->bstart.upload(bstart, s);
+    P->h_bstart = bstart;
+    P->h_lu_row = lu_row;
     P->lu_ptr.upload(lu_ptr, s);
     // 8 padding entries so every block's widened copy window stays inside
     lu_src.resize(lu_src.size() + 8, 0);
@@ -1028,6 +838,7 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     fvm_launch(c, k_fd_node, grid_for(N, 256), 256, 0, s, N, y, yp, cj, P->shift.p, c->zones.p, c->nz, c->nz_ptr.p,
                c->nz_zone.p, c->nz_w.p, c->rho0, P->krwb.p, P->krwp.p, P->dstor.p, P->ahhp.p);
     P->cj_setup = cj;
+    P->setup_id++;
     {
         const int gb = grid_for(c->T, 256);
         const bool mz = c->nz > 1;

@@ -592,10 +592,8 @@ Predictor* predictor_get(fvm_ctx* c) {
         p->ypg.alloc(c->N);
         p->Fg.alloc(c->N);
         c->pred = p;
-        FVM_CUDA(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)mlp_smem_bytes(false)));
-        FVM_CUDA(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)mlp_smem_bytes(true)));
+        raise_smem_limit(k_mlp_forward, mlp_smem_bytes(false));
+        raise_smem_limit(k_mlp_train, mlp_smem_bytes(true));
     }
     return c->pred;
 }

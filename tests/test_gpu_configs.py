@@ -8,7 +8,9 @@ sizes (through the C ABI).
 * The 2D problem as configured (81 x 41 nodes, 1 day, GMRES(30)):
   adaptive runs in FP64 and FP32 against the oracle's adaptive run, then the
   step-sequence replay: the GPU's accepted steps replayed by the GPU (FP64
-  and FP32 preconditioner and basis) and by the oracle's independent
+  and FP32 preconditioner and basis, and the FP32 path whose Krylov operator
+  is the assembled Jacobian in one fused launch per GMRES cycle) and by the
+  oracle's independent
   Lagrange-form BDF step, every corrector solved to ||delta||_wrms <= 1e-5
   (about 1e-11 m on these heads).  With the step sizes and orders fixed,
   the states must agree to 1e-10 relative, the FP32 path included: it keeps
@@ -26,6 +28,10 @@ from oracle.pyoracle import Oracle, factor_given
 pytestmark = pytest.mark.gpu
 
 REPLAY_TOL = 1e-10   # max |h_gpu - h_oracle| / max |h_oracle| after a replay
+# the GPU paths: plain FP64, FP32 factor and basis, and the FP32 path whose
+# Krylov operator is the assembled Jacobian (fused cycle)
+PATHS = {"fp64": dict(precision=0), "fp32": dict(precision=1),
+         "fp32_assembled": dict(precision=1, krylov_operator=1)}
 
 
 def T(x, dev):
@@ -126,32 +132,32 @@ def test_plane_one_day_adaptive_and_replay(plane, cuda):
     p, ph, orc, y0 = plane
     day = 86400.0
     ends, traces = {}, {}
-    for prec in (0, 1):
-        integ = fb.Integrator(ph, krylov_dim=30, max_order=5, precision=prec)
+    for key, kw in PATHS.items():
+        integ = fb.Integrator(ph, krylov_dim=30, max_order=5, **kw)
         ye = torch.empty_like(y0)
         rc, st = integ.integrate(0.0, day, y0, ye)
-        assert rc == 0 and abs(st["t"] - day) < 1e-6, st
-        ends[prec], traces[prec] = ye.cpu().numpy(), integ.trace()
+        assert rc == 0 and abs(st["t"] - day) < 1e-6, (key, st)
+        ends[key], traces[key] = ye.cpu().numpy(), integ.trace()
     nb = fb.Preconditioner(ph).info()["nblocks"]   # the partition the runs used
     y0h = y0.cpu().numpy()
     rc, yo, st_o = orc.integrate(fb.default_opts(krylov_dim=30, max_order=5), nb, 0.0, day, y0h)
     assert rc == 0, st_o
     span = np.abs(yo).max()
     # adaptive runs: each meets rtol = atol = 1e-6 on its own step sequence
-    for prec in (0, 1):
-        assert np.abs(ends[prec] - yo).max() < 1e-4 * span, (prec, np.abs(ends[prec] - yo).max())
+    for key in PATHS:
+        assert np.abs(ends[key] - yo).max() < 1e-4 * span, (key, np.abs(ends[key] - yo).max())
     # replay of the FP64 run's steps with tight correctors
-    tr = traces[0]
+    tr = traces["fp64"]
     h0 = float(tr["h"][0])
     rc, yr, st_r = orc.replay(fb.default_opts(krylov_dim=30, max_order=5), nb, 0.0, y0h, h0, tr, newton_tol=1e-5)
     assert rc == 0
-    for prec in (0, 1):
-        integ = fb.Integrator(ph, krylov_dim=30, max_order=5, precision=prec)
+    for key, kw in PATHS.items():
+        integ = fb.Integrator(ph, krylov_dim=30, max_order=5, **kw)
         yg = torch.empty_like(y0)
         rc, st = integ.replay(0.0, y0, h0, tr, yg, newton_tol=1e-5)
         assert rc == 0 and st["nst"] == len(tr)
         err = np.abs(yg.cpu().numpy() - yr).max() / np.abs(yr).max()
-        assert err <= REPLAY_TOL, (prec, err)
+        assert err <= REPLAY_TOL, (key, err)
 
 
 def test_box_first_steps_replay(box, cuda):
@@ -168,10 +174,10 @@ def test_box_first_steps_replay(box, cuda):
     y0h = y0.cpu().numpy()
     rc, yr, _ = orc.replay(fb.default_opts(krylov_dim=40, max_order=5), nb, 0.0, y0h, h0, tr, newton_tol=1e-5)
     assert rc == 0
-    for prec in (0, 1):
-        rep = fb.Integrator(ph, krylov_dim=40, max_order=5, precision=prec)
+    for key, kw in PATHS.items():
+        rep = fb.Integrator(ph, krylov_dim=40, max_order=5, **kw)
         yg = torch.empty_like(y0)
         rc, st = rep.replay(0.0, y0, h0, tr, yg, newton_tol=1e-5)
         assert rc == 0
         err = np.abs(yg.cpu().numpy() - yr).max() / np.abs(yr).max()
-        assert err <= REPLAY_TOL, (prec, err)
+        assert err <= REPLAY_TOL, (key, err)

@@ -256,6 +256,35 @@ def test_psolve_parity_blocks_per_sm(per_sm, cuda):
     assert err < 1e-10, (per_sm, err)
 
 
+def test_two_live_contexts_of_different_sizes(cuda):
+    """kernel launch limits (dynamic shared memory) belong to the kernel for
+    the whole process: a small context created after a large one must not
+    lower the limits the large one's preconditioner applies need"""
+    big = fb.make_problem("richards3d", nx=36, ny=36, nz=30, Lx=36.0, Ly=36.0, Lz=30.0)
+    small = fb.make_problem("richards2d", nx=21, ny=11)
+    out = {}
+    phs = [fb.Physics(big), fb.Physics(small)]
+    pcs = []
+    for ph, p in zip(phs, (big, small)):
+        y, yp = state(p, 6)
+        yt, ypt = T(y, cuda), T(yp, cuda)
+        ph.begin_step(0.0, yt, ypt)
+        F0 = torch.empty_like(yt)
+        ph.residual(0.0, yt, ypt, F0)
+        ewt = T(1.0 / (1e-6 * np.abs(y) + 1e-6), cuda)
+        pcs.append((fb.Preconditioner(ph), yt, ypt, F0, ewt))
+    for prec in (0, 1):
+        for k, (pc, yt, ypt, F0, ewt) in enumerate(pcs):   # large set up first, then small
+            assert pc.setup(0.0, 1e-2, 100.0, yt, ypt, F0, ewt, prec) == 0
+        for k, (pc, yt, ypt, F0, ewt) in enumerate(pcs):
+            z = torch.empty_like(yt)
+            pc.apply(torch.ones_like(yt), z)   # raised on the large context before
+            out[(k, prec)] = z.abs().max().item()
+    assert all(np.isfinite(v) and v > 0 for v in out.values()), out
+    for ph in phs:
+        ph.close()
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_gmres_converges_and_matches_oracle(case, precision, cuda):
     name, p = case
