@@ -47,6 +47,9 @@ sys.path.insert(0, HERE)
 
 METRIC = "sim-s/wall-s, 200k-node 3D Richards @1e-6: learned+FP32 vs plain FP64, 1×B200"
 WORKLOAD = "richards3d 101x101x21 nodes / 1.2M tets (214,221 nodes), one 30-day run per step"
+# the workload both arms time: the same dict in the line of each
+CONFIG = {"workload": WORKLOAD, "rtol": 1e-6, "atol": 1e-6, "simulated_s_per_step": 30 * 86400.0,
+          "l2": "inputs larger than L2 (331 MB per residual evaluation)"}
 # DRAM bytes (read + write) of one residual evaluation of this workload --
 # node pass 8.3 MB, element pass 62.6 MB, gather 13.1 MB -- as measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the --profile-case
@@ -235,13 +238,15 @@ def train_predictor(fb, torch, dev, seed, horizon):
     return P, info
 
 
-def profile_case(name):
+def profile_case(name, days=10.0):
     """Small fixed workloads of single kernels for profiler captures (not a
     bench line): 'residual' evaluates the residual five times at the
     hydrostatic head; 'precond' sets up the FP32 preconditioner three times
     and applies it 20 times after each set-up; 'krylov' integrates the first
     10 days with the FP32 Krylov path (about 120 steps, 16 Krylov iterations
-    per Newton solve by the end)."""
+    per Newton solve by the end); 'fused' integrates the first --days days
+    with the FP32 assembled Krylov operator (one fused launch per GMRES
+    cycle)."""
     import torch
 
     import fvmpor_b200 as fb
@@ -268,9 +273,13 @@ def profile_case(name):
             pc.setup(0.0, 1e-2, 100.0, y, yp, r, ewt, precision=1)
             for _ in range(20):
                 pc.apply(v, z)
-    else:
+    elif name == "krylov":
         ye = torch.empty_like(y)
         fb.Integrator(ph, krylov_dim=40, max_restarts=5, precision=1, max_order=5).integrate(0.0, 10 * 86400.0, y, ye)
+    else:
+        ye = torch.empty_like(y)
+        fb.Integrator(ph, krylov_dim=40, max_restarts=5, precision=1, krylov_operator=1, max_order=5).integrate(
+            0.0, days * 86400.0, y, ye)
     torch.cuda.synchronize()
     print(json.dumps({"profile_case": name, "ok": True}))
 
@@ -307,7 +316,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(walls) / len(walls),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded 3D jittered Kuhn mesh, lognormal Ks)",
-        "config": {"workload": WORKLOAD, "rtol": 1e-6, "atol": 1e-6},
+        "config": dict(CONFIG),
         "cpu_baseline": {
             "value": value, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": ("unit costs of the FP64 oracle on the 214,221-node mesh (Newton residual, preconditioner "
@@ -334,13 +343,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replay-steps", type=int, default=8,
                     help="steps of the headline run replayed against the CPU oracle for error_vs_oracle")
-    ap.add_argument("--profile-case", choices=["residual", "precond", "krylov"],
+    ap.add_argument("--profile-case", choices=["residual", "precond", "krylov", "fused"],
                     help="run one small fixed workload for a profiler capture instead of the bench")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.profile_case:
-        profile_case(args.profile_case)
+        profile_case(args.profile_case, args.days)
         return
     if args.impl == "reference":
         run_reference(args)
@@ -473,13 +482,13 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_learn / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded 3D jittered Kuhn mesh, lognormal Ks by FFT)",
-        "config": {"workload": f"richards3d {N} nodes / {T} tets, {args.days:g}-day run per step",
-                   "path": "learned Newton iterate (per-node MLP, BF16 weights / FP32 accumulation on tcgen05) + "
-                           "FP32 block-ILU(0), FP32 GMRES(40) basis and FP32 assembled Krylov operator (the "
-                           "set-up's difference-quotient Jacobian, one fused launch per GMRES cycle); FP64 "
-                           "residual, Newton update, least squares and tests",
-                   "rtol": 1e-6, "atol": 1e-6, "l2": "inputs larger than L2 (331 MB per residual)",
-                   "parallelism": f"replicas x{ws}"},
+        "config": dict(CONFIG) if args.days == 30.0 else dict(CONFIG, workload=WORKLOAD.replace(
+            "30-day", f"{args.days:g}-day"), simulated_s_per_step=horizon),
+        "path": "learned Newton iterate (per-node MLP, BF16 weights / FP32 accumulation on tcgen05) + "
+                "FP32 block-ILU(0), FP32 GMRES(40) basis and FP32 assembled Krylov operator (the "
+                "set-up's difference-quotient Jacobian, one fused launch per GMRES cycle); FP64 "
+                "residual, Newton update, least squares and tests",
+        "parallelism": f"replicas x{ws}",
         "comparison_paths": cmp,
         "learned_predictor": dict(train_info, accepted_steps=st0["npred"]),
         "final_head_rel_diff_vs_plain_fp64": head_diff,

@@ -779,6 +779,9 @@ CONFIGS = {
     "richards3d": Config("richards3d: 100x100x20 hex -> 6 tets (214,221 nodes), lognormal Ks, 30 days", "3d",
                          dict(nx=100, ny=100, nz=20, Lx=100.0, Ly=100.0, Lz=20.0, jitter=0.15, seed=1,
                               ln_var=1.0, cx=10.0, cy=10.0, cz=2.0, Kg=1e-5)),
+    "richards3d_1m": Config("richards3d_1m: 200x200x25 hex -> 6 tets (1,050,426 nodes), the 3D statistics", "3d",
+                            dict(nx=200, ny=200, nz=25, Lx=200.0, Ly=200.0, Lz=25.0, jitter=0.15, seed=1,
+                                 ln_var=1.0, cx=10.0, cy=10.0, cz=2.0, Kg=1e-5)),
 }
 
 

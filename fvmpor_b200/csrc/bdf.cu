@@ -496,6 +496,7 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
     bo.max_order = o.max_order;
     bo.hmax = o.hmax;
     bo.use_guess = o.use_predictor != 0;
+    bo.guess_every_step = o.use_predictor == 2;
     if (o.eps_lin > 0.0) bo.eps_lin = o.eps_lin;
     if (o.cj_refresh > 1.0) bo.cj_refresh = o.cj_refresh;
     if (o.psetup_age > 0) bo.psetup_age = o.psetup_age;

@@ -60,6 +60,9 @@ struct BdfOptions {
     int max_order = 5;
     double hmax = 0.0;
     bool use_guess = false;
+    // try the learned iterate on every step (true), not only on the retry
+    // after a failed corrector
+    bool guess_every_step = false;
     // Krylov tolerance factor (IDA's epslin).  IDA's default 0.05 assumes a
     // preconditioner close to J -- the reference's is an exact direct
     // factorisation (preconditioner_dss.cpp:284-405), so its Krylov solves
@@ -198,7 +201,10 @@ template <class Ops> struct BdfController {
             // spends 20-30 Krylov iterations removing them (30-day 3D run:
             // 4 accepted guesses in the first 2 h raised the run from 221
             // to 256 steps and from 5.2k to 6.4k Krylov iterations).
-            if (o.use_guess && ncf > 0 && ops.newton_guess(tnew, h, cj)) { st.npred++; guessed = true; }
+            if (o.use_guess && (ncf > 0 || o.guess_every_step) && ops.newton_guess(tnew, h, cj)) {
+                st.npred++;
+                guessed = true;
+            }
             bool converged = false, fresh_p = false;
             // refresh the preconditioner on the first step, when cj has moved
             // by more than cj_refresh since the last factorisation, after

@@ -270,7 +270,9 @@ typedef struct {
     int krylov_dim;          /* GMRES(m)                                   */
     int max_restarts;
     int precision;           /* 0 = FP64, 1 = FP32 factor/apply + basis    */
-    int use_predictor;       /* learned Newton initial iterate (fvm_mlp_*) */
+    int use_predictor;       /* learned Newton initial iterate (fvm_mlp_*):
+                                0 off, 1 on the retry after a failed
+                                corrector, 2 on every step             */
     double h0;               /* first step, 0 = automatic                  */
     double hmax;             /* 0 = unbounded                              */
     long max_steps;
