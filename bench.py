@@ -56,6 +56,12 @@ CONFIG = {"workload": WORKLOAD, "rtol": 1e-6, "atol": 1e-6, "simulated_s_per_ste
 # residual workload.  The algorithmic 331.7 MB assume stored face
 # coefficients; the rebuilt-geometry element pass reads a fifth of that.
 CHAIN_DRAM_BYTES = 84.0e6
+# DRAM bytes (read + write) of one k_arnoldi_fused launch, as measured by ncu
+# on the --profile-case fused workload (launch 101 of the 10-day run, about
+# 30 Arnoldi steps: 44.0 MB read, 1.6 MB written).  The operator and the FP32
+# basis stay in L2 between steps, so this stays far below the algorithmic
+# bytes, which count every L2 -> SM pass.
+FUSED_DRAM_BYTES = 45.6e6
 UNIT = "sim-s/wall-s"
 
 
@@ -333,6 +339,94 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# the other benchmark configurations (not the headline line): generator
+# name, horizon, Krylov dimension, simulated-time multiplier (ensemble
+# members), and the paths timed (the first is the line's value)
+WORKLOADS = {
+    "plane": dict(problem="richards2d", days=1.0, m=30, desc="richards2d 81x41 jittered Delaunay (3,321 nodes), "
+                  "2 layers, ponded strip, 1 day, GMRES(30), rtol = atol = 1e-6",
+                  paths={"plain_fp64": dict(precision=0), "fp32_jacobian_free": dict(precision=1),
+                         "fp32_assembled": dict(precision=1, krylov_operator=1)}),
+    "ensemble": dict(problem="ensemble2d", days=1.0, m=30, desc="ensemble2d: 256 independent 2D meshes of "
+                     "2k-40k nodes (5.37 M nodes), own lognormal Ks, 1 day, FP64 residual + FP32 preconditioner",
+                     paths={"fp32_jacobian_free": dict(precision=1), "fp32_assembled": dict(precision=1, krylov_operator=1)}),
+    "box1m": dict(problem="richards3d_1m", days=30.0, m=40, desc="richards3d_1m: 200x200x25 hex -> 6 tets "
+                  "(1,050,426 nodes), lognormal Ks, 30 days, GMRES(40)",
+                  paths={"fp32_assembled": dict(precision=1, krylov_operator=1),
+                         "fp32_jacobian_free": dict(precision=1), "plain_fp64": dict(precision=0)}),
+}
+
+
+def run_workload(args):
+    """one of the other configurations at its stated size (1 GPU): every
+    path of WORKLOADS[name] timed run by run, alternating, after one warm-up
+    run each; value = the first path's simulated seconds (times the
+    ensemble's members) per wall second of its median run"""
+    import torch
+
+    import fvmpor_b200 as fb
+
+    wl = WORKLOADS[args.workload]
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    t = time.perf_counter()
+    prob = fb.make_problem(wl["problem"])
+    gen_s = time.perf_counter() - t
+    t = time.perf_counter()
+    ph = fb.Physics(prob)
+    torch.cuda.synchronize()
+    create_s = time.perf_counter() - t
+    members = len(prob.member_ptr) - 1 if prob.member_ptr is not None else 1
+    horizon = wl["days"] * 86400.0
+    y0 = torch.empty(prob.n_nodes, dtype=torch.float64, device=dev)
+    ph.initial_head(y0)
+    ye = torch.empty_like(y0)
+    integ = {k: fb.Integrator(ph, krylov_dim=wl["m"], max_restarts=5, max_order=5, **kw)
+             for k, kw in wl["paths"].items()}
+    for it in integ.values():
+        rc, _ = it.integrate(0.0, horizon, y0, ye)
+        if rc != 0:
+            raise RuntimeError(f"warm-up run failed rc={rc}")
+    runs = {k: [] for k in integ}
+    stats = {}
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            for k, it in integ.items():
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                rc, st = it.integrate(0.0, horizon, y0, ye)
+                e1.record()
+                torch.cuda.synchronize()
+                if rc != 0:
+                    raise RuntimeError(f"{k} failed rc={rc} {st}")
+                runs[k].append(e0.elapsed_time(e1))
+                stats[k] = {q: st[q] for q in ("nst", "nni", "nli", "npe", "nre", "ncfn", "netf", "nsync")}
+    head = next(iter(integ))
+    cmp = {k: {"value": members * horizon / (float(np.median(v)) / 1e3), "ms_per_run": float(np.median(v)),
+               "ms_each_run": v, "stats": stats[k],
+               "host_waits_per_step": stats[k]["nsync"] / max(stats[k]["nst"], 1)} for k, v in runs.items()}
+    y0h = y0.cpu().numpy()
+    yh = np.zeros(prob.n_nodes)
+    t = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        integ[head].integrate_host(0.0, horizon, y0h, yh)
+    e2e_s = (time.perf_counter() - t) / max(1, args.steps // 2)
+    line = {"metric": f"sim-s/wall-s, {wl['desc']}, 1xB200", "value": cmp[head]["value"], "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": cmp[head]["ms_per_run"],
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded meshes and Ks fields)",
+            "config": {"workload": wl["desc"], "members": members, "nodes": prob.n_nodes,
+                       "elements": prob.n_elements, "simulated_s_per_member": horizon},
+            "path": head, "paths": cmp,
+            "preprocessing_s": {"generate": gen_s, "create_context": create_s},
+            "preconditioner": fb.Preconditioner(ph).info(),
+            "e2e": {"value": members * horizon / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * prob.n_nodes,
+                    "d2h_bytes_per_step": 8 * prob.n_nodes},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    ph.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,9 +439,15 @@ def main():
                     help="steps of the headline run replayed against the CPU oracle for error_vs_oracle")
     ap.add_argument("--profile-case", choices=["residual", "precond", "krylov", "fused"],
                     help="run one small fixed workload for a profiler capture instead of the bench")
+    ap.add_argument("--workload", default="richards3d", choices=["richards3d"] + sorted(WORKLOADS),
+                    help="richards3d: the headline line; plane, ensemble, box1m: the other configurations at their "
+                         "stated sizes (1 GPU)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload != "richards3d" and args.impl == "ours" and not args.profile_case:
+        run_workload(args)
+        return
     if args.profile_case:
         profile_case(args.profile_case, args.days)
         return
@@ -495,7 +595,7 @@ def main():
         "stats": {k: st0[k] for k in ("nst", "nni", "nli", "npe", "nps", "nre", "ncfn", "netf", "npred",
                                       "last_order")},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": FUSED_DRAM_BYTES,
                      "kernel": "k_arnoldi_fused (one GMRES cycle: assembled operator, block-ILU(0) sweeps, CGS2, "
                                "Givens)",
                      "algorithmic_bytes_per_launch": bytes_steps / launches_k,

@@ -116,7 +116,7 @@ class Stats(C.Structure):
     _fields_ = [("nst", C.c_long), ("nre", C.c_long), ("nni", C.c_long), ("nli", C.c_long),
                 ("npe", C.c_long), ("nps", C.c_long), ("ncfn", C.c_long), ("ncfl", C.c_long),
                 ("netf", C.c_long), ("npred", C.c_long), ("last_order", C.c_int),
-                ("last_h", C.c_double), ("t", C.c_double)]
+                ("last_h", C.c_double), ("t", C.c_double), ("nsync", C.c_long)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -179,6 +179,8 @@ def _declare(L):
     L.fvm_set_element_pass.argtypes = [_P, _I, _I]
     L.fvm_element_pass.argtypes = [_P, C.POINTER(_I), C.POINTER(_I)]
     L.fvm_set_precond_blocks.argtypes = [_P, _I]
+    L.fvm_set_precond_schur.argtypes = [_P, _I]
+    L.fvm_precond_schur_info.argtypes = [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]
     L.fvm_mlp_nparams.restype = _I
     L.fvm_mlp_set_params.argtypes = [_P, _P]
     L.fvm_mlp_get_params.argtypes = [_P, _P]
@@ -487,6 +489,17 @@ class Preconditioner:
     def set_blocks_per_sm(self, per_sm):
         """block-ILU blocks per SM on large meshes (drops the current factor)"""
         _check(lib().fvm_set_precond_blocks(self.ph._c, per_sm), "fvm_set_precond_blocks")
+
+    def set_schur(self, iters):
+        """Schur interface coupling of the block ILU(0): iters < 0 off, else
+        the interface sweeps of every apply (drops the current factor)"""
+        _check(lib().fvm_set_precond_schur(self.ph._c, int(iters)), "fvm_set_precond_schur")
+
+    def schur_info(self):
+        a, b, c = _I(), _I(), _I()
+        _check(lib().fvm_precond_schur_info(self.ph._c, C.byref(a), C.byref(b), C.byref(c)),
+               "fvm_precond_schur_info")
+        return {"iters": a.value, "interface_rows": b.value, "fp64": bool(c.value & 1), "fp32": bool(c.value & 2)}
 
     def info(self):
         a, b, c, d = _I(), _I(), _I(), _I()

@@ -349,7 +349,9 @@ __global__ void k_op_refresh(long ne, const int* __restrict__ src, const double*
 // resident at once); the caller then uses the separate kernels.
 bool fused_prepare(fvm_ctx* c, int m) {
     BlockILU* P = c->ilu;
-    if (!P || !P->built || P->factored != 1 || m + 2 > 64) return false;
+    // the cycle inlines the block-Jacobi apply; the Schur-coupled apply
+    // runs as its own cooperative launch between the separate kernels
+    if (!P || !P->built || P->factored != 1 || m + 2 > 64 || P->schur_iters >= 0) return false;
     cudaStream_t s = c->stream;
     if (!P->op_built) {
         P->op_built = true;

@@ -89,6 +89,19 @@ __global__ void k_newton_update(int N, const double* __restrict__ x, double cj,
     last_block_reduce(partial, 1, counter, out);
 }
 
+// out = sum (y ewt)^2: the predictor's squared WRMS norm times N
+__global__ void k_pred_sumsq(int N, const double* __restrict__ y, const double* __restrict__ ewt, double* partial,
+                             unsigned* counter, double* out) {
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double w = y[i] * ewt[i];
+        s += w * w;
+    }
+    double t = block_sum(s);
+    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    last_block_reduce(partial, 1, counter, out);
+}
+
 // squared error-test norms times N:
 //  0: e  1: phi_k + e  2: phi_{k-1} + phi_k + e  3: e - phi_{k+1}
 __global__ void k_err_norms(int N, int k, PhiPtrs ph, const double* __restrict__ e,
@@ -257,7 +270,9 @@ static IntegWork& integ_work(fvm_ctx* c) {
     for (int j = 0; j < kNPhi; ++j) w.phi[j].alloc(N);
     w.y.alloc(N); w.yp.alloc(N); w.e.alloc(N); w.ewt.alloc(N); w.F.alloc(N); w.x.alloc(N); w.tmp.alloc(N);
     w.partial.alloc((size_t)kRedBlocks * 4);
-    const size_t nh = (size_t)std::max(8, 4 * c->n_members);
+    // reduction results: Newton norms [0, nm), error norms [nm, 5 nm), the
+    // predictor's norm at 5 nm (fetched together, one host wait)
+    const size_t nh = (size_t)(5 * std::max(1, c->n_members) + 8);
     w.res.alloc(nh);
     w.counter.alloc(1);
     if (w.host_n < nh) {
@@ -287,6 +302,22 @@ struct DeviceOps {
     bool f_fresh = false;          // F already holds F(t, y, y')
 
     int nm = 1;                    // ensemble members (per-member norms when > 1)
+    // Krylov tolerance factor of an ensemble: GMRES stops on the RMS over
+    // all nodes, so it runs to tol * sqrt(N_min / N), which bounds every
+    // member's own RMS by tol (N_m rms_m^2 <= N rms^2); with the plain
+    // global tolerance the smallest members' Newton updates were up to
+    // sqrt(N / N_min) times less accurate than their own Newton test
+    // needs, and their correctors failed until the step size collapsed
+    double tol_scale = 1.0;
+    // One host wait per Newton iteration: predict() queues the predictor's
+    // norm, newton_update() queues its own norm and, speculatively, the
+    // error norms the step's test needs if this update converges; one fetch
+    // brings all three.  psetup() does not wait for the pivot status either:
+    // gmres() reads it after its own wait.
+    int korder = 1;                // order of the step being solved (set_order)
+    double pn = 0.0;               // WRMS norm of this attempt's predictor
+    bool err_ready = false;        // err_cache holds the norms for (korder, e)
+    double err_cache[4] = {};
 
     DeviceOps(fvm_ctx* ctx, const fvm_opts& opts)
         : c(ctx), o(opts), N(ctx->N), w(integ_work(ctx)), phi(w.phi), y(w.y), yp(w.yp), e(w.e), ewt(w.ewt),
@@ -294,17 +325,24 @@ struct DeviceOps {
           ypred(w.ypred), yppred(w.yppred), hprev(w.hprev), feat(w.feat) {
         for (int j = 0; j < kNPhi; ++j) phi[j].zero(c->stream);
         nm = c->n_members;
+        if (nm > 1) {
+            int nmin = N;
+            for (int m = 0; m < nm; ++m) nmin = std::min(nmin, c->h_member_ptr[m + 1] - c->h_member_ptr[m]);
+            tol_scale = std::sqrt((double)std::max(nmin, 1) / N);
+        }
         counter.zero(c->stream);
     }
-    // largest per-member WRMS norm from per-member squared sums out[m*nq + q]
-    double member_max(int nq, int q) const {
+    // largest per-member WRMS norm from per-member squared sums
+    // host[off + m*nq + q]
+    double member_max_at(size_t off, int nq, int q) const {
         double best = 0.0;
         for (int m = 0; m < nm; ++m) {
             const int nmem = c->h_member_ptr[m + 1] - c->h_member_ptr[m];
-            if (nmem > 0) best = std::max(best, std::sqrt(host[(size_t)m * nq + q] / nmem));
+            if (nmem > 0) best = std::max(best, std::sqrt(host[off + (size_t)m * nq + q] / nmem));
         }
         return best;
     }
+    double member_max(int nq, int q) const { return member_max_at(0, nq, q); }
     int g() const { return grid_for(N, 256); }
     PhiPtrs ptrs() const {
         PhiPtrs p;
@@ -313,9 +351,10 @@ struct DeviceOps {
     }
     double fetch(int n) {
         FVM_CUDA(cudaMemcpyAsync(host, res.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
-        FVM_CUDA(cudaStreamSynchronize(c->stream));
+        ctx_sync(c);
         return host[0];
     }
+    size_t pn_slot() const { return 5 * (size_t)std::max(1, nm); }
 
     // ---- controller interface
     void set_time(double t) { tcur = t; }
@@ -332,6 +371,9 @@ struct DeviceOps {
         Coef7 gm;
         for (int j = 0; j < kNPhi; ++j) gm.v[j] = gamma[j];
         fvm_launch(c, k_predict, g(), 256, 0, c->stream, N, k, ptrs(), gm, y.p, yp.p, e.p);
+        fvm_launch(c, k_pred_sumsq, kRedBlocks, kRedThreads, 0, c->stream, N, y.p, ewt.p, partial.p, counter.p,
+                   res.p + pn_slot());
+        err_ready = false;
         f_fresh = false;
         hcur = h;
         if (pred || rec) {
@@ -341,7 +383,10 @@ struct DeviceOps {
             predictor_features(c, phi[0].p, hprev.p, ypred.p, h, feat.p);
         }
     }
-    double wrms_y() { return std::sqrt(reduce_sumsq(c, y.p, ewt.p) / N); }
+    // the predictor's WRMS norm, as fetched by the attempt's first
+    // newton_update (the only place the controller reads it)
+    double pred_norm() const { return pn; }
+    void set_order(int k) { korder = k; err_ready = false; }
     void residual() {
         if (f_fresh) {   // the learned-iterate check already evaluated it
             f_fresh = false;
@@ -360,30 +405,49 @@ struct DeviceOps {
             feat.alloc((size_t)N * 8);
         }
     }
+    // the pivot status is copied behind the factorisation and read by
+    // gmres() after its wait (status 3 there)
     int psetup(double cj, double h) {
         psetup_dev(c, cj, h, y.p, yp.p, F.p, ewt.p, o.precision);
-        return ilu_status(c);
+        return 0;
     }
     int gmres(double cj, double tol, int* its, double* rn, long* nps, long* njv) {
         GmresCounters gc;
         int r = gmres_dev(c, cj, y.p, yp.p, F.p, ewt.p, F.p, x.p, o.krylov_dim, o.max_restarts,
-                          o.precision, tol, its, rn, &gc, o.krylov_operator);
+                          o.precision, tol * tol_scale, its, rn, &gc, o.krylov_operator);
         *nps = gc.nps;
         *njv = gc.njv;
+        if (ilu_status_seen(c)) return 3;   // zero pivot in the factor this solve used
         return r;
     }
     double newton_update(double cj) {
+        const size_t ps = pn_slot();
         if (nm > 1) {
             fvm_launch(c, k_newton_update_seg, nm, 256, 0, c->stream, c->member_ptr.p, x.p, cj, ewt.p, y.p, yp.p,
                        e.p, res.p);
-            fetch(nm);
+            fvm_launch(c, k_err_norms_seg, nm, 256, 0, c->stream, c->member_ptr.p, korder, ptrs(), e.p, ewt.p,
+                       res.p + nm);
+            fetch((int)ps + 1);
+            for (int q = 0; q < 4; ++q) err_cache[q] = member_max_at(nm, 4, q);
+            err_ready = true;
+            pn = std::sqrt(host[ps] / N);
             return member_max(1, 0);
         }
         fvm_launch(c, k_newton_update, kRedBlocks, kRedThreads, 0, c->stream, N, x.p, cj, ewt.p, y.p, yp.p, e.p,
                                                                    partial.p, counter.p, res.p);
-        return std::sqrt(fetch(1) / N);
+        fvm_launch(c, k_err_norms, kRedBlocks, kRedThreads, 0, c->stream, N, korder, ptrs(), e.p, ewt.p, partial.p,
+                                                               counter.p, res.p + 1);
+        const double d = fetch((int)ps + 1);
+        for (int q = 0; q < 4; ++q) err_cache[q] = std::sqrt(host[1 + q] / N);
+        err_ready = true;
+        pn = std::sqrt(host[ps] / N);
+        return std::sqrt(d / N);
     }
     void err_norms(int k, double out[4]) {
+        if (err_ready && k == korder) {
+            for (int q = 0; q < 4; ++q) out[q] = err_cache[q];
+            return;
+        }
         if (nm > 1) {
             fvm_launch(c, k_err_norms_seg, nm, 256, 0, c->stream, c->member_ptr.p, k, ptrs(), e.p, ewt.p, res.p);
             fetch(4 * nm);
@@ -482,6 +546,7 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
     if (o.max_order < 1 || o.max_order > 5) throw Error("integrate: max_order must be 1..5");
     if (!(o.rtol > 0) || !(o.atol > 0)) throw Error("integrate: tolerances must be positive");
     if (!(t_end > t0)) throw Error("integrate: t_end must exceed t0");
+    const long nsync0 = c->n_syncs;
     c->last_trace.clear();
     DeviceOps ops(c, o);
     Predictor* pred = nullptr;
@@ -524,7 +589,7 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
     }
     if (y_end)
         FVM_CUDA(cudaMemcpyAsync(y_end, ops.phi[0].p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
-    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    ctx_sync(c);
     c->last_trace.swap(ctl.trace);
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
@@ -541,6 +606,7 @@ int integrate_dev(fvm_ctx* c, const fvm_opts* opts, double t0, double t_end, con
         stats->last_order = ctl.st.last_order;
         stats->last_h = ctl.st.last_h;
         stats->t = ctl.t;
+        stats->nsync = c->n_syncs - nsync0;
     }
     return rc;
 }
@@ -564,14 +630,24 @@ int replay_dev(fvm_ctx* c, const fvm_opts* opts, double t0, const double* y0, do
     }
     o.h0 = h0;      // the first-step rule returns the given h0
     o.hmax = 0.0;
-    o.use_predictor = 0;
+    const long nsync0 = c->n_syncs;
     c->last_trace.clear();
     DeviceOps ops(c, o);
-    ops.enable_learning(nullptr, nullptr);
+    // with use_predictor every replayed step first tries the learned iterate
+    // (kept when its residual test passes), so that two replays of one step
+    // sequence, with and without it, measure the Newton and Krylov work it
+    // saves at the same corrector tolerance
+    Predictor* pred = nullptr;
+    if (o.use_predictor) {
+        pred = predictor_of(c);
+        if (!pred) throw Error("replay: use_predictor set but no trained predictor loaded");
+    }
+    ops.enable_learning(pred, nullptr);
     BdfOptions bo;
     bo.rtol = o.rtol;
     bo.atol = o.atol;
     bo.max_order = o.max_order;
+    bo.use_guess = pred != nullptr;
     BdfController<DeviceOps> ctl(ops, bo);
     const long nre0 = c->n_residuals;
     const double hs = ops.start(t0, y0, t0 + h0);
@@ -584,7 +660,7 @@ int replay_dev(fvm_ctx* c, const fvm_opts* opts, double t0, const double* y0, do
     }
     if (y_end)
         FVM_CUDA(cudaMemcpyAsync(y_end, ops.phi[0].p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
-    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    ctx_sync(c);
     c->last_trace.swap(ctl.trace);
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
@@ -594,9 +670,11 @@ int replay_dev(fvm_ctx* c, const fvm_opts* opts, double t0, const double* y0, do
         stats->nli = ctl.st.nli;
         stats->npe = ctl.st.npe;
         stats->nps = ctl.st.nps;
+        stats->npred = ctl.st.npred;
         stats->last_order = ctl.st.last_order;
         stats->last_h = ctl.st.last_h;
         stats->t = ctl.t;
+        stats->nsync = c->n_syncs - nsync0;
     }
     return rc;
 }
@@ -700,7 +778,7 @@ extern "C" int fvm_integrate_host(fvm_ctx* c, const fvm_opts* opts, double t0, d
         FVM_CUDA(cudaMemcpyAsync(a.p, y0_host, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
         int rc = integrate_dev(c, opts, t0, t_end, a.p, b.p, stats);
         FVM_CUDA(cudaMemcpyAsync(y_end_host, b.p, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
-        FVM_CUDA(cudaStreamSynchronize(c->stream));
+        ctx_sync(c);
         if (rc < 0) set_error("fvm_integrate_host: step failure code " + std::to_string(rc));
         return rc;
     } catch (const Error& ex) {

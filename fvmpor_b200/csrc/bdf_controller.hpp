@@ -25,12 +25,17 @@
 //   void   begin_step();                     // freeze upwinding at (phi_0, y')
 //   void   phi_scale(int j0, int j1, const double* f);   // phi_j *= f[j]
 //   void   predict(int k, const double* gamma, double h); // y, y' ; e = 0
-//   double wrms_y();
+//   double pred_norm();                      // ||y||_wrms of the last predict,
+//                                            // read after the first newton_update
+//   void   set_order(int k);                 // order of the corrector being solved
 //   void   residual();                       // F = F(t, y, y')
 //   int    psetup(double cj, double h);      // 0 ok, else zero pivot
 //   int    gmres(double cj, double tol, int* its, double* rn, long* nps,
 //                long* njv);                 // J x = F; 0 ok, 1 not converged,
-//                                            // 2 breakdown / non-finite
+//                                            // 2 breakdown / non-finite, 3 zero
+//                                            // pivot in the set-up it used (an Ops
+//                                            // whose psetup does not wait reports
+//                                            // the set-up's status here)
 //   double newton_update(double cj);         // y -= x, y' -= cj x, e -= x;
 //                                            // returns ||x||_wrms
 //   void   err_norms(int k, double out[4]);  // see below
@@ -189,7 +194,7 @@ template <class Ops> struct BdfController {
             if (k >= ns) ops.phi_scale(ns, k, beta);
             double tnew = t + h;
             ops.predict(k, gamma, h);
-            double pnorm = ops.wrms_y();
+            ops.set_order(k);
             bool guessed = false;
             ++attempts;
             // The learned iterate is tried only on a retry after a failed
@@ -245,13 +250,14 @@ template <class Ops> struct BdfController {
                     long nps = 0, njv = 0;
                     int lr = ops.gmres(cj, o.eps_lin * epcon, &its, &rn, &nps, &njv);
                     st.nli += its; st.nps += nps; st.njv += njv; st.nni++;
+                    if (lr == 3) return -3;
                     if (lr != 0) st.ncfl++;
                     if (lr == 2) break;
                     double delnrm = ops.newton_update(cj);
                     if (!std::isfinite(delnrm)) break;
                     if (m == 0) {
                         oldnrm = delnrm;
-                        if (delnrm <= 100.0 * uround * pnorm) { converged = true; break; }
+                        if (delnrm <= 100.0 * uround * ops.pred_norm()) { converged = true; break; }
                     } else {
                         double rate = std::pow(delnrm / oldnrm, 1.0 / m);
                         if (rate > 0.9) break;
@@ -386,8 +392,11 @@ template <class Ops> int bdf_replay_step(BdfController<Ops>& c, double hh, int k
     if (k >= c.ns) ops.phi_scale(c.ns, k, c.beta);
     const double tnew = c.t + h;
     ops.predict(k, c.gamma, h);
+    ops.set_order(k);
     ops.set_time(tnew);
     const long nni0 = c.st.nni, nli0 = c.st.nli;
+    const bool guessed = c.o.use_guess && ops.newton_guess(tnew, h, c.cj);
+    if (guessed) c.st.npred++;
     bool conv = false;
     for (int m = 0; m < max_newton; ++m) {
         ops.residual();
@@ -400,6 +409,7 @@ template <class Ops> int bdf_replay_step(BdfController<Ops>& c, double hh, int k
         long nps = 0, njv = 0;
         int lr = ops.gmres(c.cj, 0.05 * newton_tol, &its, &rn, &nps, &njv);
         c.st.nli += its; c.st.nps += nps; c.st.njv += njv; c.st.nni++;
+        if (lr == 3) return -3;
         if (lr == 2) return -7;
         const double d = ops.newton_update(c.cj);
         if (!std::isfinite(d)) return -7;
@@ -413,6 +423,7 @@ template <class Ops> int bdf_replay_step(BdfController<Ops>& c, double hh, int k
     fvm_step_record rec = {};
     rec.t = c.t; rec.h = h; rec.order = k; rec.attempts = 1;
     rec.nni = (int)(c.st.nni - nni0); rec.nli = (int)(c.st.nli - nli0); rec.npe = 1;
+    rec.learned = guessed ? 1 : 0;
     rec.wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - c.wall0).count();
     c.trace.push_back(rec);
     ops.phi_update(k, k + 1 < c.kMaxOrd + 2 ? 1 : 0);

@@ -815,16 +815,46 @@ static void build(fvm_ctx* c, const fvm_mesh* m, const fvm_physics* ph, int flag
 
     // ---- global edges: sort (min,max) keys; first encounter fixes the
     // orientation (Edge(front = node a, back = node b), mesh.cpp:383-441)
+    // The faces in (key, face id) order, built as a counting sort on the
+    // smaller node (faces enter their bucket in ascending face id) followed
+    // by a stable insertion sort on the larger node inside each bucket
+    // (about 35 faces per bucket on a tetrahedral mesh): linear in the
+    // faces, where one global sort of the 36 M keys of the 1M-node mesh took
+    // seconds.
     std::vector<std::pair<uint64_t, int>> keys((size_t)T * nfe);
-    for (int e = 0; e < T; ++e)
-        for (int f = 0; f < nfe; ++f) {
+    {
+        auto ends = [&](int e, int f, int& a, int& b) {
             const int* v = m->elem_nodes + (size_t)e * npe;
-            int a = v[dim == 3 ? tet_edge_a(f) : tri_edge_a(f)];
-            int b = v[dim == 3 ? tet_edge_b(f) : tri_edge_b(f)];
-            uint64_t key = ((uint64_t)(uint32_t)std::min(a, b) << 32) | (uint32_t)std::max(a, b);
-            keys[(size_t)e * nfe + f] = {key, e * nfe + f};
-        }
-    std::sort(keys.begin(), keys.end());
+            a = v[dim == 3 ? tet_edge_a(f) : tri_edge_a(f)];
+            b = v[dim == 3 ? tet_edge_b(f) : tri_edge_b(f)];
+        };
+        std::vector<size_t> bptr((size_t)N + 1, 0);
+        for (int e = 0; e < T; ++e)
+            for (int f = 0; f < nfe; ++f) {
+                int a, b;
+                ends(e, f, a, b);
+                bptr[(size_t)std::min(a, b) + 1]++;
+            }
+        for (int i = 0; i < N; ++i) bptr[i + 1] += bptr[i];
+        std::vector<size_t> fill(bptr.begin(), bptr.end() - 1);
+        for (int e = 0; e < T; ++e)
+            for (int f = 0; f < nfe; ++f) {
+                int a, b;
+                ends(e, f, a, b);
+                const uint64_t key = ((uint64_t)(uint32_t)std::min(a, b) << 32) | (uint32_t)std::max(a, b);
+                keys[fill[std::min(a, b)]++] = {key, e * nfe + f};
+            }
+        for (int i = 0; i < N; ++i)
+            for (size_t r = bptr[i] + 1; r < bptr[i + 1]; ++r) {
+                const auto kv = keys[r];
+                size_t q = r;
+                while (q > bptr[i] && keys[q - 1].first > kv.first) {
+                    keys[q] = keys[q - 1];
+                    --q;
+                }
+                keys[q] = kv;
+            }
+    }
     std::vector<int> edge_ptr(1, 0), edge_face;
     std::vector<double> edge_w;
     std::vector<unsigned char> flip(T, 0);

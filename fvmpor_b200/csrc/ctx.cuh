@@ -230,7 +230,8 @@ struct fvm_ctx {
     fvmb::DevBuf<float> statf;       // [3][N] static node features: mean ln K, elevation,
                                      // CV surface area (learned predictor inputs)
 
-    int ilu_per_sm = 1;              // block-ILU blocks per SM on large meshes
+    int ilu_per_sm = 0;              // block-ILU blocks per SM on large meshes, 0 = automatic
+    int schur_iters = -1;            // Schur interface coupling: < 0 off, else sweeps per apply
     // ensemble of independent members (disjoint node ranges): the integrator's
     // error and Newton tests take the largest per-member WRMS norm
     int n_members = 1;
@@ -244,6 +245,7 @@ struct fvm_ctx {
 
     long n_residuals = 0;
     long launches = 0;               // kernels launched on this context
+    long n_syncs = 0;                // host waits on the context's stream (ctx_sync)
     fvmb::KernelTimer tm;
     std::string err;
 };
@@ -285,6 +287,12 @@ inline void fvm_launch_pdl(fvm_ctx* c, void (*k)(KArgs...), dim3 grid, dim3 bloc
 // first statement of a kernel launched by fvm_launch_pdl: wait for the
 // previous kernel's completion (a no-op after an ordinary launch), then let
 // the next programmatic launch begin
+// the host waits for the context's stream (counted: fvm_stats.nsync)
+inline void ctx_sync(fvm_ctx* c) {
+    c->n_syncs++;
+    FVM_CUDA(cudaStreamSynchronize(c->stream));
+}
+
 __device__ __forceinline__ void pdl_wait_and_trigger() {
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");

@@ -69,6 +69,23 @@ struct BlockILU {
     size_t smem_stage[2] = {0, 0};   // staged apply: shared bytes for FP64 / FP32, 0 = not possible
     int lanes = 4;                   // row entries prefetched per thread in the staged sweeps
     int apply_threads = 128;         // CTA of the staged apply: 128, or 256 when a level is wider
+    // Schur interface coupling (fvm_set_precond_schur; decomp/schur.c):
+    // each block's interface rows (coupled to another block) follow its
+    // interior rows in the factor; the forward levels [0, lvB) of a block
+    // hold only interior rows and the rest only interface rows, the
+    // backward levels [0, uvS) only interface rows and the rest only
+    // interior rows (sch_lv[2b] = lvB, sch_lv[2b+1] = uvS, sch_nin[b] =
+    // interior rows).  o_ptr/o_col/o_src: the off-block entries of each
+    // factor position (global column, index into J), ascending column.
+    int schur_iters = -1;
+    DevBuf<int> sch_lv, sch_nin, o_ptr, o_col, o_src;
+    std::vector<int> h_sch_nin;
+    DevBuf<double> xg;               // 2 N: published interface iterates (node order), by parity
+    DevBuf<unsigned> sbar;           // grid barrier of the coupled apply
+    DevBuf<int> serr;                // 3: a grid barrier of the coupled apply timed out
+    int* h_serr = nullptr;           // pinned
+    size_t schur_smem[2] = {0, 0};   // dynamic shared bytes of the coupled apply, 0 = not possible
+    int schur_nrmax = 0;
 };
 
 // largest dynamic shared-memory carve-out a CTA may request on sm_100

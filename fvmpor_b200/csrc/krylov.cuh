@@ -76,5 +76,9 @@ void fused_cycle(fvm_ctx* c, Krylov* K, double cj, const double* ewt, double* H_
                  double* g_d);
 bool ilu_ready(fvm_ctx* c);
 int ilu_status(fvm_ctx* c);   // 0 ok, 1 zero pivot in the last factorisation
+// the same status as the last host wait saw it (no wait of its own: valid
+// once any ctx_sync has followed the set-up)
+int ilu_status_seen(fvm_ctx* c);
+int schur_status(fvm_ctx* c); // 0 ok, 3 a barrier of the Schur-coupled apply timed out (then cleared)
 
 } // namespace fvmb

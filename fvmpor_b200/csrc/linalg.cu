@@ -365,7 +365,7 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
     Krylov* K = c->kry[precision];
     if (K && K->m >= m) return c->kry_last = K;
     if (K) {
-        FVM_CUDA(cudaStreamSynchronize(c->stream));
+        ctx_sync(c);
         fvmb_destroy_krylov_impl(K);
         c->kry[precision] = nullptr;
     }
@@ -436,7 +436,7 @@ double reduce_sumsq(fvm_ctx* c, const double* x, const double* w) {
     Krylov* K = krylov_scratch(c);
     fvm_launch(c, k_sumsq, kRedBlocks, kRedThreads, 0, c->stream, c->N, x, w, K->partial.p, K->counter.p, K->res.p);
     FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    ctx_sync(c);
     return K->host[0];
 }
 
@@ -444,7 +444,7 @@ double reduce_dot(fvm_ctx* c, const double* x, const double* y) {
     Krylov* K = krylov_scratch(c);
     fvm_launch(c, k_dot, kRedBlocks, kRedThreads, 0, c->stream, c->N, x, y, K->partial.p, K->counter.p, K->res.p);
     FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    ctx_sync(c);
     return K->host[0];
 }
 
@@ -503,7 +503,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         std::fill(g.begin(), g.end(), 0.0);
         if (!fused) {
             FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-            FVM_CUDA(cudaStreamSynchronize(s));
+            ctx_sync(c);
             const double beta = std::sqrt(K->host[0]);
             rnorm = beta / sqrtN;
             if (!std::isfinite(beta)) { *iters = total; *res_norm = rnorm; return 2; }
@@ -531,7 +531,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                                      s));
             FVM_CUDA(cudaMemcpyAsync(K->host + 3 * (m + 2), K->scale.p, sizeof(double) * (m + 1),
                                      cudaMemcpyDeviceToHost, s));
-            FVM_CUDA(cudaStreamSynchronize(s));
+            ctx_sync(c);
             if (*herr != 0) {
                 // a grid barrier, a flag wait or the factor copy gave up
                 K->err.zero(s);
@@ -624,7 +624,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                 int* herr = reinterpret_cast<int*>(K->host + 4 * (m + 2) + 7);
                 FVM_CUDA(cudaMemcpyAsync(hst, K->st.p, sizeof(ArnState), cudaMemcpyDeviceToHost, s));
                 FVM_CUDA(cudaMemcpyAsync(herr, K->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-                FVM_CUDA(cudaStreamSynchronize(s));
+                ctx_sync(c);
                 if (*herr != 0) {
                     // a grid barrier gave up: the step's numbers are not valid
                     K->err.zero(s);
@@ -647,7 +647,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
             FVM_CUDA(cudaMemcpyAsync(g.data(), g_d, sizeof(double) * (m + 1), cudaMemcpyDeviceToHost, s));
             FVM_CUDA(cudaMemcpyAsync(K->host + 3 * (m + 2), K->scale.p, sizeof(double) * std::max(j, 1),
                                      cudaMemcpyDeviceToHost, s));
-            FVM_CUDA(cudaStreamSynchronize(s));
+            ctx_sync(c);
         }
         for (; K->coop_grid == 0 && j < m; ++j) {
             // w = D P^-1 J D^-1 V_j (left preconditioning, scaled by D = ewt)
@@ -671,7 +671,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
             c->tm.end(TM_CGS, s);
             FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, s));
             FVM_CUDA(cudaMemcpyAsync(K->host + 3 * (m + 2), K->scale.p, sizeof(double) * (nv), cudaMemcpyDeviceToHost, s));
-            FVM_CUDA(cudaStreamSynchronize(s));
+            ctx_sync(c);
             const double* ha = K->host;
             const double* hb = K->host + (m + 2);
             const double* hsc = K->host + 3 * (m + 2);
@@ -715,13 +715,13 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         fvm_launch(c, k_axpy, grid_for(N, 256), 256, 0, s, N, 1.0, K->t.p, x);
         have_x = true;
         if (conv) {
-            FVM_CUDA(cudaStreamSynchronize(s));
+            ctx_sync(c);
             *iters = total;
             *res_norm = rnorm;
             return 0;
         }
     }
-    FVM_CUDA(cudaStreamSynchronize(s));
+    ctx_sync(c);
     *iters = total;
     *res_norm = rnorm;
     return 1;
@@ -732,9 +732,12 @@ int gmres_dev(fvm_ctx* c, double cj, const double* y, const double* yp, const do
               int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt, int op) {
     if (m < 1 || m > 60) throw Error("gmres: krylov dimension must be in [1, 60]");
     Krylov* K = krylov_get(c, m, precision);
-    if (precision)
-        return gmres_impl<float>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op);
-    return gmres_impl<double>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op);
+    const int r = precision
+                      ? gmres_impl<float>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op)
+                      : gmres_impl<double>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op);
+    // a timed-out barrier of the Schur-coupled apply voids the solve
+    if (schur_status(c)) return 2;
+    return r;
 }
 
 } // namespace fvmb

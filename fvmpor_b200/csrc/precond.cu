@@ -25,6 +25,7 @@
 // level only depend on rows of earlier levels), with a barrier between
 // levels, for both the factorisation and the triangular solves
 // (decomp/ILU.c:133-223).
+#include "cgs.cuh"
 #include "ctx.cuh"
 #include "ilu.cuh"
 #include "krylov.cuh"
@@ -379,6 +380,179 @@ __global__ void __launch_bounds__(kIluThreads) k_ilu_apply_smem(const int* __res
     for (int i = threadIdx.x; i < nr; i += blockDim.x) z[lu_row[r0 + i]] = (double)x[i];
 }
 
+// Block ILU(0) coupled through the Schur complement of the block
+// interfaces (decomp/schur.c:1407-1636, precon_schur_apply).  Each block's
+// factor is ordered [interior B; interface] so that it reads
+//   [L_B 0; F~ L_S] [U_B E~; 0 U_S],
+// L_S U_S being the ILU(0) of the block's local Schur complement
+// C - F B^-1 E on C's pattern; the interface system of the whole matrix is
+// S = L_S U_S + C_o, C_o the couplings to the other blocks' interface rows.
+// One cooperative launch, one CTA per block, the factor staged in shared
+// memory once for the whole apply:
+//   z = L^-1 r (the forward sweep; x_L = M_B f and g - F x_L of the
+//     reference), kept in shared memory;
+//   x_S = U_S^-1 z_S, then `iters` times: publish x_S, grid barrier,
+//     x_S <- U_S^-1 (z_S - L_S^-1 C_o x_S) with the other blocks' published
+//     values (block-Jacobi sweeps on S, the reference's level-0 solve);
+//   x_B = U_B^-1 (z_B - E~ x_S) (x_L = M_B (f - E y)).
+// The published iterates alternate between two node-order buffers, so a
+// block still reading sweep i never sees sweep i + 1's values.  Barrier
+// waits are bounded (error 3 in serr, every block leaves at its next
+// barrier); a factor that never reached shared memory passes r through and
+// records error 2, as the staged apply does.
+template <class T> struct SchurArgs {
+    int N, iters;
+    size_t stage_max;          // offset of the forward result in shared memory
+    const int* bstart;
+    const int* lu_ptr;
+    const unsigned short* lu_col;
+    const unsigned short* meta;
+    const int* meta_off;
+    const int* blk_lvl;
+    const int* blk_ulvl;
+    const T* lu;
+    const int* lu_row;
+    const int* sch_lv;
+    const int* sch_nin;
+    const int* o_ptr;
+    const int* o_col;
+    const int* o_src;
+    const double* J;
+    double* xg;
+    unsigned* bar;
+    int* serr;
+    const double* r;
+    double* z;
+    int* err;
+    const int* skip;
+};
+
+template <class T, int KM>
+__global__ void __launch_bounds__(kIluThreads) k_ilu_apply_schur(SchurArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int b = blockIdx.x;
+    const int r0 = a.bstart[b], r1 = a.bstart[b + 1], nr = r1 - r0;
+    const IluWindow w = ilu_window(a.lu_ptr[r0], a.lu_ptr[r1]);
+    const int la = a.blk_lvl[b], nl = a.blk_lvl[b + 1] - la;
+    const int ua = a.blk_ulvl[b], nu = a.blk_ulvl[b + 1] - ua;
+    T* x = reinterpret_cast<T*>(smem_raw);
+    T* val = reinterpret_cast<T*>(smem_raw + round16(sizeof(T) * nr));
+    unsigned short* col = reinterpret_cast<unsigned short*>(val + w.wn);
+    unsigned short* rp = col + w.wn;
+    unsigned short* dg = rp + nr + 1;
+    unsigned short* lrow = dg + nr;
+    unsigned short* urow = lrow + nr;
+    unsigned short* lptr = urow + nr;
+    unsigned short* uptr = lptr + nl + 1;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + ilu_stage_bytes(nr, w.wn, nl + nu + 2, sizeof(T)) - 16);
+    T* zs = reinterpret_cast<T*>(smem_raw + a.stage_max);
+    if (threadIdx.x == 0) {
+        tc05::mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    __syncthreads();
+    const int mo = a.meta_off[b];
+    ilu_stage_bulk(val, col, a.lu, a.lu_col, w, mbar, rp, a.meta + mo, a.meta_off[b + 1] - mo);
+    pdl_wait_and_trigger();
+    if (a.skip && *a.skip) {
+        // a step queued after the stop: every block leaves before any barrier
+        tc05::mbar_wait(mbar, 0);
+        return;
+    }
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) x[i] = (T)a.r[a.lu_row[r0 + i]];
+    bool ok = tc05::mbar_wait(mbar, 0);
+    if (!ok) ok = tc05::mbar_wait(mbar, 0);
+    const bool good = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (!good && threadIdx.x == 0) atomicExch(a.err, 2);
+    const int lvB = a.sch_lv[2 * b], uvS = a.sch_lv[2 * b + 1], nin = a.sch_nin[b];
+    if (good) {
+        ilu_sweep<T, KM, false>(x, val, col, rp, dg, lrow, lptr, 1, nl);
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) zs[i] = x[i];
+        __syncthreads();
+        ilu_sweep<T, KM, true>(x, val, col, rp, dg, urow, uptr, 0, uvS);
+    }
+    for (int it = 0; it < a.iters; ++it) {
+        double* xo = a.xg + (size_t)(it & 1) * a.N;
+        if (good)
+            for (int q = nin + threadIdx.x; q < nr; q += blockDim.x) xo[a.lu_row[r0 + q]] = (double)x[q];
+        // a block without its factor still takes part in every barrier
+        if (!grid_barrier(a.bar, a.bar + 1, a.serr)) return;
+        if (!good) continue;
+        for (int q = threadIdx.x; q < nin; q += blockDim.x) x[q] = (T)0;
+        for (int q = nin + threadIdx.x; q < nr; q += blockDim.x) {
+            T acc = (T)0;
+            const int e1 = a.o_ptr[r0 + q + 1];
+            for (int e = a.o_ptr[r0 + q]; e < e1; ++e) acc += (T)a.J[a.o_src[e]] * (T)__ldcg(xo + a.o_col[e]);
+            x[q] = acc;
+        }
+        __syncthreads();
+        ilu_sweep<T, KM, false>(x, val, col, rp, dg, lrow, lptr, lvB, nl);
+        for (int q = nin + threadIdx.x; q < nr; q += blockDim.x) x[q] = zs[q] - x[q];
+        __syncthreads();
+        ilu_sweep<T, KM, true>(x, val, col, rp, dg, urow, uptr, 0, uvS);
+    }
+    if (!good) {
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) a.z[a.lu_row[r0 + i]] = (double)x[i];
+        return;
+    }
+    if (a.iters > 0) {
+        for (int q = threadIdx.x; q < nin; q += blockDim.x) x[q] = zs[q];
+        __syncthreads();
+    }
+    ilu_sweep<T, KM, true>(x, val, col, rp, dg, urow, uptr, uvS, nu);
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) a.z[a.lu_row[r0 + i]] = (double)x[i];
+}
+
+static const void* schur_kernel(int precision, int lanes) {
+    if (precision) return lanes == 8 ? (const void*)k_ilu_apply_schur<float, 8> : (const void*)k_ilu_apply_schur<float, 4>;
+    return lanes == 8 ? (const void*)k_ilu_apply_schur<double, 8> : (const void*)k_ilu_apply_schur<double, 4>;
+}
+
+template <class T>
+static void launch_schur_apply(fvm_ctx* c, BlockILU* P, const T* lu, const double* r, double* z, const int* skip) {
+    SchurArgs<T> a;
+    a.N = c->N;
+    a.iters = P->schur_iters;
+    a.stage_max = round16(P->smem_stage[P->factored]);
+    a.bstart = P->bstart.p;
+    a.lu_ptr = P->lu_ptr.p;
+    a.lu_col = P->lu_col.p;
+    a.meta = P->meta.p;
+    a.meta_off = P->meta_off.p;
+    a.blk_lvl = P->blk_lvl.p;
+    a.blk_ulvl = P->blk_ulvl.p;
+    a.lu = lu;
+    a.lu_row = P->lu_row.p;
+    a.sch_lv = P->sch_lv.p;
+    a.sch_nin = P->sch_nin.p;
+    a.o_ptr = P->o_ptr.p;
+    a.o_col = P->o_col.p;
+    a.o_src = P->o_src.p;
+    a.J = P->J.p;
+    a.xg = P->xg.p;
+    a.bar = P->sbar.p;
+    a.serr = P->serr.p;
+    a.r = r;
+    a.z = z;
+    a.err = P->status.p;
+    a.skip = skip;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(P->nb);
+    cfg.blockDim = dim3(P->apply_threads);
+    cfg.dynamicSmemBytes = P->schur_smem[P->factored];
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    if (P->lanes == 8) FVM_CUDA(cudaLaunchKernelEx(&cfg, k_ilu_apply_schur<T, 8>, a));
+    else FVM_CUDA(cudaLaunchKernelEx(&cfg, k_ilu_apply_schur<T, 4>, a));
+    c->launches++;
+}
+
 // Shared-memory factorisation: gather the block's Jacobian entries into the
 // same copy window the apply uses, eliminate level by level in shared
 // memory (IKJ, pivots inverted after their row), write the block back.
@@ -500,15 +674,22 @@ __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__
 // Colour order of the rows [r0, r1) of a block (offsets from r0): greedy
 // colouring in natural order over the couplings inside the block, then
 // stable by colour.  The CPU oracle restates the same rule.
-static std::vector<int> block_colour_order(const std::vector<int>& rp, const std::vector<int>& cl, int r0, int r1) {
+//
+// With interface_last (Schur coupling) the rows coupled to a node outside the
+// block (interface rows) follow all interior rows: the sort key is
+// (interface, colour); *n_interior gets the number of interior rows.
+static std::vector<int> block_colour_order(const std::vector<int>& rp, const std::vector<int>& cl, int r0, int r1,
+                                           bool interface_last = false, int* n_interior = nullptr) {
     const int nr = r1 - r0;
-    std::vector<int> colour(nr, 0), ord(nr);
-    int ncol = 1;
+    std::vector<int> colour(nr, 0), ord(nr), key(nr);
+    int ncol = 1, nin = 0;
     for (int i = r0; i < r1; ++i) {
         unsigned long long used = 0ull;
         std::vector<int> more;
+        bool iface = false;
         for (int p = rp[i]; p < rp[i + 1]; ++p) {
             const int j = cl[p];
+            if (j < r0 || j >= r1) iface = true;
             if (j < r0 || j >= i) continue;
             const int cj = colour[j - r0];
             if (cj < 64) used |= 1ull << cj;
@@ -522,10 +703,13 @@ static std::vector<int> block_colour_order(const std::vector<int>& rp, const std
                 if (m == cc) ++cc;
         }
         colour[i - r0] = cc;
+        key[i - r0] = interface_last && iface ? (1 << 20) + cc : cc;
+        if (!iface) ++nin;
         ncol = std::max(ncol, cc + 1);
     }
+    if (n_interior) *n_interior = interface_last ? nin : nr;
     for (int ii = 0; ii < nr; ++ii) ord[ii] = ii;
-    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b2) { return colour[a] < colour[b2]; });
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b2) { return key[a] < key[b2]; });
     return ord;
 }
 
@@ -610,7 +794,13 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
     FVM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
     int target = 1500;
     int nb;
-    if (N >= nsm * 256) nb = nsm * std::max(1, c->ilu_per_sm);
+    // per_sm 0 (the default): the fewest blocks per SM that keep a block at
+    // most kAutoBlockRows rows, the size whose FP32 factor window still fits
+    // the staged apply's shared memory (1 on the 200k-node box, 5 at 1M)
+    constexpr double kAutoBlockRows = 1600.0;
+    const int per_sm = c->ilu_per_sm > 0 ? c->ilu_per_sm
+                                         : std::max(1, (int)std::ceil((double)N / (nsm * kAutoBlockRows)));
+    if (N >= nsm * 256) nb = nsm * per_sm;
     else nb = std::max(1, (N + target - 1) / target);
     nb = std::min(nb, N);
     std::vector<int> bstart(nb + 1);
@@ -630,9 +820,16 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
     std::vector<int> lvl(N), ulvl(N);
     std::vector<int> lvl_ptr(1, 0), lvl_rows, blk_lvl(1, 0), ulvl_ptr(1, 0), ulvl_rows, blk_ulvl(1, 0);
     int nlmax = 0;
+    // Schur coupling: interface rows last, levels split by group, and the
+    // off-block entries of each factor position
+    P->schur_iters = c->schur_iters;
+    const bool schur = P->schur_iters >= 0;
+    std::vector<int> sch_lv(2 * (size_t)nb, 0), sch_nin(nb, 0), o_ptr(N + 1, 0), o_col, o_src;
     for (int b = 0; b < nb; ++b) {
         int r0 = bstart[b], r1 = bstart[b + 1];
-        const std::vector<int> ord = block_colour_order(rp, cl, r0, r1);
+        int nin = r1 - r0;
+        const std::vector<int> ord = block_colour_order(rp, cl, r0, r1, schur, &nin);
+        sch_nin[b] = nin;
         std::vector<int> linv(r1 - r0);
         for (int ii = 0; ii < r1 - r0; ++ii) linv[ord[ii]] = ii;
         std::vector<std::pair<int, int>> ent;
@@ -642,9 +839,13 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
             ent.clear();
             for (int p = rp[i]; p < rp[i + 1]; ++p) {
                 int j = cl[p];
-                if (j < r0 || j >= r1) continue;
+                if (j < r0 || j >= r1) {
+                    if (schur) { o_col.push_back(j); o_src.push_back(p); }
+                    continue;
+                }
                 ent.emplace_back(linv[j - r0], p);
             }
+            o_ptr[q + 1] = (int)o_col.size();
             std::sort(ent.begin(), ent.end());
             lu_diag[q] = -1;
             for (auto& e : ent) {
@@ -655,20 +856,29 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
             lu_ptr[q + 1] = (int)lu_src.size();
             if (lu_diag[q] < 0) throw Error("block-ILU: missing diagonal");
         }
-        int nl = 0;
+        // with the Schur coupling no level mixes interior and interface
+        // rows: forward, every interface row comes after the last interior
+        // level; backward, every interior row after the last interface level
+        int nl = 0, lvB = 0;
         for (int i = r0; i < r1; ++i) {
             int l = 0;
             for (int p = lu_ptr[i]; p < lu_diag[i]; ++p) l = std::max(l, lvl[r0 + lu_col[p]] + 1);
+            if (schur && i - r0 >= nin) l = std::max(l, lvB);
             lvl[i] = l;
             nl = std::max(nl, l + 1);
+            if (i - r0 < nin) lvB = nl;
         }
-        int nu = 0;
+        int nu = 0, uvS = 0;
         for (int i = r1 - 1; i >= r0; --i) {
             int l = 0;
             for (int p = lu_diag[i] + 1; p < lu_ptr[i + 1]; ++p) l = std::max(l, ulvl[r0 + lu_col[p]] + 1);
+            if (schur && i - r0 < nin) l = std::max(l, uvS);
             ulvl[i] = l;
             nu = std::max(nu, l + 1);
+            if (i - r0 >= nin) uvS = nu;
         }
+        sch_lv[2 * (size_t)b] = lvB;
+        sch_lv[2 * (size_t)b + 1] = uvS;
         nlmax = std::max(nlmax, std::max(nl, nu));
         for (int l = 0; l < nl; ++l) {
             for (int i = r0; i < r1; ++i) if (lvl[i] == l) lvl_rows.push_back(i);
@@ -772,6 +982,17 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
         for (size_t g = 0; g + 1 < lvl_ptr.size(); ++g) widest = std::max(widest, lvl_ptr[g + 1] - lvl_ptr[g]);
         for (size_t g = 0; g + 1 < ulvl_ptr.size(); ++g) widest = std::max(widest, ulvl_ptr[g + 1] - ulvl_ptr[g]);
         P->apply_threads = widest > 128 ? 256 : 128;
+        // the global-memory apply keeps the block's vector in shared memory
+        if (!P->smem_stage[0]) {
+            if (sizeof(double) * (size_t)maxb > kMaxDynSmem)
+                throw Error("block-ILU: blocks too large for the FP64 apply (set more blocks per SM)");
+            raise_smem_limit(k_ilu_apply<double>, sizeof(double) * (size_t)maxb);
+        }
+        if (!P->smem_stage[1]) {
+            if (sizeof(float) * (size_t)maxb > kMaxDynSmem)
+                throw Error("block-ILU: blocks too large for the FP32 apply (set more blocks per SM)");
+            raise_smem_limit(k_ilu_apply<float>, sizeof(float) * (size_t)maxb);
+        }
         if (P->smem_stage[0]) {
             raise_smem_limit(k_ilu_apply_smem<double, 4>, (size_t)P->smem_stage[0]);
             raise_smem_limit(k_ilu_apply_smem<double, 8>, (size_t)P->smem_stage[0]);
@@ -783,7 +1004,44 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
             raise_smem_limit(k_ilu_factor_smem<float>, (size_t)(round16(P->smem_stage[1]) + 8 * (size_t)P->scr_words[1]));
         }
     }
+    if (schur) {
+        // the coupled apply keeps each block's staged factor plus the
+        // forward result in shared memory through its grid barriers, so it
+        // needs both to fit and every block resident at once
+        int nsm2 = 148, coop = 0;
+        FVM_CUDA(cudaDeviceGetAttribute(&nsm2, cudaDevAttrMultiProcessorCount, c->device));
+        FVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
+        for (int pr = 0; pr < 2; ++pr) {
+            P->schur_smem[pr] = 0;
+            if (!P->smem_stage[pr] || !coop) continue;
+            const size_t sz = pr ? sizeof(float) : sizeof(double);
+            const size_t need = round16(P->smem_stage[pr]) + round16(sz * (size_t)maxb);
+            if (need > kMaxDynSmem) continue;
+            const void* kfn = schur_kernel(pr, P->lanes);
+            raise_smem_limit(kfn, need);
+            int per_sm = 0;
+            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, P->apply_threads, need));
+            if ((long)per_sm * nsm2 >= nb) P->schur_smem[pr] = need;
+        }
+        P->schur_nrmax = maxb;
+    }
     cudaStream_t s = c->stream;
+    if (schur) {
+        P->sch_lv.upload(sch_lv, s);
+        P->sch_nin.upload(sch_nin, s);
+        P->h_sch_nin = sch_nin;
+        P->o_ptr.upload(o_ptr, s);
+        if (o_col.empty()) { o_col.push_back(0); o_src.push_back(0); }
+        P->o_col.upload(o_col, s);
+        P->o_src.upload(o_src, s);
+        P->xg.alloc(2 * (size_t)N);
+        P->sbar.alloc(2);
+        P->sbar.zero(s);
+        P->serr.alloc(1);
+        P->serr.zero(s);
+        FVM_CUDA(cudaMallocHost(&P->h_serr, sizeof(int)));
+        *P->h_serr = 0;
+    }
     P->col.upload(P->h_col, s);
     P->rowof.upload(rowof, s);
     P->J.alloc(P->nnz);
@@ -906,11 +1164,23 @@ void jacobian_apply(fvm_ctx* c, double cj, const double* x, double* y, const int
 
 int ilu_status(fvm_ctx* c) {
     if (!c->ilu || !c->ilu->h_status) return 0;
-    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    ctx_sync(c);
     return *c->ilu->h_status;
 }
 
+int ilu_status_seen(fvm_ctx* c) { return c->ilu && c->ilu->h_status ? *c->ilu->h_status : 0; }
+
 bool ilu_ready(fvm_ctx* c) { return c->ilu && c->ilu->factored >= 0; }
+
+int schur_status(fvm_ctx* c) {
+    BlockILU* P = c->ilu;
+    if (!P || P->schur_iters < 0 || !P->h_serr) return 0;
+    FVM_CUDA(cudaMemcpyAsync(P->h_serr, P->serr.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    ctx_sync(c);
+    const int e = *P->h_serr;
+    if (e) FVM_CUDA(cudaMemsetAsync(P->serr.p, 0, sizeof(int), c->stream));
+    return e;
+}
 
 void psolve_dev(fvm_ctx* c, const double* r, double* z, const int* skip) {
     BlockILU* P = c->ilu;
@@ -921,6 +1191,14 @@ void psolve_dev(fvm_ctx* c, const double* r, double* z, const int* skip) {
         fvm_ctx* c;
         ~EndTimer() { c->tm.end(TM_ILU_APPLY, c->stream); }
     } end_timer{c};
+    if (P->schur_iters >= 0) {
+        if (!P->schur_smem[P->factored])
+            throw Error("psolve: the Schur coupling needs every block's staged factor and forward result in shared "
+                        "memory with all blocks resident at once (use the FP32 factor on large blocks)");
+        if (P->factored) launch_schur_apply(c, P, P->lu32.p, r, z, skip);
+        else launch_schur_apply(c, P, P->lu64.p, r, z, skip);
+        return;
+    }
     if (P->smem_stage[P->factored]) {
         size_t sm = P->smem_stage[P->factored];
         auto go = [&](auto kern, const auto* lu) {
@@ -954,6 +1232,7 @@ using namespace fvmb;
 void fvmb_destroy_ilu(fvmb::BlockILU* p) {
     if (!p) return;
     if (p->h_status) cudaFreeHost(p->h_status);
+    if (p->h_serr) cudaFreeHost(p->h_serr);
     delete p;
 }
 
@@ -981,6 +1260,7 @@ extern "C" int fvm_psolve(fvm_ctx* c, const double* r, double* z) {
         psolve_dev(c, r, z);
         FVM_CUDA(cudaGetLastError());
         FVM_CUDA(cudaStreamSynchronize(c->stream));
+        if (schur_status(c)) throw Error("fvm_psolve: a grid barrier of the Schur-coupled apply timed out");
         return 0;
     } catch (const Error& ex) {
         set_error(ex.what());
@@ -994,13 +1274,56 @@ extern "C" int fvm_psolve(fvm_ctx* c, const double* r, double* z) {
 extern "C" int fvm_set_precond_blocks(fvm_ctx* c, int per_sm) {
     try {
         if (!c) throw Error("fvm_set_precond_blocks: null context");
-        if (per_sm < 1 || per_sm > 16) throw Error("fvm_set_precond_blocks: blocks per SM must be in [1, 16]");
+        if (per_sm < 0 || per_sm > 16)
+            throw Error("fvm_set_precond_blocks: blocks per SM must be in [1, 16], or 0 for automatic");
         FVM_CUDA(cudaStreamSynchronize(c->stream));
         c->ilu_per_sm = per_sm;
         if (c->ilu) {
             fvmb_destroy_ilu(c->ilu);
             c->ilu = nullptr;
         }
+        return 0;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+extern "C" int fvm_set_precond_schur(fvm_ctx* c, int iters) {
+    try {
+        if (!c) throw Error("fvm_set_precond_schur: null context");
+        if (iters < -1 || iters > 64) throw Error("fvm_set_precond_schur: iterations must be in [-1, 64]");
+        FVM_CUDA(cudaStreamSynchronize(c->stream));
+        c->schur_iters = iters;
+        if (c->ilu) {
+            fvmb_destroy_ilu(c->ilu);
+            c->ilu = nullptr;
+        }
+        return 0;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+extern "C" int fvm_precond_schur_info(fvm_ctx* c, int* iters, int* interface_rows, int* supported) {
+    try {
+        if (!c || !c->ilu || !c->ilu->built) throw Error("fvm_precond_schur_info: no preconditioner");
+        BlockILU* P = c->ilu;
+        if (iters) *iters = P->schur_iters;
+        if (interface_rows) {
+            long n = 0;
+            if (P->schur_iters >= 0)
+                for (int b = 0; b < P->nb; ++b) n += P->h_bstart[b + 1] - P->h_bstart[b] - P->h_sch_nin[b];
+            *interface_rows = (int)n;
+        }
+        if (supported) *supported = (P->schur_smem[0] ? 1 : 0) | (P->schur_smem[1] ? 2 : 0);
         return 0;
     } catch (const Error& ex) {
         set_error(ex.what());

@@ -650,7 +650,7 @@ bool predictor_apply(fvm_ctx* c, Predictor* p, double rtol, double atol, double 
     fvm_launch(c, k_dot3, kRedBlocks, kRedThreads, 0, c->stream, N, F, p->Fg.p, K->partial.p, K->counter.p,
                K->res.p);
     FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    FVM_CUDA(cudaStreamSynchronize(c->stream));
+    ctx_sync(c);
     const double A = K->host[0], B = K->host[1], Cc = K->host[2];
     const double curv = A - 2.0 * B + Cc;   // |F1 - F0|^2
     if (!std::isfinite(A) || !std::isfinite(Cc) || !(curv > 0.0)) return false;

@@ -244,13 +244,32 @@ int fvm_autotune(fvm_ctx* ctx, fvm_tune_result* out);
  * and Krylov kernels run over all members in the same launches.  No
  * counterpart in the reference (one mesh per run). */
 int fvm_set_members(fvm_ctx* ctx, int n_members, const int* member_ptr);
-/* Block-ILU partition on large meshes: per_sm (1..16) blocks per SM.  Fewer,
+/* Block-ILU partition on large meshes: per_sm (1..16) blocks per SM, or 0
+ * (the default) for the fewest blocks per SM that keep every block at most
+ * 1,600 rows, the size whose FP32 factor fits the shared-memory apply.  Fewer,
  * larger blocks couple more nodes inside the factor (fewer Krylov
  * iterations); more, smaller ones shorten the level chains of the
  * triangular solves and let several blocks share an SM.  Drops the current
  * factor; the next fvm_psetup rebuilds the pattern.  The reference's
  * preconditioner is one direct factorisation (preconditioner_dss.cpp:284-405). */
 int fvm_set_precond_blocks(fvm_ctx* ctx, int per_sm);
+/* Schur interface coupling of the block ILU(0) (decomp/schur.c:887-987
+ * S = C - F B^-1 E, :1407-1636 precon_schur_apply).  iters < 0: off (plain
+ * block-Jacobi ILU(0), the default).  iters >= 0: every block orders its
+ * interface rows (those coupled to another block) after its interior rows,
+ * so its ILU(0) holds the ILU(0) of its local Schur complement, and each
+ * apply runs `iters` block-Jacobi sweeps of the global interface system
+ * (local Schur factors plus the couplings between blocks) before the
+ * interior back substitution.  Needs every block's staged factor in shared
+ * memory (the FP32 factor on the 3D meshes); fvm_psolve reports an error
+ * otherwise.  Drops the current factor; the next fvm_psetup rebuilds the
+ * pattern.  The Krylov paths then use separate kernels per Arnoldi step
+ * (no fused cycle). */
+int fvm_set_precond_schur(fvm_ctx* ctx, int iters);
+/* The Schur option of the current pattern: its iterations, the number of
+ * interface rows, and which factor precisions can run it (bit 0 FP64,
+ * bit 1 FP32).  Any pointer may be NULL. */
+int fvm_precond_schur_info(fvm_ctx* ctx, int* iters, int* interface_rows, int* supported);
 int fvm_set_element_pass(fvm_ctx* ctx, int variant, int chunk);
 int fvm_element_pass(const fvm_ctx* ctx, int* variant, int* chunk);
 
@@ -310,6 +329,7 @@ typedef struct {
     int  last_order;
     double last_h;
     double t;
+    long nsync;   /* host waits on the device during the call      */
 } fvm_stats;
 
 void fvm_opts_default(fvm_opts* o);
@@ -366,7 +386,11 @@ int fvm_integrate_outputs(fvm_ctx* ctx, const fvm_opts* opts, double t0,
  * with GMRES(opts->krylov_dim) at 0.05 newton_tol in opts->precision.  Run
  * on the trace of an adaptive integration (fvm_step_trace), it removes the
  * step-size decisions from a comparison of two implementations, so that
- * their states agree to the corrector tolerance rather than to rtol.  The
+ * their states agree to the corrector tolerance rather than to rtol.  With
+ * opts->use_predictor set, every replayed step first tries the learned
+ * Newton iterate (kept when its residual test passes; stats->npred counts
+ * the kept ones, the trace marks them), so that replays with and without it
+ * measure the work it saves at one corrector tolerance.  The
  * orders may rise by at most one per step.  y0, y_end are device pointers.
  * Returns 0, 1 when some corrector stopped at max_newton (the run still
  * completes), < 0 on failure.  No counterpart in the reference: IDAS has no

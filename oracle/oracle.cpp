@@ -170,6 +170,16 @@ struct Oracle {
     // positions, fsrc the source entry of J
     std::vector<int> frow, fptr, fcol, fsrc, fdiag;
     std::vector<double> LU;
+    // Schur interface coupling (decomp/schur.c:887-987, 1407-1636).  < 0:
+    // off (block-Jacobi ILU(0)).  >= 0: every block orders its interior
+    // rows (no coupling outside the block) before its interface rows, each
+    // group in colour order, and the apply iterates the interface system
+    // that many times against the other blocks' interface values.
+    // fifc[b]: first interface position of block b; optr/ocol/osrc: the
+    // off-block entries of each factor position (global column, J entry),
+    // in J's column order.
+    int schur_iters = -1;
+    std::vector<int> fifc, optr, ocol, osrc;
 
     void build(const fvm_mesh* m, const fvm_physics* ph);
     void residual(double t, const double* y, const double* yp, double* res);
@@ -756,24 +766,34 @@ void Oracle::psetup(double t, double cj, double hh, const double* y, const doubl
 // row of the block), then stable by colour.  The same rule as the device
 // factor's set-up: rows of one colour are uncoupled, so each triangular
 // sweep of a block has as many levels as colours.
+//
+// With interface_last (the Schur coupling), rows coupled to a node outside
+// the block (interface rows) come after all interior rows: the sort key is
+// (interface, colour), so each (group, colour) is still one level.
 static std::vector<int> block_colour_order(const std::vector<int>& jrow, const std::vector<int>& jcol, int r0,
-                                           int r1) {
+                                           int r1, bool interface_last = false, int* n_interior = nullptr) {
     const int nr = r1 - r0;
-    std::vector<int> colour(nr, 0), ord(nr);
+    std::vector<int> colour(nr, 0), ord(nr), key(nr);
+    int nin = 0;
     for (int i = r0; i < r1; ++i) {
         std::vector<int> used;
+        bool iface = false;
         for (int p = jrow[i]; p < jrow[i + 1]; ++p) {
             const int j = jcol[p];
             if (j >= r0 && j < i) used.push_back(colour[j - r0]);
+            if (j < r0 || j >= r1) iface = true;
         }
         std::sort(used.begin(), used.end());
         int cc = 0;
         for (int u : used)
             if (u == cc) ++cc;
         colour[i - r0] = cc;
+        key[i - r0] = interface_last && iface ? (1 << 20) + cc : cc;
+        if (!iface) ++nin;
     }
+    if (n_interior) *n_interior = interface_last ? nin : nr;
     for (int ii = 0; ii < nr; ++ii) ord[ii] = ii;
-    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return colour[a] < colour[b]; });
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return key[a] < key[b]; });
     return ord;
 }
 
@@ -787,9 +807,16 @@ int Oracle::ilu_factor() {
     fcol.clear();
     fsrc.clear();
     std::vector<std::pair<int, int>> ent;
+    const bool schur = schur_iters >= 0;
+    fifc.assign(nb, 0);
+    optr.assign(N + 1, 0);
+    ocol.clear();
+    osrc.clear();
     for (int b = 0; b < nb; ++b) {
         const int r0 = bstart[b], r1 = bstart[b + 1];
-        const std::vector<int> ord = block_colour_order(jrow, jcol, r0, r1);
+        int nin = 0;
+        const std::vector<int> ord = block_colour_order(jrow, jcol, r0, r1, schur, &nin);
+        fifc[b] = r0 + nin;
         std::vector<int> linv(r1 - r0);
         for (int ii = 0; ii < r1 - r0; ++ii) linv[ord[ii]] = ii;
         for (int ii = 0; ii < r1 - r0; ++ii) {
@@ -799,7 +826,9 @@ int Oracle::ilu_factor() {
             for (int p = jrow[i]; p < jrow[i + 1]; ++p) {
                 const int j = jcol[p];
                 if (j >= r0 && j < r1) ent.emplace_back(r0 + linv[j - r0], p);
+                else if (schur) { ocol.push_back(j); osrc.push_back(p); }
             }
+            optr[q + 1] = (int)ocol.size();
             std::sort(ent.begin(), ent.end());
             for (auto& e : ent) {
                 if (e.first == q) fdiag[q] = (int)fcol.size();
@@ -836,6 +865,69 @@ int Oracle::ilu_factor() {
 
 void Oracle::psolve(const double* r, double* z) const {
     int nb = (int)bstart.size() - 1;
+    if (schur_iters >= 0) {
+        // Schur coupling of the blocks through their interface rows
+        // (precon_schur_apply, decomp/schur.c:1407-1636).  With each block's
+        // factor ordered [interior B; interface S~] = [L_B 0; F~ L_S] [U_B E~;
+        // 0 U_S], S~ = L_S U_S is the ILU(0) of the local Schur complement
+        // C - F B^-1 E on C's pattern, and the global interface system is
+        // S = S~ + C_o (C_o: couplings to other blocks' interface rows).
+        //   forward  z = L^-1 r                       (x_L = M_B f, g - F x_L)
+        //   x_S = U_S^-1 z_S, then schur_iters times
+        //        x_S <- U_S^-1 (z_S - L_S^-1 C_o x_S)  (block-Jacobi on S)
+        //   x_B = U_B^-1 (z_B - E~ x_S)              (x_L = M_B (f - E y))
+        // With schur_iters = 0 this is the block-Jacobi apply in the
+        // interface-last order.
+        std::vector<double> zf(N), x(N), xn(N), xg(N);
+#pragma omp parallel for schedule(dynamic)
+        for (int b = 0; b < nb; ++b) {
+            const int r0 = bstart[b], r1 = bstart[b + 1], i0 = fifc[b];
+            for (int q = r0; q < r1; ++q) {
+                double acc = r[frow[q]];
+                for (int p = fptr[q]; p < fdiag[q]; ++p) acc -= LU[p] * zf[fcol[p]];
+                zf[q] = acc;
+            }
+            for (int q = r1 - 1; q >= i0; --q) {
+                double acc = zf[q];
+                for (int p = fdiag[q] + 1; p < fptr[q + 1]; ++p) acc -= LU[p] * x[fcol[p]];
+                x[q] = acc * LU[fdiag[q]];
+            }
+        }
+        for (int it = 0; it < schur_iters; ++it) {
+            for (int q = 0; q < N; ++q) xg[frow[q]] = x[q];
+#pragma omp parallel for schedule(dynamic)
+            for (int b = 0; b < nb; ++b) {
+                const int r1 = bstart[b + 1], i0 = fifc[b];
+                // c = L_S^-1 C_o x_S (interior entries of L meet zeros)
+                for (int q = i0; q < r1; ++q) {
+                    double acc = 0.0;
+                    for (int p = optr[q]; p < optr[q + 1]; ++p) acc += J[osrc[p]] * xg[ocol[p]];
+                    for (int p = fptr[q]; p < fdiag[q]; ++p)
+                        if (fcol[p] >= i0) acc -= LU[p] * xn[fcol[p]];
+                    xn[q] = acc;
+                }
+                for (int q = i0; q < r1; ++q) xn[q] = zf[q] - xn[q];
+                for (int q = r1 - 1; q >= i0; --q) {
+                    double acc = xn[q];
+                    for (int p = fdiag[q] + 1; p < fptr[q + 1]; ++p) acc -= LU[p] * xn[fcol[p]];
+                    xn[q] = acc * LU[fdiag[q]];
+                }
+            }
+            for (int b = 0; b < nb; ++b)
+                for (int q = fifc[b]; q < bstart[b + 1]; ++q) x[q] = xn[q];
+        }
+#pragma omp parallel for schedule(dynamic)
+        for (int b = 0; b < nb; ++b) {
+            const int r0 = bstart[b], i0 = fifc[b];
+            for (int q = i0 - 1; q >= r0; --q) {
+                double acc = zf[q];
+                for (int p = fdiag[q] + 1; p < fptr[q + 1]; ++p) acc -= LU[p] * x[fcol[p]];
+                x[q] = acc * LU[fdiag[q]];
+            }
+            for (int q = r0; q < bstart[b + 1]; ++q) z[frow[q]] = x[q];
+        }
+        return;
+    }
 #pragma omp parallel for schedule(dynamic)
     for (int b = 0; b < nb; ++b) {
         const int r0 = bstart[b], r1 = bstart[b + 1];
@@ -1012,8 +1104,11 @@ struct CpuOps {
             for (int j = 1; j <= k; ++j) { s += phi[j][i]; sp += gamma[j] * phi[j][i]; }
             y[i] = s; yp[i] = sp; e[i] = 0.0;
         }
+        pn = wrms(y);
     }
-    double wrms_y() { return wrms(y); }
+    double pn = 0.0;
+    double pred_norm() const { return pn; }
+    void set_order(int) {}
     void residual() {
         const double a = omp_get_wtime();
         o.residual(tcur, y.data(), yp.data(), F.data());
@@ -1176,6 +1271,23 @@ int orc_vg(double alpha, double n, double S_r, int count, const double* h, doubl
     std::copy(b.begin(), b.end(), dSw);
     std::copy(k.begin(), k.end(), krw);
     return 0;
+}
+
+// Schur interface coupling of the block ILU(0) (< 0 off, >= 0 interface
+// iterations per apply); takes effect at the next factorisation
+int orc_set_schur(orc_ctx* c, int iters) {
+    reinterpret_cast<Oracle*>(c)->schur_iters = iters;
+    return 0;
+}
+
+// interface rows of each block after the last factorisation (0 when the
+// Schur coupling is off)
+int orc_schur_interface_rows(orc_ctx* c) {
+    Oracle* o = reinterpret_cast<Oracle*>(c);
+    if (o->schur_iters < 0) return 0;
+    long n = 0;
+    for (size_t b = 0; b + 1 < o->bstart.size(); ++b) n += o->bstart[b + 1] - o->fifc[b];
+    return (int)n;
 }
 
 int orc_psolve(orc_ctx* c, const double* r, double* z) {

@@ -44,6 +44,8 @@ def lib():
         L.orc_jacobian_nnz.argtypes = [P]
         L.orc_jacobian.argtypes = [P, P, P, P, P]
         L.orc_psolve.argtypes = [P, P, P]
+        L.orc_set_schur.argtypes = [P, I]
+        L.orc_schur_interface_rows.argtypes = [P]
         L.orc_gmres.argtypes = [P, D, P, P, P, P, P, P, I, I, D, P, P]
         L.orc_integrate.argtypes = [P, P, I, D, D, P, P, P]
         L.orc_integrate_outputs.argtypes = [P, P, I, D, P, I, P, P, P, P]
@@ -136,6 +138,14 @@ class Oracle:
         colour = np.zeros(self.N, np.int32)
         lib().orc_jacobian(self._c, _p(rp), _p(col), _p(val), _p(colour))
         return rp, col, val, colour
+
+    def set_schur(self, iters):
+        """Schur interface coupling of the block ILU(0): < 0 off, >= 0 the
+        interface iterations of every apply (next factorisation on)"""
+        lib().orc_set_schur(self._c, int(iters))
+
+    def schur_interface_rows(self):
+        return lib().orc_schur_interface_rows(self._c)
 
     def psolve(self, r):
         z = np.zeros(self.N)

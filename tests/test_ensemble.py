@@ -86,3 +86,44 @@ def test_ensemble_matches_members_integrated_alone(cuda):
         err = np.abs(yu[mp[m]:mp[m + 1]] - ym).max() / span
         # both runs meet rtol = atol = 1e-6 per member, with different steps
         assert err < 1e-4, (m, err)
+
+
+@pytest.mark.gpu
+def test_sixteen_members_of_the_configured_sizes(cuda):
+    # 16 members drawn from the configured size range (2k-40k nodes each):
+    # the union's residual against the oracle, then a one-hour union run
+    # (FP32 preconditioner, per-member Newton and error tests, the Krylov
+    # tolerance scaled to the smallest member) against every member
+    # integrated on its own
+    p = fb.Problem("ensemble2d", n_members=16, nmin=2000, nmax=40000, seed=5)
+    mp = p.member_ptr
+    n = np.diff(mp)
+    assert len(n) == 16 and n.min() < 10000 and n.max() > 25000
+    ph = fb.Physics(p)
+    orc = Oracle(p)
+    y, yp = state(p, 4)
+    res = torch.empty(p.n_nodes, dtype=torch.float64, device=cuda)
+    ph.residual(0.0, torch.as_tensor(y, device=cuda), torch.as_tensor(yp, device=cuda), res)
+    ref = orc.residual(0.0, y, yp)
+    scale = np.abs(ref) + 1e-3 * np.abs(ref).max() + np.abs(orc.ahh() * yp)
+    assert (np.abs(res.cpu().numpy() - ref) / scale).max() < 1e-11
+    del orc
+    y0 = torch.empty(p.n_nodes, dtype=torch.float64, device=cuda)
+    ph.initial_head(y0)
+    yu = torch.empty_like(y0)
+    rc, st = fb.Integrator(ph, krylov_dim=30, precision=1).integrate(0.0, 3600.0, y0, yu)
+    assert rc == 0, st
+    yu = yu.cpu().numpy()
+    for m in range(len(mp) - 1):
+        q = p.member(m)
+        phm = fb.Physics(q)
+        y0m = torch.empty(q.n_nodes, dtype=torch.float64, device=cuda)
+        phm.initial_head(y0m)
+        ym = torch.empty_like(y0m)
+        rc, _ = fb.Integrator(phm, krylov_dim=30, precision=1).integrate(0.0, 3600.0, y0m, ym)
+        assert rc == 0
+        ym = ym.cpu().numpy()
+        err = np.abs(yu[mp[m]:mp[m + 1]] - ym).max() / np.abs(ym).max()
+        assert err < 1e-4, (m, n[m], err)
+        phm.close()
+    ph.close()

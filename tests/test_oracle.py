@@ -305,6 +305,119 @@ def test_block_ilu_colour_order_matches_a_dense_restatement(p2, nblocks):
     assert np.abs(zo - z).max() <= 1e-10 * np.abs(z).max()
 
 
+def _schur_blocks(rp, col, val, N, nblocks):
+    """per block of the Schur variant: the factor order (interior rows, then
+    interface rows, each by greedy colour, stable), the first interface
+    position, and the block's ILU(0) restricted to its pattern (dense)"""
+    out = []
+    bstart = [(N * b) // nblocks for b in range(nblocks + 1)]
+    for b in range(nblocks):
+        r0, r1 = bstart[b], bstart[b + 1]
+        _, colour = _colour_order(rp, col, r0, r1)
+        iface = {g: any(not (r0 <= j < r1) for j in col[rp[g]:rp[g + 1]]) for g in range(r0, r1)}
+        order = sorted(range(r0, r1), key=lambda g: (iface[g], colour[g], g))
+        n = r1 - r0
+        pos = {g: k for k, g in enumerate(order)}
+        A = np.zeros((n, n))
+        mask = np.zeros((n, n), bool)
+        for g in range(r0, r1):
+            for p in range(rp[g], rp[g + 1]):
+                if r0 <= col[p] < r1:
+                    A[pos[g], pos[col[p]]] = val[p]
+                    mask[pos[g], pos[col[p]]] = True
+        LU = A.copy()
+        for i in range(n):
+            for k in range(i):
+                if mask[i, k]:
+                    LU[i, k] /= LU[k, k]
+                    for j in range(k + 1, n):
+                        if mask[i, j] and mask[k, j]:
+                            LU[i, j] -= LU[i, k] * LU[k, j]
+        L = np.tril(LU * mask, -1) + np.eye(n)
+        U = np.triu(LU * mask)
+        nin = sum(1 for g in order if not iface[g])
+        out.append((r0, r1, order, nin, L, U))
+    return out
+
+
+@pytest.mark.parametrize("iters", [0, 1, 3])
+def test_schur_apply_matches_a_dense_restatement(p2, iters):
+    # The Schur coupling (decomp/schur.c:1407-1636) restated with dense
+    # arrays: each block's factor in the interface-last order gives
+    # [L_B 0; F~ L_S][U_B E~; 0 U_S]; the interface system is L_S U_S + C_o
+    # with C_o the couplings to other blocks, solved by `iters` block-Jacobi
+    # sweeps from the block-Jacobi start; then x_B = U_B^-1 (z_B - E~ x_S).
+    o = Oracle(p2)
+    y, yp = setup_state(p2, 9)
+    F0 = o.residual(0.0, y, yp)
+    ewt = 1.0 / (1e-6 * np.abs(y) + 1e-6)
+    nb = 4
+    o.set_schur(iters)
+    assert o.psetup(0.0, 1e-2, 1e2, y, yp, F0, ewt, nb) == 0
+    rp, col, val, _ = o.jacobian()
+    N = p2.n_nodes
+    blocks = _schur_blocks(rp, col, val, N, nb)
+    assert o.schur_interface_rows() == sum(r1 - r0 - nin for r0, r1, _, nin, _, _ in blocks)
+    r = np.random.default_rng(10).standard_normal(N)
+    zf, xs = {}, {}
+    for bi, (r0, r1, order, nin, L, U) in enumerate(blocks):
+        zf[bi] = np.linalg.solve(L, r[order])
+        xs[bi] = np.linalg.solve(U[nin:, nin:], zf[bi][nin:])
+    for _ in range(iters):
+        xg = np.zeros(N)
+        for bi, (r0, r1, order, nin, L, U) in enumerate(blocks):
+            xg[np.array(order[nin:], int)] = xs[bi]
+        new = {}
+        for bi, (r0, r1, order, nin, L, U) in enumerate(blocks):
+            c = np.array([sum(val[p] * xg[col[p]] for p in range(rp[g], rp[g + 1]) if not (r0 <= col[p] < r1))
+                          for g in order[nin:]])
+            new[bi] = np.linalg.solve(U[nin:, nin:], zf[bi][nin:] - np.linalg.solve(L[nin:, nin:], c))
+        xs = new
+    z = np.zeros(N)
+    for bi, (r0, r1, order, nin, L, U) in enumerate(blocks):
+        xb = np.linalg.solve(U[:nin, :nin], zf[bi][:nin] - U[:nin, nin:] @ xs[bi])
+        z[np.array(order, int)] = np.concatenate([xb, xs[bi]])
+    zo = o.psolve(r)
+    assert np.abs(zo - z).max() <= 1e-10 * np.abs(z).max()
+    if iters == 0:
+        # no interface iteration: the block-Jacobi apply in the new order
+        o.set_schur(-1)
+        factor_given(o, val, nb)
+        zj = o.psolve(r)
+        assert np.abs(zo - zj).max() > 0.0   # a different row order, a different ILU(0)
+    o.set_schur(-1)
+
+
+def test_schur_apply_converges_to_the_coupled_preconditioner(p2):
+    # With many interface sweeps the apply solves M x = r for
+    # M = (block factors L U) + C_o: the blocks coupled through their
+    # interface rows, the local Schur complements by ILU(0)
+    o = Oracle(p2)
+    y, yp = setup_state(p2, 11)
+    F0 = o.residual(0.0, y, yp)
+    ewt = 1.0 / (1e-6 * np.abs(y) + 1e-6)
+    nb = 4
+    assert o.psetup(0.0, 1e-2, 1e2, y, yp, F0, ewt, nb) == 0
+    rp, col, val, _ = o.jacobian()
+    N = p2.n_nodes
+    blocks = _schur_blocks(rp, col, val, N, nb)
+    M = np.zeros((N, N))
+    for r0, r1, order, nin, L, U in blocks:
+        idx = np.array(order, int)
+        M[np.ix_(idx, idx)] = L @ U
+        for g in order[nin:]:
+            for p in range(rp[g], rp[g + 1]):
+                if not (r0 <= col[p] < r1):
+                    M[g, col[p]] = val[p]
+    r = np.random.default_rng(12).standard_normal(N)
+    zx = np.linalg.solve(M, r)
+    o.set_schur(60)
+    factor_given(o, val, nb)
+    z = o.psolve(r)
+    o.set_schur(-1)
+    assert np.abs(z - zx).max() <= 1e-8 * np.abs(zx).max()
+
+
 def test_block_ilu_given_matrix_is_deterministic(p2):
     o = Oracle(p2)
     y, yp = setup_state(p2, 5)
