@@ -109,7 +109,7 @@ class Opts(C.Structure):
                 ("krylov_dim", C.c_int), ("max_restarts", C.c_int), ("precision", C.c_int),
                 ("use_predictor", C.c_int), ("h0", C.c_double), ("hmax", C.c_double),
                 ("max_steps", C.c_long), ("eps_lin", C.c_double), ("cj_refresh", C.c_double),
-                ("psetup_age", C.c_int), ("krylov_operator", C.c_int)]
+                ("psetup_age", C.c_int), ("krylov_operator", C.c_int), ("graph", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -162,6 +162,8 @@ def _declare(L):
     L.fvm_set_members.argtypes = [_P, _I, _P]
     L.fvm_integrate_replay.argtypes = [_P, C.POINTER(Opts), _D, _P, _D, C.c_long, C.POINTER(StepRecord), _D,
                                        C.c_int, _P, C.POINTER(Stats)]
+    L.fvm_graph_counters.argtypes = [_P, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+    L.fvm_integrate_batch.argtypes = [_P, _I, C.POINTER(Opts), _D, _D, _P, _P, _P, _P, _I]
     L.fvm_step_trace.restype = C.c_long
     L.fvm_step_trace.argtypes = [_P, C.POINTER(StepRecord), C.c_long]
     L.fvm_pmesh_read.argtypes = [C.c_char_p, _I, C.POINTER(PmeshStruct)]
@@ -326,13 +328,25 @@ class Problem:
     def member(self, m):
         """member m of an ensemble problem as a standalone problem"""
         a, b = int(self.member_ptr[m]), int(self.member_ptr[m + 1])
-        arr = self.arrays()
+        if getattr(self, "_member_index", None) is None:
+            # once per problem: the arrays and, per member, its elements and
+            # boundary faces (members never share either)
+            arr = self.arrays()
+            nm = len(self.member_ptr) - 1
+            eown = np.searchsorted(self.member_ptr, arr["elem_nodes"][:, 0], side="right") - 1
+            bown = np.searchsorted(self.member_ptr, arr["bface_nodes"][:, 0], side="right") - 1
+            eord = np.argsort(eown, kind="stable")
+            bord = np.argsort(bown, kind="stable")
+            eptr = np.searchsorted(eown[eord], np.arange(nm + 1))
+            bptr = np.searchsorted(bown[bord], np.arange(nm + 1))
+            self._member_index = (arr, eord, eptr, bord, bptr)
+        arr, eord, eptr, bord, bptr = self._member_index
         d = self.mesh.dim
         en = arr["elem_nodes"]
-        sel = (en[:, 0] >= a) & (en[:, 0] < b)
-        eidx = np.nonzero(sel)[0]
+        eidx = eord[eptr[m]:eptr[m + 1]]
+        sel = eidx
         bf = arr["bface_nodes"]
-        bsel = (bf[:, 0] >= a) & (bf[:, 0] < b)
+        bsel = bord[bptr[m]:bptr[m + 1]]
         be = np.ctypeslib.as_array(self.mesh.bface_elem, (self.mesh.n_bfaces,))[bsel]
         emap = np.full(self.n_elements, -1, np.int64)
         emap[eidx] = np.arange(len(eidx))
@@ -522,6 +536,23 @@ class Preconditioner:
                             max_restarts, precision, tol, C.byref(its), C.byref(rn))
         _check(r, "fvm_gmres")
         return r, its.value, rn.value
+
+
+def integrate_batch(physics_list, t0, t_end, y0_list, y_end_list, n_threads=8, **opts):
+    """independent problems, one Physics context each, integrated
+    concurrently with their own step sequences (fvm_integrate_batch);
+    returns (rc, per-member status codes, per-member stats dicts)"""
+    n = len(physics_list)
+    o = default_opts(**opts)
+    ctxs = (C.c_void_p * n)(*[ph._c for ph in physics_list])
+    y0s = (C.c_void_p * n)(*[_ptr(v) for v in y0_list])
+    yes = (C.c_void_p * n)(*[_ptr(v) for v in y_end_list])
+    st = (Stats * n)()
+    status = (C.c_int * n)()
+    rc = lib().fvm_integrate_batch(ctxs, n, C.byref(o), t0, t_end, y0s, yes, st, status, n_threads)
+    if rc < 0:
+        raise _err("fvm_integrate_batch", rc)
+    return rc, [int(x) for x in status], [s_.as_dict() for s_ in st]
 
 
 def default_opts(**kw) -> Opts:

@@ -11,9 +11,12 @@
 #include "reduce.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <thread>
+#include <vector>
 
 namespace fvmb {
 
@@ -331,7 +334,11 @@ struct DeviceOps {
             tol_scale = std::sqrt((double)std::max(nmin, 1) / N);
         }
         counter.zero(c->stream);
+        c->use_graph = o.graph != 0;
     }
+    ~DeviceOps() { c->use_graph = false; }
+    DeviceOps(const DeviceOps&) = delete;
+    DeviceOps& operator=(const DeviceOps&) = delete;
     // largest per-member WRMS norm from per-member squared sums
     // host[off + m*nq + q]
     double member_max_at(size_t off, int nq, int q) const {
@@ -704,6 +711,59 @@ extern "C" int fvm_integrate(fvm_ctx* c, const fvm_opts* opts, double t0, double
         FVM_CUDA(cudaGetLastError());
         if (rc < 0) set_error("fvm_integrate: step failure code " + std::to_string(rc));
         return rc;
+    } catch (const Error& ex) {
+        set_error(ex.what());
+        return ex.code;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+// Independent problems (ensemble members), each in its own context, each
+// with its own step-size and order sequence: n_threads host threads take
+// the contexts in turn (largest first when the caller sorts them), so the
+// members' kernels overlap on the device through their own streams.  A
+// member that fails stops alone; status[i] is its fvm_integrate code.
+extern "C" int fvm_integrate_batch(fvm_ctx* const* ctxs, int n, const fvm_opts* opts, double t0, double t_end,
+                                   const double* const* y0, double* const* y_end, fvm_stats* stats, int* status,
+                                   int n_threads) {
+    try {
+        if (!ctxs || !opts || !y0 || !y_end || !status || n < 1) throw Error("fvm_integrate_batch: bad argument");
+        for (int i = 0; i < n; ++i)
+            if (!ctxs[i] || !y0[i] || !y_end[i]) throw Error("fvm_integrate_batch: null context or vector");
+        const int nt = std::max(1, std::min(n_threads, n));
+        std::atomic<int> next{0};
+        std::vector<std::string> errs(n);
+        auto work = [&]() {
+            for (;;) {
+                const int i = next.fetch_add(1);
+                if (i >= n) return;
+                fvm_ctx* c = ctxs[i];
+                try {
+                    FVM_CUDA(cudaSetDevice(c->device));
+                    status[i] = integrate_dev(c, opts, t0, t_end, y0[i], y_end[i], stats ? stats + i : nullptr);
+                    FVM_CUDA(cudaGetLastError());
+                } catch (const Error& ex) {
+                    status[i] = ex.code;
+                    errs[i] = ex.what();
+                } catch (const std::exception& ex) {
+                    status[i] = -1;
+                    errs[i] = ex.what();
+                }
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int k = 1; k < nt; ++k) pool.emplace_back(work);
+        work();
+        for (auto& th : pool) th.join();
+        int worst = 0, first_bad = -1;
+        for (int i = 0; i < n; ++i)
+            if (status[i] < 0 && first_bad < 0) { first_bad = i; worst = status[i]; }
+        if (first_bad >= 0)
+            set_error("fvm_integrate_batch: member " + std::to_string(first_bad) + " failed with code " +
+                      std::to_string(worst) + (errs[first_bad].empty() ? "" : ": " + errs[first_bad]));
+        return first_bad >= 0 ? 1 : 0;
     } catch (const Error& ex) {
         set_error(ex.what());
         return ex.code;

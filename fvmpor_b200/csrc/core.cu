@@ -72,7 +72,7 @@ __global__ void k_node(int N, const double* __restrict__ y, const double* __rest
         double sg = pt.sigma_dev ? *pt.sigma_dev : pt.sigma;
         double p = sg * pt.v[i];
         h = h + p;
-        hp = hp + pt.cj * p;
+        hp = hp + (pt.cj_dev ? *pt.cj_dev : pt.cj) * p;
         hstar[i] = h;
     } else if (pt.mode == 2) {
         if (pt.colour[i] == pt.c) {
@@ -381,6 +381,44 @@ __global__ void k_faceq(int T, int N, const int4* __restrict__ en, const double*
     }
 }
 
+// The same face fluxes for the rebuilt-geometry 3D variant: the face
+// geometry from the element's vertices (tet_face_fluxes, the quantity
+// sum_k C[f][k] h_k + G[f] with the head gradient formed once), so that the
+// step's upwinding reads the vertices and one K instead of 30 stored
+// coefficients per element (the element pass of this variant does the same)
+template <bool MULTIZONE>
+__global__ void k_faceq_rc(int T, int N, const int4* __restrict__ en, const double* __restrict__ xyz,
+                           const double* __restrict__ eK, int kiso, int estride, const int* __restrict__ ezone,
+                           const double* __restrict__ krw, const double* __restrict__ h,
+                           const unsigned char* __restrict__ flip, double* __restrict__ faceq) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= T) return;
+    const int4 nd = en[e];
+    const int ids[4] = {nd.x, nd.y, nd.z, nd.w};
+    const size_t zo = MULTIZONE ? (size_t)ezone[e] * N : 0;
+    double X[4][3], hv[4], kr[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        X[k][0] = xyz[ids[k]];
+        X[k][1] = xyz[(size_t)N + ids[k]];
+        X[k][2] = xyz[(size_t)2 * N + ids[k]];
+        hv[k] = h[ids[k]];
+        kr[k] = krw[zo + ids[k]];
+    }
+    double Kx, Ky, Kz;
+    if (kiso) Kx = Ky = Kz = eK[e];
+    else { Kx = eK[e]; Ky = eK[(size_t)estride + e]; Kz = eK[(size_t)2 * estride + e]; }
+    double q[6];
+    tet_face_fluxes(X[0], X[1], X[2], X[3], Kx, Ky, Kz, hv[0], hv[1], hv[2], hv[3], q);
+    const unsigned fl = flip[e];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const double kf = kr[tet_edge_a(f)] * 0.5 + kr[tet_edge_b(f)] * 0.5;
+        const double qn = q[f] * kf;
+        faceq[(size_t)6 * e + f] = ((fl >> f) & 1u) ? qn : -qn;
+    }
+}
+
 // per edge: edge_flux = sum_j (1/A_edge) qdotn_j; upwind = front when the
 // edge flux is negative, back otherwise (process_spatial_weights,
 // fvmpor.h:765, 784-793).  Writes the per-face flag in element-local terms.
@@ -614,7 +652,14 @@ void launch_begin_step(fvm_ctx* c, const double* y, const double* yp) {
                                                       c->nz_zone.p, c->nz_w.p, c->rho0, c->krw.p,
                                                       c->hstar.p, c->stor.p, node_copies(c));
     int gb = grid_for(c->T, kBlock);
-    if (c->dim == 3) {
+    if (c->dim == 3 && c->recompute) {
+        if (c->nz > 1)
+            fvm_launch(c, k_faceq_rc<true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->xyz.p, c->eK.p,
+                       c->kiso ? 1 : 0, c->estride, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
+        else
+            fvm_launch(c, k_faceq_rc<false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->xyz.p, c->eK.p,
+                       c->kiso ? 1 : 0, c->estride, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
+    } else if (c->dim == 3) {
         if (c->nz > 1) fvm_launch(c, k_faceq<4, 6, true>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
         else fvm_launch(c, k_faceq<4, 6, false>, gb, kBlock, 0, s, c->T, c->N, c->enodes.p, c->coef.p, c->ezone.p, c->krw.p, y, c->flip.p, c->faceq.p);
     } else {
@@ -1177,6 +1222,13 @@ extern "C" int fvm_profile_read(fvm_ctx* c, double* ms, long* counts) {
     }
     return 0;
     FVM_API_END
+}
+
+extern "C" int fvm_graph_counters(fvm_ctx* c, long* captures, long* replays) {
+    if (!c) return -1;
+    if (captures) *captures = c->graph_captures;
+    if (replays) *replays = c->graph_replays;
+    return 0;
 }
 
 extern "C" int fvm_counters(fvm_ctx* c, long* launches, long* residuals) {

@@ -114,6 +114,7 @@ struct Perturb {
     int c = 0;                       // mode 2: active colour
     const int* skip = nullptr;       // when set and *skip != 0 the evaluation is skipped
                                      // (a device-driven loop that has already finished)
+    const double* cj_dev = nullptr;  // mode 1: device-resident cj (overrides cj; graph replays)
 };
 
 // Node gather of the residual chain: the sum of a node's per-chunk element
@@ -246,6 +247,9 @@ struct fvm_ctx {
     long n_residuals = 0;
     long launches = 0;               // kernels launched on this context
     long n_syncs = 0;                // host waits on the context's stream (ctx_sync)
+    bool graph_ok = true;            // cleared when a batch capture failed: launch directly
+    bool use_graph = false;          // the running integration asked for CUDA-graph batches
+    long graph_captures = 0, graph_replays = 0;   // CUDA-graph batches of the Arnoldi loop
     fvmb::KernelTimer tm;
     std::string err;
 };

@@ -39,6 +39,15 @@ struct Krylov {
     DevBuf<double> ls;        // H [(m+1) x m], cs [m], sn [m], g [m+1]
     double* host = nullptr;   // pinned
     double* host_ls = nullptr;   // pinned: H and g of a fused cycle
+    // CUDA graph of one full batch (8 steps) of the device-driven Arnoldi
+    // loop (fvm_opts.graph): captured for one key (operator, precision,
+    // vectors, preconditioner state), replayed for every full batch; cj and
+    // the operator's cj shift come from cjd, written before each batch
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    size_t gkey = 0;
+    long g_launches = 0, g_residuals = 0;   // launches and residuals one replay runs
+    DevBuf<double> cjd;       // [0] cj, [1] cj - cj of the set-up
 };
 
 struct GmresCounters {
@@ -66,7 +75,11 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
 void psolve_dev(fvm_ctx* c, const double* r, double* z, const int* skip = nullptr);
 // y = J(cj) x with the assembled difference-quotient Jacobian of the last
 // set-up (the Krylov operator of fvm_opts.krylov_operator = 1)
-void jacobian_apply(fvm_ctx* c, double cj, const double* x, double* y, const int* skip = nullptr);
+void jacobian_apply(fvm_ctx* c, double cj, const double* x, double* y, const int* skip = nullptr,
+                    const double* dcj_dev = nullptr);
+double jacobian_cj_setup(fvm_ctx* c);   // cj of the last set-up
+int ilu_factored(fvm_ctx* c);           // precision of the current factor, -1 none
+bool schur_active(fvm_ctx* c);          // the Schur-coupled apply is on
 // fused Arnoldi cycle of the assembled operator (arnoldi_fused.cu):
 // fused_prepare refreshes the operator after a set-up and tells whether the
 // cycle can run (FP32 factor staged in shared memory, every block resident);

@@ -425,6 +425,8 @@ Krylov* krylov_get(fvm_ctx* c, int m, int precision) {
 
 void fvmb_destroy_krylov_impl(Krylov* K) {
     if (!K) return;
+    if (K->gexec) cudaGraphExecDestroy(K->gexec);
+    if (K->graph) cudaGraphDestroy(K->graph);
     if (K->U) cudaFree(K->U);
     if (K->host) cudaFreeHost(K->host);
     if (K->host_ls) cudaFreeHost(K->host_ls);
@@ -463,6 +465,11 @@ static void jv_dev(fvm_ctx* c, Krylov* K, double cj, const double* y, const doub
     pt.v = v;
     pt.sigma_dev = K->sigma.p;
     launch_residual(c, y, yp, pt, F0, out);
+}
+
+__global__ void k_set_cj(double* cjd, double cj, double dcj) {
+    cjd[0] = cj;
+    cjd[1] = dcj;
 }
 
 template <class B>
@@ -565,6 +572,14 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
             FVM_CUDA(cudaMemcpyAsync(g_d, g.data(), sizeof(double) * (m + 1), cudaMemcpyHostToDevice, s));
             const int* skip = &K->st.p->done;
             int queued = 0;
+            // full batches from a CUDA graph (fvm_opts.graph): cj and the
+            // operator's cj shift come from device memory so that one
+            // capture serves every Newton solve with the same vectors
+            const bool graph = c->use_graph && c->graph_ok && !c->tm.on && !schur_active(c);
+            if (graph) {
+                if (K->cjd.n < 2) K->cjd.alloc(2);
+                fvm_launch(c, k_set_cj, 1, 1, 0, s, K->cjd.p, cj, cj - jacobian_cj_setup(c));
+            }
             // first direction and its increment
             fvm_launch(c, k_unscale<B>, grid_for(N, 256), 256, 0, s, N, U, K->scale.p, 0, ewt, K->t.p);
             fvm_launch(c, k_sumsq, kRedBlocks, kRedThreads, 0, s, N, K->t.p, ewt, K->partial.p, K->counter.p,
@@ -576,14 +591,16 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                 // host round trip costs the GPU idle time (30-day 3D run:
                 // 771 ms with batches of 4, 764 ms with 8)
                 const int batch = std::min(m - queued, queued < 2 ? 2 : 8);
-                for (int q = 0; q < batch; ++q) {
+                auto enqueue = [&](int nsteps, bool dev_cj) {
+                for (int q = 0; q < nsteps; ++q) {
                     Perturb pt;
                     pt.mode = 1;
                     pt.cj = cj;
+                    pt.cj_dev = dev_cj ? K->cjd.p : nullptr;
                     pt.v = K->t.p;
                     pt.sigma_dev = K->sigma.p;
                     pt.skip = skip;
-                    if (op) jacobian_apply(c, cj, K->t.p, K->Jv.p, skip);
+                    if (op) jacobian_apply(c, cj, K->t.p, K->Jv.p, skip, dev_cj ? K->cjd.p + 1 : nullptr);
                     else launch_residual(c, y, yp, pt, F0, K->Jv.p);
                     psolve_dev(c, K->Jv.p, K->z.p, skip);
                     c->tm.begin(TM_CGS, s);
@@ -619,6 +636,61 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
                                                 (const double*)ew, Wp, pp, bp, ep, tp, sgp, H_d, cs_d, sn_d, g_d));
                     c->launches++;
                     c->tm.end(TM_CGS, s);
+                }
+                };
+                if (graph && batch == 8) {
+                    // the key: everything a captured launch bakes in
+                    size_t key = 1469598103934665603ull;
+                    auto mix = [&](size_t v) { key = (key ^ v) * 1099511628211ull; };
+                    mix((size_t)op); mix((size_t)y); mix((size_t)yp); mix((size_t)F0); mix((size_t)ewt);
+                    mix((size_t)c->ilu); mix((size_t)(ilu_factored(c) + 2)); mix((size_t)c->chunk_e);
+                    mix((size_t)c->recompute); mix((size_t)K->coop_grid);
+                    bool ready = K->gexec && K->gkey == key;
+                    if (!ready) {
+                        const long l0 = c->launches, r0 = c->n_residuals;
+                        cudaGraph_t g = nullptr;
+                        bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                        if (ok) {
+                            try {
+                                enqueue(8, true);
+                            } catch (...) {
+                                ok = false;
+                            }
+                            ok = cudaStreamEndCapture(s, &g) == cudaSuccess && ok && g;
+                        }
+                        K->g_launches = c->launches - l0;
+                        K->g_residuals = c->n_residuals - r0;
+                        c->launches = l0;
+                        c->n_residuals = r0;
+                        if (ok) {
+                            if (K->gexec) cudaGraphExecDestroy(K->gexec);
+                            K->gexec = nullptr;
+                            ok = cudaGraphInstantiate(&K->gexec, g, 0) == cudaSuccess;
+                        }
+                        if (K->graph) cudaGraphDestroy(K->graph);
+                        K->graph = g;
+                        if (!ok) {
+                            // launch directly from now on
+                            cudaGetLastError();
+                            c->graph_ok = false;
+                            if (K->gexec) cudaGraphExecDestroy(K->gexec);
+                            K->gexec = nullptr;
+                        } else {
+                            K->gkey = key;
+                            c->graph_captures++;
+                        }
+                        ready = ok;
+                    }
+                    if (ready) {
+                        FVM_CUDA(cudaGraphLaunch(K->gexec, s));
+                        c->graph_replays++;
+                        c->launches += K->g_launches;
+                        c->n_residuals += K->g_residuals;
+                    } else {
+                        enqueue(batch, false);
+                    }
+                } else {
+                    enqueue(batch, false);
                 }
                 queued += batch;
                 int* herr = reinterpret_cast<int*>(K->host + 4 * (m + 2) + 7);

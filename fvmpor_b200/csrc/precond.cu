@@ -102,9 +102,11 @@ __global__ void k_fd_node(int N, const double* __restrict__ y, const double* __r
 __global__ void k_jac_apply(int N, const int* __restrict__ rowptr, const int* __restrict__ col,
                             const double* __restrict__ J, const double* __restrict__ ahhp,
                             const unsigned char* __restrict__ ntype, double dcj, const double* __restrict__ x,
-                            double* __restrict__ y, const int* __restrict__ skip) {
+                            double* __restrict__ y, const int* __restrict__ skip,
+                            const double* __restrict__ dcj_dev) {
     pdl_wait_and_trigger();
     if (skip && *skip) return;
+    if (dcj_dev) dcj = *dcj_dev;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = g >> 2, lane = g & 3;
     if (i >= N) return;
@@ -1155,12 +1157,16 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
     P->factored = precision;
 }
 
-void jacobian_apply(fvm_ctx* c, double cj, const double* x, double* y, const int* skip) {
+void jacobian_apply(fvm_ctx* c, double cj, const double* x, double* y, const int* skip, const double* dcj_dev) {
     BlockILU* P = c->ilu;
     if (!P || P->factored < 0) throw Error("jacobian_apply: preconditioner not set up");
     fvm_launch_pdl(c, k_jac_apply, grid_for(4L * c->N, 256), 256, 0, c->stream, c->N, P->rowptr.p, P->col.p,
-                   P->J.p, P->ahhp.p, c->ntype.p, cj - P->cj_setup, x, y, skip);
+                   P->J.p, P->ahhp.p, c->ntype.p, cj - P->cj_setup, x, y, skip, dcj_dev);
 }
+
+double jacobian_cj_setup(fvm_ctx* c) { return c->ilu ? c->ilu->cj_setup : 0.0; }
+int ilu_factored(fvm_ctx* c) { return c->ilu ? c->ilu->factored : -1; }
+bool schur_active(fvm_ctx* c) { return c->ilu && c->ilu->schur_iters >= 0; }
 
 int ilu_status(fvm_ctx* c) {
     if (!c->ilu || !c->ilu->h_status) return 0;

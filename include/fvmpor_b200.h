@@ -313,6 +313,13 @@ typedef struct {
                                 difference-quotient Jacobian, shifted
                                 exactly to the current cj (the residual,
                                 Newton update and tests stay FP64)        */
+    int graph;               /* 1: the device-driven Arnoldi loop runs its
+                                full batches (8 steps of the separate
+                                kernels: J v, apply, orthogonalisation)
+                                from one CUDA graph per operator and
+                                vector set, instead of 40 launches; no
+                                effect on the fused cycle (one launch per
+                                GMRES cycle already)                     */
 } fvm_opts;
 
 typedef struct {
@@ -395,6 +402,27 @@ int fvm_integrate_outputs(fvm_ctx* ctx, const fvm_opts* opts, double t0,
  * Returns 0, 1 when some corrector stopped at max_newton (the run still
  * completes), < 0 on failure.  No counterpart in the reference: IDAS has no
  * replay mode (the step loop it replaces is ida_integrator.h:296-321). */
+/* CUDA-graph batches of the Arnoldi loop run on this context so far
+ * (fvm_opts.graph): graphs captured and batches replayed from them.  Either
+ * pointer may be NULL. */
+int fvm_graph_counters(fvm_ctx* ctx, long* captures, long* replays);
+
+/* Independent problems, one context each (for example the members of an
+ * ensemble, each with its own mesh and Ks field), integrated from t0 to
+ * t_end with one step-size and order sequence per member: n_threads host
+ * threads take the contexts in turn, and the members' kernels overlap on
+ * the device through their own streams.  y0[i], y_end[i] are device
+ * vectors of context i; stats (may be NULL) and status have n entries;
+ * status[i] is what fvm_integrate would return for member i, and a member
+ * that fails stops alone.  Returns 0 when every member reached t_end, 1
+ * when some did not (the first failure in fvm_last_error()), < 0 on a bad
+ * call.  The reference runs one mesh per process
+ * (examples/fvmporMinlin/fvmpor_ODE.cpp:75-266). */
+int fvm_integrate_batch(fvm_ctx* const* ctxs, int n, const fvm_opts* opts,
+                        double t0, double t_end, const double* const* y0,
+                        double* const* y_end, fvm_stats* stats, int* status,
+                        int n_threads);
+
 int fvm_integrate_replay(fvm_ctx* ctx, const fvm_opts* opts, double t0,
                          const double* y0, double h0, long n_steps,
                          const fvm_step_record* steps, double newton_tol,

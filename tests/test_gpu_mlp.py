@@ -129,3 +129,23 @@ def test_learned_iterate_in_the_integrator(cuda):
             "newton_per_step_learned": st2["nni"] / st2["nst"], "newton_per_step_plain": st["nni"] / st["nst"]}
     print("learned-iterate gain", gain)
     assert gain["krylov_per_newton_learned"] < 1.5 * gain["krylov_per_newton_plain"]
+    # replay A/B: the learned run's accepted steps replayed with the learned
+    # start tried on every step and without it, each corrector solved to
+    # ||delta|| <= 1e-4; both must reach the same state (the learned start
+    # only moves where Newton begins), and the trace must mark the kept starts
+    h0 = float(tr["h"][0])
+    ys = {}
+    work = {}
+    for up in (0, 2):
+        rep = fb.Integrator(ph, krylov_dim=20, use_predictor=up)
+        yr = torch.empty_like(y0)
+        rc, st3 = rep.replay(0.0, y0, h0, tr, yr, newton_tol=1e-4)
+        assert rc == 0
+        rt = rep.trace()
+        assert int(rt["learned"].sum()) == st3["npred"]
+        if up == 0:
+            assert st3["npred"] == 0
+        ys[up] = yr
+        work[up] = {"krylov": st3["nli"], "newton": st3["nni"], "kept": st3["npred"]}
+    print("replay A/B (plain, learned on every step)", work)
+    assert (ys[0] - ys[2]).abs().max().item() < 1e-6 * span
