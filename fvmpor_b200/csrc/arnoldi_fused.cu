@@ -99,7 +99,6 @@ constexpr int kFusedThreads = 384;
 template <int KM>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a) {
     __shared__ double ca[64], cb[64], coef[64], sc[64], rc[64], rs[64], gs[64];
-    __shared__ double dred[kFusedThreads / 32];   // split-warp partial dots (block_dots_by_warp)
     __shared__ int s_done;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int b = blockIdx.x, nblk = gridDim.x;
@@ -204,7 +203,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         for (int k = threadIdx.x; k < nr; k += blockDim.x) Ws[k] = a.ewt[r0 + k] * (double)x[inv[k]];
         __syncthreads();
         // pass 1: a = U^T W
-        block_dots_by_warp(a.U, a.ld, Ws, r0, r1, nv, false, ca, dred);
+        block_dots_by_warp(a.U, a.ld, Ws, r0, r1, nv, false, ca);
         for (int i = threadIdx.x; i < nv; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
         if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
         block_reduce_all_vmajor(pa, nv, nblk, ca);
@@ -219,7 +218,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
                 if (r + e >= r0 && r + e < r1) Ws[r + e - r0] -= acc[e];
         }
         __syncthreads();
-        block_dots_by_warp(a.U, a.ld, Ws, r0, r1, nv, true, cb, dred);
+        block_dots_by_warp(a.U, a.ld, Ws, r0, r1, nv, true, cb);
         for (int i = threadIdx.x; i <= nv; i += blockDim.x) pb[(size_t)i * nblk + b] = cb[i];
         if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
         block_reduce_all_vmajor(pb, nv + 1, nblk, cb);

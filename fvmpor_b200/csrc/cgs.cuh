@@ -234,35 +234,27 @@ __device__ __forceinline__ void quad_combine(const BasisRows<B, CG>& U, const do
 // tree.  No block-wide reduction is needed, so vectors finish
 // independently.  out[i] is valid in every thread after the call.  Rows of
 // the edge quads outside [k0, k1) enter as zeros.
-// With fewer vectors than warps (the first steps of a cycle) each vector
-// gets g = nw / nvec warps, which take interleaved groups of the quads, so
-// the block keeps all its warps' loads in flight; the g partial sums of a
-// vector are added in warp order (red: nw doubles of shared memory).
 __device__ __forceinline__ void block_dots_by_warp(const float* __restrict__ U, size_t ld,
                                                    const double* __restrict__ Wl, int k0, int k1, int nv,
-                                                   bool with_norm, double* out, double* red) {
+                                                   bool with_norm, double* out) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int a0 = k0 & ~3;
     const int nq = (k1 - a0 + 3) >> 2;
     const int nvec = nv + (with_norm ? 1 : 0);
-    const int g = nvec < nw ? nw / nvec : 1;   // warps per vector
-    const int nslot = g > 1 ? nvec * g : nw;   // warps in use with g > 1
-    for (int w0 = warp; w0 < (g > 1 ? nslot : nvec); w0 += nw) {
-        const int i = g > 1 ? w0 / g : w0;
-        const int sub = g > 1 ? w0 - i * g : 0;
+    for (int i = warp; i < nvec; i += nw) {
         double acc = 0.0;
         const float* Ui = U + ld * (i < nv ? i : 0);
-        for (int q0 = 32 * sub + lane; q0 < nq; q0 += 32 * 8 * g) {
+        for (int q0 = lane; q0 < nq; q0 += 32 * 8) {
             float4 u[8];
 #pragma unroll
             for (int t = 0; t < 8; ++t) {
-                const int q = q0 + 32 * g * t;
+                const int q = q0 + 32 * t;
                 u[t] = (i < nv && q < nq) ? __ldg(reinterpret_cast<const float4*>(Ui + a0 + 4 * q))
                                           : make_float4(0.f, 0.f, 0.f, 0.f);
             }
 #pragma unroll
             for (int t = 0; t < 8; ++t) {
-                const int q = q0 + 32 * g * t;
+                const int q = q0 + 32 * t;
                 if (q >= nq) continue;
                 const int r = a0 + 4 * q;
                 double w[4];
@@ -276,18 +268,7 @@ __device__ __forceinline__ void block_dots_by_warp(const float* __restrict__ U, 
             }
         }
         acc = warp_sum(acc);
-        if (lane == 0) {
-            if (g > 1) red[w0] = acc;
-            else out[i] = acc;
-        }
-    }
-    if (g > 1) {
-        __syncthreads();
-        for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
-            double t = 0.0;
-            for (int k = 0; k < g; ++k) t += red[i * g + k];
-            out[i] = t;
-        }
+        if (lane == 0) out[i] = acc;
     }
     __syncthreads();
 }
