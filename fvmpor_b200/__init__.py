@@ -162,6 +162,7 @@ def _declare(L):
     L.fvm_set_members.argtypes = [_P, _I, _P]
     L.fvm_integrate_replay.argtypes = [_P, C.POINTER(Opts), _D, _P, _D, C.c_long, C.POINTER(StepRecord), _D,
                                        C.c_int, _P, C.POINTER(Stats)]
+    L.fvm_set_krylov_variant.argtypes = [_P, _I]
     L.fvm_graph_counters.argtypes = [_P, C.POINTER(C.c_long), C.POINTER(C.c_long)]
     L.fvm_integrate_batch.argtypes = [_P, _I, C.POINTER(Opts), _D, _D, _P, _P, _P, _P, _I]
     L.fvm_step_trace.restype = C.c_long

@@ -96,9 +96,14 @@ __device__ __forceinline__ void named_barrier(int id, int count) {
 // loop), so a thread may hold up to 170 registers
 constexpr int kFusedThreads = 384;
 
-template <int KM>
+template <int KM, bool DEL>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a) {
-    __shared__ double ca[64], cb[64], coef[64], sc[64], rc[64], rs[64], gs[64];
+    // ca holds up to 2 (m + 1) + 2 reduced numbers on the delayed variant
+    __shared__ double ca[DEL ? 132 : 64], cb[64], coef[64], sc[64], rc[64], rs[64], gs[64];
+    // delayed variant: first projection of the pending column, t, p, H t and
+    // the two combine coefficient sets
+    __shared__ double hp[DEL ? 64 : 1], tv[DEL ? 64 : 1], pv[DEL ? 64 : 1], htv[DEL ? 64 : 1],
+        c1[DEL ? 64 : 1], c2[DEL ? 64 : 1];
     __shared__ int s_done;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int b = blockIdx.x, nblk = gridDim.x;
@@ -121,6 +126,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     unsigned short* inv = reinterpret_cast<unsigned short*>(smem_raw + a.stage_max);
     double* Ws = reinterpret_cast<double*>(smem_raw + a.stage_max + round16(2 * (size_t)a.nr_max));
     float* tl = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(Ws) + 8 * (size_t)a.nr_max);
+    // delayed variant: the block's rows of the pending vector v_k, then the
+    // unrotated Hessenberg matrix (column c at Hs[64 c ..])
+    double* Vs = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(tl) + round16(4 * (size_t)a.nh_max));
+    double* Hs = Vs + a.nr_max;
     if (threadIdx.x == 0) {
         tc05::mbar_init(mbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;");
@@ -163,6 +172,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     const int nb0 = a.nbr_ptr[b], nb1 = a.nbr_ptr[b + 1];
     // step 0's direction was written before the launch
     for (int k = threadIdx.x; k < nh; k += blockDim.x) tl[k] = __ldcg(a.tdir + a.halo_node[h0 + k]);
+    if constexpr (DEL)
+        for (int k = threadIdx.x; k < nr; k += blockDim.x) Vs[k] = 0.0;
     __syncthreads();
     for (int j = 0;; ++j) {
         const int nv = j + 1;
@@ -202,6 +213,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         ilu_sweep<float, KM, true>(x, val, col, rp, dg, urow, uptr, 0, nu);
         for (int k = threadIdx.x; k < nr; k += blockDim.x) Ws[k] = a.ewt[r0 + k] * (double)x[inv[k]];
         __syncthreads();
+        // Hessenberg column finalised by this step (-1: none yet), the entry
+        // below its diagonal, and the scale of the basis vector it finalises
+        int hcol = j;
+        double hn = 0.0;
+        double newscale = 0.0;
+        if constexpr (!DEL) {
         // pass 1: a = U^T W
         block_dots_by_warp(a.U, a.ld, Ws, r0, r1, nv, false, ca);
         for (int i = threadIdx.x; i < nv; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
@@ -247,22 +264,121 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
                 }
             }
         }
+        // the Hessenberg column of the two projections
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) ca[i] = sc[i] * (ca[i] + cb[i]);
+        hn = sqrt(nrm2);
+        newscale = snv;
+        } else {
+        // Delayed reorthogonalisation (DCGS2: Swirydowicz, Langou, Ananthan,
+        // Yang & Thomas, Numer. Linear Algebra Appl. 28 (2021) e2343).  The
+        // step's direction is v_k, the previous step's vector after one
+        // projection; z = A v_k.  One pass over the basis gives
+        // t = V^T v_k, p = V^T z, v_k.v_k and v_k.z, one grid barrier reduces
+        // them.  Then q_k = (v_k - V t) / beta with beta^2 = v.v - t.t
+        // finalises column k-1 of H (first projection of step k-1 plus t,
+        // and beta below it); A q_k = (z - V_k H t) / beta by the Arnoldi
+        // relation, so its first projection s and the next vector
+        // v_{k+1} = A q_k - V_k s follow from the reduced numbers, and one
+        // more pass over the basis writes both q_k (as U_k, scale 1/beta)
+        // and v_{k+1}.  Two passes and one barrier per step instead of
+        // four and two; the column of step k is final one step later.
+        const int k = j;
+        const int nbv = k == 0 ? 1 : k;   // basis vectors this step reads
+        block_dots2_by_warp(a.U, a.ld, Vs, Ws, r0, r1, nbv, ca);
+        const int nred = 2 * nbv + 2;
+        for (int i = threadIdx.x; i < nred; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
+        if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
+        block_reduce_all_vmajor(pa, nred, nblk, ca);
+        double beta = 1.0, ck = 0.0;
+        if (k == 0) {
+            // v_1 = z - V_0 p_0
+            if (threadIdx.x == 0) {
+                const double p0 = sc[0] * ca[1];
+                hp[0] = p0;
+                c1[0] = 0.0;
+                c2[0] = sc[0] * p0;
+            }
+            hcol = -1;
+        } else {
+            double tt = 0.0;
+            for (int i = 0; i < k; ++i) {
+                const double t = sc[i] * ca[i];
+                tt += t * t;
+            }
+            const double b2 = ca[2 * k] - tt;
+            beta = b2 > 0.0 ? sqrt(b2) : 0.0;
+            for (int i = threadIdx.x; i <= k; i += blockDim.x) {
+                const double t = i < k ? sc[i] * ca[i] : 0.0;
+                tv[i] = t;
+                pv[i] = i < k ? sc[i] * ca[k + i] : 0.0;
+                Hs[(size_t)(k - 1) * 64 + i] = i < k ? hp[i] + t : beta;
+            }
+            __syncthreads();
+            // Ht = H[0..k][0..k-1] t (H[i][c] is zero below c + 1)
+            for (int i = threadIdx.x; i <= k; i += blockDim.x) {
+                double acc = 0.0;
+                for (int c = i > 0 ? i - 1 : 0; c < k; ++c) acc += Hs[(size_t)c * 64 + i] * tv[c];
+                htv[i] = acc;
+            }
+            __syncthreads();
+            double tp = 0.0;
+            for (int i = 0; i < k; ++i) tp += tv[i] * pv[i];
+            const double rb = beta > 0.0 ? 1.0 / beta : 0.0;
+            const double sk = (ca[2 * k + 1] - tp - beta * htv[k]) * rb * rb;
+            ck = htv[k] * rb + sk;
+            for (int i = threadIdx.x; i < k; i += blockDim.x) {
+                const double si = (pv[i] - htv[i]) * rb;
+                c1[i] = sc[i] * tv[i];
+                c2[i] = sc[i] * (htv[i] * rb + si - ck * tv[i] * rb);
+                hp[i] = si;
+            }
+            if (threadIdx.x == 0) {
+                hp[k] = sk;
+                sc[k] = rb;
+            }
+            hcol = k - 1;
+            hn = beta;
+            newscale = rb;
+        }
+        __syncthreads();
+        // q_k = v_k - V t (k >= 1), v_{k+1} = z / beta - (c_k / beta) v_k - V c2,
+        // and the next direction D^-1 v_{k+1}
+        {
+            float* Uk = a.U + a.ld * k;
+            const double rb = k == 0 ? 1.0 : (beta > 0.0 ? 1.0 / beta : 0.0);
+            const double vcoef = k == 0 ? 0.0 : ck * rb;
+            for (int r = q0 + 4 * threadIdx.x; r < r1; r += 4 * blockDim.x) {
+                double acc1[4], acc2[4];
+                quad_combine2(UR, c1, c2, nbv, r, acc1, acc2);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int q = r + e;
+                    if (q >= r0 && q < r1) {
+                        const double vq = Vs[q - r0];
+                        if (k >= 1) Uk[q] = (float)(vq - acc1[e]);
+                        const double vn = Ws[q - r0] * rb - vcoef * vq - acc2[e];
+                        Vs[q - r0] = vn;
+                        a.tdir[q] = (float)(vn / a.ewt[q]);
+                    }
+                }
+            }
+        }
+        }
         // publish this block's rows of the next direction
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
             st_release_gpu(a.flags + b, (unsigned)nv);
         }
-        // Hessenberg column, rotations and stopping test, the same in every
-        // block (the same reduced numbers, the same operations), on thread
-        // 0 while the other warps wait for the next direction's rows this
-        // block reads (bounded) and gather them into shared memory
-        for (int i = threadIdx.x; i < nv; i += blockDim.x) ca[i] = sc[i] * (ca[i] + cb[i]);
         __syncthreads();
+        // rotations and stopping test for the finalised column, the same in
+        // every block (the same reduced numbers, the same operations), on
+        // thread 0 while the other warps wait for the next direction's rows
+        // this block reads (bounded) and gather them into shared memory
         if (warp > 0) {
             if (warp == 1) {
-                for (int k = nb0 + lane; k < nb1; k += 32) {
-                    const unsigned* f = a.flags + a.nbr[k];
+                for (int kk = nb0 + lane; kk < nb1; kk += 32) {
+                    const unsigned* f = a.flags + a.nbr[kk];
                     long it = 0;
                     while (ld_acquire_gpu(f) < (unsigned)nv) {
                         if (++it > (1l << 26)) { atomicExch(a.err, 3); break; }
@@ -270,46 +386,50 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
                 }
             }
             named_barrier(1, blockDim.x - 32);
-            for (int k = threadIdx.x - 32; k < nh; k += blockDim.x - 32)
-                tl[k] = __ldcg(a.tdir + a.halo_node[h0 + k]);
+            for (int kk = threadIdx.x - 32; kk < nh; kk += blockDim.x - 32)
+                tl[kk] = __ldcg(a.tdir + a.halo_node[h0 + kk]);
         } else if (threadIdx.x == 0) {
-            double* hc = ca;
-            const double hn = sqrt(nrm2);
-            hc[nv] = hn;
             int done = 0;
-            if (!isfinite(hn) || !isfinite(hc[j])) {
-                done = 3;
-            } else {
-                double cur = hc[0];
-                for (int i = 0; i < j; ++i) {
-                    const double nx = hc[i + 1];
-                    hc[i] = rc[i] * cur + rs[i] * nx;
-                    cur = -rs[i] * cur + rc[i] * nx;
+            if (hcol >= 0) {
+                double* hc = ca;
+                if constexpr (DEL) {
+                    for (int i = 0; i <= hcol; ++i) hc[i] = Hs[(size_t)hcol * 64 + i];
                 }
-                hc[j] = cur;
-                const double den = hypot(hc[j], hc[j + 1]);
-                double cj_, sj_;
-                if (den == 0.0) { cj_ = 1.0; sj_ = 0.0; }
-                else { cj_ = hc[j] / den; sj_ = hc[j + 1] / den; }
-                rc[j] = cj_;
-                rs[j] = sj_;
-                hc[j] = den;
-                const double gj = gs[j];
-                gs[j + 1] = -sj_ * gj;
-                gs[j] = cj_ * gj;
-                sc[nv] = snv;
-                const double rn = fabs(gs[j + 1]) / sqrtN;
-                if (rn <= tol || hn == 0.0) done = 1;
-                else if (j + 1 == m) done = 2;
-                if (b == 0) {
-                    for (int i = 0; i <= j; ++i) a.H[(size_t)i * m + j] = hc[i];
-                    a.cs[j] = cj_;
-                    a.sn[j] = sj_;
-                    a.g[j] = gs[j];
-                    a.g[j + 1] = gs[j + 1];
-                    a.scale[nv] = snv;
-                    a.st->rnorm = rn;
-                    a.st->j = j + 1;
+                hc[hcol + 1] = hn;
+                if (!isfinite(hn) || !isfinite(hc[hcol])) {
+                    done = 3;
+                } else {
+                    double cur = hc[0];
+                    for (int i = 0; i < hcol; ++i) {
+                        const double nx = hc[i + 1];
+                        hc[i] = rc[i] * cur + rs[i] * nx;
+                        cur = -rs[i] * cur + rc[i] * nx;
+                    }
+                    hc[hcol] = cur;
+                    const double den = hypot(hc[hcol], hc[hcol + 1]);
+                    double cj_, sj_;
+                    if (den == 0.0) { cj_ = 1.0; sj_ = 0.0; }
+                    else { cj_ = hc[hcol] / den; sj_ = hc[hcol + 1] / den; }
+                    rc[hcol] = cj_;
+                    rs[hcol] = sj_;
+                    hc[hcol] = den;
+                    const double gj = gs[hcol];
+                    gs[hcol + 1] = -sj_ * gj;
+                    gs[hcol] = cj_ * gj;
+                    sc[hcol + 1] = newscale;
+                    const double rn = fabs(gs[hcol + 1]) / sqrtN;
+                    if (rn <= tol || hn == 0.0) done = 1;
+                    else if (hcol + 1 == m) done = 2;
+                    if (b == 0) {
+                        for (int i = 0; i <= hcol; ++i) a.H[(size_t)i * m + hcol] = hc[i];
+                        a.cs[hcol] = cj_;
+                        a.sn[hcol] = sj_;
+                        a.g[hcol] = gs[hcol];
+                        a.g[hcol + 1] = gs[hcol + 1];
+                        a.scale[hcol + 1] = newscale;
+                        a.st->rnorm = rn;
+                        a.st->j = hcol + 1;
+                    }
                 }
             }
             if (b == 0) a.st->done = done;
@@ -326,6 +446,15 @@ __global__ void k_first_dir(int N, const float* __restrict__ U0, const double* _
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < N) t[k] = (float)(scale[0] * (double)U0[k] / ewt[k]);
 }
+
+static const void* fused_kernel(int lanes, int variant) {
+    if (lanes == 8) return variant ? (const void*)k_arnoldi_fused<8, true> : (const void*)k_arnoldi_fused<8, false>;
+    return variant ? (const void*)k_arnoldi_fused<4, true> : (const void*)k_arnoldi_fused<4, false>;
+}
+
+// Gram-Schmidt of the fused cycle on this context: 0 CGS2 (two projections,
+// two grid barriers per step), 1 delayed reorthogonalisation (DCGS2)
+static int fused_variant(const fvm_ctx* c) { return c->krylov_variant ? 1 : 0; }
 
 // values of the operator's slices from the set-up's Jacobian (FP64 CSR) and
 // the cj coefficient of its diagonal, in factor order
@@ -429,30 +558,39 @@ bool fused_prepare(fvm_ctx* c, int m) {
         P->fused_nrmax = nr_max;
         P->fused_nhmax = nh_max;
         P->fused_stage = round16(P->smem_stage[1]);
-        P->fused_smem = P->fused_stage + round16(2 * (size_t)nr_max) + 8 * (size_t)nr_max + 4 * (size_t)nh_max;
+        // CGS2: staged factor | row order | rows of W | direction at the
+        // block's nodes; the delayed variant adds the pending vector's rows
+        // and the unrotated Hessenberg matrix (64 x 64)
+        const size_t base = P->fused_stage + round16(2 * (size_t)nr_max) + 8 * (size_t)nr_max;
+        P->fused_smem = base + 4 * (size_t)nh_max;
+        P->fused_smem_d = base + round16(4 * (size_t)nh_max) + 8 * (size_t)nr_max + 8 * 64 * 64;
         // one thread per row quad of the largest block, whole warps
         P->fused_threads = std::min(kFusedThreads, std::max(128, ((nr_max + 3) / 4 + 1 + 31) / 32 * 32));
-        if (P->fused_smem > kMaxDynSmem) return false;
-        const void* kfn = P->lanes == 8 ? (const void*)k_arnoldi_fused<8> : (const void*)k_arnoldi_fused<4>;
-        raise_smem_limit(kfn, P->fused_smem);
-        // the smallest shared-memory carveout that holds the block's
-        // shared data (dynamic + static, about 1 KB reserved), so that the
-        // rest of the SM's 256 KB stays L1 for the block's basis rows
-        {
-            cudaFuncAttributes fa;
-            FVM_CUDA(cudaFuncGetAttributes(&fa, kfn));
-            const double need = (double)(P->fused_smem + fa.sharedSizeBytes + 1024);
-            const int pct = std::min(100, (int)std::ceil(100.0 * need / (228.0 * 1024.0)));
-            FVM_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
-        }
-        int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+        int dev = 0, coop = 0, nsm = 0;
         FVM_CUDA(cudaGetDevice(&dev));
         FVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         FVM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, P->fused_threads, P->fused_smem));
-        P->fused_ok = coop && per_sm > 0 && nb <= per_sm * nsm;
+        for (int v = 0; v < 2; ++v) {
+            const size_t smem = v ? P->fused_smem_d : P->fused_smem;
+            P->fused_var_ok[v] = false;
+            if (smem > kMaxDynSmem) continue;
+            const void* kfn = fused_kernel(P->lanes, v);
+            raise_smem_limit(kfn, smem);
+            // the smallest shared-memory carveout that holds the block's
+            // shared data (dynamic + static, about 1 KB reserved), so that
+            // the rest of the SM's 256 KB stays L1 for the block's basis rows
+            cudaFuncAttributes fa;
+            FVM_CUDA(cudaFuncGetAttributes(&fa, kfn));
+            const double need = (double)(smem + fa.sharedSizeBytes + 1024);
+            const int pct = std::min(100, (int)std::ceil(100.0 * need / (228.0 * 1024.0)));
+            FVM_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+            int per_sm = 0;
+            FVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, P->fused_threads, smem));
+            P->fused_var_ok[v] = coop && per_sm > 0 && nb <= per_sm * nsm;
+        }
+        P->fused_ok = P->fused_var_ok[0] || P->fused_var_ok[1];
     }
-    if (!P->fused_ok) return false;
+    if (!P->fused_ok || !P->fused_var_ok[fused_variant(c)]) return false;
     if (P->op_setup_id != P->setup_id) {
         const long ne = (long)P->op_val.n;
         const long nt = std::max(ne, (long)c->N);
@@ -516,7 +654,8 @@ void fused_cycle(fvm_ctx* c, Krylov* K, double cj, const double* ewt, double* H_
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(P->nb);
     cfg.blockDim = dim3(P->fused_threads);
-    cfg.dynamicSmemBytes = P->fused_smem;
+    const int var = fused_variant(c);
+    cfg.dynamicSmemBytes = var ? P->fused_smem_d : P->fused_smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -525,8 +664,13 @@ void fused_cycle(fvm_ctx* c, Krylov* K, double cj, const double* ewt, double* H_
     cfg.numAttrs = 1;
     P->flags.zero(s);
     c->tm.begin(TM_CGS, s);
-    if (P->lanes == 8) FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_fused<8>, a));
-    else FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_fused<4>, a));
+    if (P->lanes == 8) {
+        if (var) FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_fused<8, true>, a));
+        else FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_fused<8, false>, a));
+    } else {
+        if (var) FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_fused<4, true>, a));
+        else FVM_CUDA(cudaLaunchKernelEx(&cfg, k_arnoldi_fused<4, false>, a));
+    }
     c->tm.end(TM_CGS, s);
     c->launches++;
 }

@@ -273,4 +273,90 @@ __device__ __forceinline__ void block_dots_by_warp(const float* __restrict__ U, 
     __syncthreads();
 }
 
+// Two block-local dot-product sets in one pass over the basis (FP32, one
+// warp per basis vector): out[i] = <U_i, A>, out[nb + i] = <U_i, B> for
+// i < nb, then out[2 nb] = <A, A> and out[2 nb + 1] = <A, B>, with A and B
+// the block's rows in shared memory (node order, rows [k0, k1)).  Each
+// basis row quad is loaded once for both products.  out[] is valid in every
+// thread after the call.
+__device__ __forceinline__ void block_dots2_by_warp(const float* __restrict__ U, size_t ld,
+                                                    const double* __restrict__ A, const double* __restrict__ Bv,
+                                                    int k0, int k1, int nb, double* out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int a0 = k0 & ~3;
+    const int nq = (k1 - a0 + 3) >> 2;
+    for (int i = warp; i < nb + 1; i += nw) {
+        double sa = 0.0, sb = 0.0;
+        const float* Ui = U + ld * (i < nb ? i : 0);
+        for (int q0 = lane; q0 < nq; q0 += 32 * 8) {
+            float4 u[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const int q = q0 + 32 * t;
+                u[t] = (i < nb && q < nq) ? __ldg(reinterpret_cast<const float4*>(Ui + a0 + 4 * q))
+                                          : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const int q = q0 + 32 * t;
+                if (q >= nq) continue;
+                const int r = a0 + 4 * q;
+                double va[4], vb[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const bool in = r + e >= k0 && r + e < k1;
+                    va[e] = in ? A[r + e - k0] : 0.0;
+                    vb[e] = in ? Bv[r + e - k0] : 0.0;
+                }
+                if (i < nb) {
+                    sa += (double)u[t].x * va[0] + (double)u[t].y * va[1] + (double)u[t].z * va[2] +
+                          (double)u[t].w * va[3];
+                    sb += (double)u[t].x * vb[0] + (double)u[t].y * vb[1] + (double)u[t].z * vb[2] +
+                          (double)u[t].w * vb[3];
+                } else {
+                    sa += va[0] * va[0] + va[1] * va[1] + va[2] * va[2] + va[3] * va[3];
+                    sb += va[0] * vb[0] + va[1] * vb[1] + va[2] * vb[2] + va[3] * vb[3];
+                }
+            }
+        }
+        sa = warp_sum(sa);
+        sb = warp_sum(sb);
+        if (lane == 0) {
+            if (i < nb) {
+                out[i] = sa;
+                out[nb + i] = sb;
+            } else {
+                out[2 * nb] = sa;
+                out[2 * nb + 1] = sb;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// acc1[e] = sum_i c1[i] U_i[r + e], acc2[e] = sum_i c2[i] U_i[r + e] (e < 4)
+// from one load of each basis row quad
+template <class B, bool CG>
+__device__ __forceinline__ void quad_combine2(const BasisRows<B, CG>& U, const double* c1, const double* c2, int nv,
+                                              int r, double acc1[4], double acc2[4]) {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc1[e] = acc2[e] = 0.0;
+    for (int i0 = 0; i0 < nv; i0 += kCgsGroup) {
+#pragma unroll
+        for (int q = 0; q < kCgsGroup; ++q) {
+            const int i = i0 + q;
+            if (i < nv) {
+                double u[4];
+                U.quad(i, r, u);
+                const double a = c1[i], b = c2[i];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    acc1[e] += a * u[e];
+                    acc2[e] += b * u[e];
+                }
+            }
+        }
+    }
+}
+
 } // namespace fvmb

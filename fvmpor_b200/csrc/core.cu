@@ -1224,6 +1224,16 @@ extern "C" int fvm_profile_read(fvm_ctx* c, double* ms, long* counts) {
     FVM_API_END
 }
 
+extern "C" int fvm_set_krylov_variant(fvm_ctx* c, int variant) {
+    if (!c) return -1;
+    if (variant != 0 && variant != 1) {
+        set_error("fvm_set_krylov_variant: variant must be 0 or 1");
+        return -1;
+    }
+    c->krylov_variant = variant;
+    return 0;
+}
+
 extern "C" int fvm_graph_counters(fvm_ctx* c, long* captures, long* replays) {
     if (!c) return -1;
     if (captures) *captures = c->graph_captures;

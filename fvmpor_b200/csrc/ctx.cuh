@@ -249,6 +249,7 @@ struct fvm_ctx {
     long n_syncs = 0;                // host waits on the context's stream (ctx_sync)
     bool graph_ok = true;            // cleared when a batch capture failed: launch directly
     bool use_graph = false;          // the running integration asked for CUDA-graph batches
+    int krylov_variant = 1;          // fused cycle's Gram-Schmidt: 0 CGS2, 1 delayed (fvm_set_krylov_variant)
     long graph_captures = 0, graph_replays = 0;   // CUDA-graph batches of the Arnoldi loop
     fvmb::KernelTimer tm;
     std::string err;

@@ -43,7 +43,8 @@ struct BlockILU {
     DevBuf<int> nbr_ptr, nbr;                  // blocks whose rows a block's operator reads
     DevBuf<unsigned> flags;                    // per block: last step published
     DevBuf<float> op_val, op_dg;
-    size_t fused_smem = 0, fused_stage = 0;
+    size_t fused_smem = 0, fused_smem_d = 0, fused_stage = 0;
+    bool fused_var_ok[2] = {false, false};   // CGS2 / delayed variant can run
     int fused_threads = 0, fused_nrmax = 0, fused_nhmax = 0;
     int nb = 0, maxb = 0;
     DevBuf<int> bstart, lu_ptr, lu_src, lu_diag;

@@ -402,6 +402,13 @@ int fvm_integrate_outputs(fvm_ctx* ctx, const fvm_opts* opts, double t0,
  * Returns 0, 1 when some corrector stopped at max_newton (the run still
  * completes), < 0 on failure.  No counterpart in the reference: IDAS has no
  * replay mode (the step loop it replaces is ida_integrator.h:296-321). */
+/* Gram-Schmidt of the fused GMRES cycle (fvm_opts.krylov_operator = 1):
+ * 1 (the default) delayed reorthogonalisation, one reduction and two passes
+ * over the basis per Arnoldi step; 0 classical Gram-Schmidt with
+ * reorthogonalisation, two reductions and four passes.  The same Krylov
+ * space; decomp/gmres.c:412-511 orthogonalises by modified Gram-Schmidt. */
+int fvm_set_krylov_variant(fvm_ctx* ctx, int variant);
+
 /* CUDA-graph batches of the Arnoldi loop run on this context so far
  * (fvm_opts.graph): graphs captured and batches replayed from them.  Either
  * pointer may be NULL. */
