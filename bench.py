@@ -630,21 +630,21 @@ def main():
     cmp["fp32_assembled_without_learned"]["clocks_comparison_runs"] = clk_cmp.summary()
 
     peak, peak_kind = peaks()
-    # roofline of the dominant kernel, the fused Arnoldi cycle: algorithmic
-    # bytes of Arnoldi step j (nv = j + 1 basis vectors) are the assembled
-    # operator (FP32 value + 4-byte column per non-zero), per node the
-    # direction and the cj coefficient (4 B each), ewt (8 B), four passes
-    # over the FP32 basis (16 nv B) and the new basis vector and direction
-    # (8 B); the factor stays in shared memory for the whole cycle.  Per
-    # launch = per cycle; the time is the kernel's CUDA-event total over its
-    # launches of the profiled run.
+    # roofline of the dominant kernel, the fused Arnoldi cycle (delayed
+    # reorthogonalisation): algorithmic bytes of Arnoldi step j (nv = j + 1
+    # basis vectors) are the assembled operator (FP32 value + 4-byte column
+    # per non-zero), per node the direction and the cj coefficient (4 B
+    # each), ewt (8 B), two passes over the FP32 basis (8 nv B) and the new
+    # basis vector and direction (8 B); the factor stays in shared memory
+    # for the whole cycle.  Per launch = per cycle; the time is the kernel's
+    # CUDA-event total over its launches of the profiled run.
     nnz = fb.Preconditioner(ph).info()["nnz"]
     nv_sum, n_ar = 0.0, 0
     for nli_s, nni_s in zip(st_prof["nli"], st_prof["nni"]):
         per = nli_s / max(int(nni_s), 1)   # Krylov iterations of each Newton solve of the step
         nv_sum += max(int(nni_s), 1) * per * (per + 1) / 2.0
         n_ar += int(nli_s)
-    bytes_steps = n_ar * (8.0 * nnz + 24.0 * N) + 16.0 * N * nv_sum
+    bytes_steps = n_ar * (8.0 * nnz + 24.0 * N) + 8.0 * N * nv_sum
     launches_k = max(int(prof["gram_schmidt"][1]), 1)
     fused_ms = prof["gram_schmidt"][0]
     achieved = bytes_steps / launches_k / (fused_ms / launches_k * 1e-3) / 1e9
@@ -678,8 +678,8 @@ def main():
         "host_waits_per_step": st0["nsync"] / max(st0["nst"], 1),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": FUSED_DRAM_BYTES,
-                     "kernel": "k_arnoldi_fused (one GMRES cycle: assembled operator, block-ILU(0) sweeps, CGS2, "
-                               "Givens)",
+                     "kernel": "k_arnoldi_fused (one GMRES cycle: assembled operator, block-ILU(0) sweeps, "
+                               "delayed-reorthogonalisation Gram-Schmidt, Givens)",
                      "algorithmic_bytes_per_launch": bytes_steps / launches_k,
                      "avg_ms": fused_ms / launches_k, "arnoldi_steps_per_launch": n_ar / launches_k,
                      "peak_kind": peak_kind},

@@ -41,6 +41,7 @@ namespace fvmb {
 
 struct FusedArgs {
     int N, m, nr_max, nh_max;
+    int nqp;                   // quads per block row array in shared memory (quad-transposed, quad_pos)
     size_t stage_max;          // shared bytes of the largest block's staged factor
     ArnState* st;
     float* U;
@@ -124,12 +125,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     unsigned short* uptr = lptr + nl + 1;
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + ilu_stage_bytes(nr, w.wn, nl + nu + 2, sizeof(float)) - 16);
     unsigned short* inv = reinterpret_cast<unsigned short*>(smem_raw + a.stage_max);
+    // the block's rows of W (and of the pending vector), quad-transposed
+    const int nqp = a.nqp;
     double* Ws = reinterpret_cast<double*>(smem_raw + a.stage_max + round16(2 * (size_t)a.nr_max));
-    float* tl = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(Ws) + 8 * (size_t)a.nr_max);
+    float* tl = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(Ws) + 32 * (size_t)nqp);
     // delayed variant: the block's rows of the pending vector v_k, then the
     // unrotated Hessenberg matrix (column c at Hs[64 c ..])
     double* Vs = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(tl) + round16(4 * (size_t)a.nh_max));
-    double* Hs = Vs + a.nr_max;
+    double* Hs = Vs + 4 * (size_t)nqp;
     if (threadIdx.x == 0) {
         tc05::mbar_init(mbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;");
@@ -172,8 +175,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     const int nb0 = a.nbr_ptr[b], nb1 = a.nbr_ptr[b + 1];
     // step 0's direction was written before the launch
     for (int k = threadIdx.x; k < nh; k += blockDim.x) tl[k] = __ldcg(a.tdir + a.halo_node[h0 + k]);
-    if constexpr (DEL)
-        for (int k = threadIdx.x; k < nr; k += blockDim.x) Vs[k] = 0.0;
+    // the padding rows of the edge quads stay zero
+    for (int k = threadIdx.x; k < 4 * nqp; k += blockDim.x) {
+        Ws[k] = 0.0;
+        if constexpr (DEL) Vs[k] = 0.0;
+    }
     __syncthreads();
     for (int j = 0;; ++j) {
         const int nv = j + 1;
@@ -211,7 +217,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         // preconditioner: both triangular sweeps in shared memory
         ilu_sweep<float, KM, false>(x, val, col, rp, dg, lrow, lptr, 1, nl);
         ilu_sweep<float, KM, true>(x, val, col, rp, dg, urow, uptr, 0, nu);
-        for (int k = threadIdx.x; k < nr; k += blockDim.x) Ws[k] = a.ewt[r0 + k] * (double)x[inv[k]];
+        for (int k = threadIdx.x; k < nr; k += blockDim.x) Ws[quad_pos(r0, nqp, r0 + k)] = a.ewt[r0 + k] * (double)x[inv[k]];
         __syncthreads();
         // Hessenberg column finalised by this step (-1: none yet), the entry
         // below its diagonal, and the scale of the basis vector it finalises
@@ -220,7 +226,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         double newscale = 0.0;
         if constexpr (!DEL) {
         // pass 1: a = U^T W
-        block_dots_by_warp(a.U, a.ld, Ws, r0, r1, nv, false, ca);
+        block_dots_by_warp(a.U, a.ld, Ws, nqp, r0, r1, nv, false, ca);
         for (int i = threadIdx.x; i < nv; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
         if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
         block_reduce_all_vmajor(pa, nv, nblk, ca);
@@ -232,10 +238,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
             quad_combine(UR, coef, nv, r, acc);
 #pragma unroll
             for (int e = 0; e < 4; ++e)
-                if (r + e >= r0 && r + e < r1) Ws[r + e - r0] -= acc[e];
+                if (r + e >= r0 && r + e < r1) Ws[quad_pos(r0, nqp, r + e)] -= acc[e];
         }
         __syncthreads();
-        block_dots_by_warp(a.U, a.ld, Ws, r0, r1, nv, true, cb);
+        block_dots_by_warp(a.U, a.ld, Ws, nqp, r0, r1, nv, true, cb);
         for (int i = threadIdx.x; i <= nv; i += blockDim.x) pb[(size_t)i * nblk + b] = cb[i];
         if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
         block_reduce_all_vmajor(pb, nv + 1, nblk, cb);
@@ -258,7 +264,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
             for (int e = 0; e < 4; ++e) {
                 const int k = r + e;
                 if (k >= r0 && k < r1) {
-                    const float u = (float)(Ws[k - r0] - acc[e]);
+                    const float u = (float)(Ws[quad_pos(r0, nqp, k)] - acc[e]);
                     Un[k] = u;
                     a.tdir[k] = (float)(snv * (double)u / a.ewt[k]);
                 }
@@ -284,7 +290,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         // four and two; the column of step k is final one step later.
         const int k = j;
         const int nbv = k == 0 ? 1 : k;   // basis vectors this step reads
-        block_dots2_by_warp(a.U, a.ld, Vs, Ws, r0, r1, nbv, ca);
+        block_dots2_by_warp(a.U, a.ld, Vs, Ws, nqp, r0, r1, nbv, ca);
         const int nred = 2 * nbv + 2;
         for (int i = threadIdx.x; i < nred; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
         if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
@@ -354,10 +360,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
                 for (int e = 0; e < 4; ++e) {
                     const int q = r + e;
                     if (q >= r0 && q < r1) {
-                        const double vq = Vs[q - r0];
+                        const int qp = quad_pos(r0, nqp, q);
+                        const double vq = Vs[qp];
                         if (k >= 1) Uk[q] = (float)(vq - acc1[e]);
-                        const double vn = Ws[q - r0] * rb - vcoef * vq - acc2[e];
-                        Vs[q - r0] = vn;
+                        const double vn = Ws[qp] * rb - vcoef * vq - acc2[e];
+                        Vs[qp] = vn;
                         a.tdir[q] = (float)(vn / a.ewt[q]);
                     }
                 }
@@ -561,9 +568,13 @@ bool fused_prepare(fvm_ctx* c, int m) {
         // CGS2: staged factor | row order | rows of W | direction at the
         // block's nodes; the delayed variant adds the pending vector's rows
         // and the unrotated Hessenberg matrix (64 x 64)
-        const size_t base = P->fused_stage + round16(2 * (size_t)nr_max) + 8 * (size_t)nr_max;
+        // block row arrays quad-transposed: nqp quads cover any block's rows
+        // from its first quad boundary
+        P->fused_nqp = nr_max / 4 + 2;
+        const size_t rows = 32 * (size_t)P->fused_nqp;
+        const size_t base = P->fused_stage + round16(2 * (size_t)nr_max) + rows;
         P->fused_smem = base + 4 * (size_t)nh_max;
-        P->fused_smem_d = base + round16(4 * (size_t)nh_max) + 8 * (size_t)nr_max + 8 * 64 * 64;
+        P->fused_smem_d = base + round16(4 * (size_t)nh_max) + rows + 8 * 64 * 64;
         // one thread per row quad of the largest block, whole warps
         P->fused_threads = std::min(kFusedThreads, std::max(128, ((nr_max + 3) / 4 + 1 + 31) / 32 * 32));
         int dev = 0, coop = 0, nsm = 0;
@@ -614,6 +625,7 @@ void fused_cycle(fvm_ctx* c, Krylov* K, double cj, const double* ewt, double* H_
     a.N = c->N;
     a.m = K->m;
     a.nr_max = P->fused_nrmax;
+    a.nqp = P->fused_nqp;
     a.nh_max = P->fused_nhmax;
     a.stage_max = P->fused_stage;
     a.st = K->st.p;

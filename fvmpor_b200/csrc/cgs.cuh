@@ -227,15 +227,25 @@ __device__ __forceinline__ void quad_combine(const BasisRows<B, CG>& U, const do
     }
 }
 
+// Rows of a block held in shared memory quad-transposed: the block's row
+// quads start at a0 = k0 & ~3, and row a0 + 4 q + e sits at e * nqp + q,
+// so the lanes of a warp, each on its own quad, read consecutive doubles
+// (no bank conflicts; row-major quads would put every fourth lane on the
+// same banks).  Rows of the edge quads outside [k0, k1) hold zeros.
+__device__ __forceinline__ int quad_pos(int k0, int nqp, int k) {
+    const int t = k - (k0 & ~3);
+    return (t & 3) * nqp + (t >> 2);
+}
+
 // Block-local dot products <U_i, W> over rows [k0, k1) for i < nv (and
 // sum W^2 as entry nv when with_norm) for an FP32 basis, one warp per
 // vector: the warp's lanes take the block's row quads in turn with eight
 // quads' loads (float4, read-only path) in flight per lane, then one shuffle
 // tree.  No block-wide reduction is needed, so vectors finish
-// independently.  out[i] is valid in every thread after the call.  Rows of
-// the edge quads outside [k0, k1) enter as zeros.
+// independently.  out[i] is valid in every thread after the call.  Wt is
+// quad-transposed (quad_pos).
 __device__ __forceinline__ void block_dots_by_warp(const float* __restrict__ U, size_t ld,
-                                                   const double* __restrict__ Wl, int k0, int k1, int nv,
+                                                   const double* __restrict__ Wt, int nqp, int k0, int k1, int nv,
                                                    bool with_norm, double* out) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int a0 = k0 & ~3;
@@ -256,10 +266,9 @@ __device__ __forceinline__ void block_dots_by_warp(const float* __restrict__ U, 
             for (int t = 0; t < 8; ++t) {
                 const int q = q0 + 32 * t;
                 if (q >= nq) continue;
-                const int r = a0 + 4 * q;
                 double w[4];
 #pragma unroll
-                for (int e = 0; e < 4; ++e) w[e] = (r + e >= k0 && r + e < k1) ? Wl[r + e - k0] : 0.0;
+                for (int e = 0; e < 4; ++e) w[e] = Wt[e * nqp + q];
                 if (i < nv)
                     acc += (double)u[t].x * w[0] + (double)u[t].y * w[1] + (double)u[t].z * w[2] +
                            (double)u[t].w * w[3];
@@ -276,12 +285,12 @@ __device__ __forceinline__ void block_dots_by_warp(const float* __restrict__ U, 
 // Two block-local dot-product sets in one pass over the basis (FP32, one
 // warp per basis vector): out[i] = <U_i, A>, out[nb + i] = <U_i, B> for
 // i < nb, then out[2 nb] = <A, A> and out[2 nb + 1] = <A, B>, with A and B
-// the block's rows in shared memory (node order, rows [k0, k1)).  Each
+// the block's rows in shared memory (quad-transposed, quad_pos).  Each
 // basis row quad is loaded once for both products.  out[] is valid in every
 // thread after the call.
 __device__ __forceinline__ void block_dots2_by_warp(const float* __restrict__ U, size_t ld,
                                                     const double* __restrict__ A, const double* __restrict__ Bv,
-                                                    int k0, int k1, int nb, double* out) {
+                                                    int nqp, int k0, int k1, int nb, double* out) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int a0 = k0 & ~3;
     const int nq = (k1 - a0 + 3) >> 2;
@@ -300,13 +309,11 @@ __device__ __forceinline__ void block_dots2_by_warp(const float* __restrict__ U,
             for (int t = 0; t < 8; ++t) {
                 const int q = q0 + 32 * t;
                 if (q >= nq) continue;
-                const int r = a0 + 4 * q;
                 double va[4], vb[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
-                    const bool in = r + e >= k0 && r + e < k1;
-                    va[e] = in ? A[r + e - k0] : 0.0;
-                    vb[e] = in ? Bv[r + e - k0] : 0.0;
+                    va[e] = A[e * nqp + q];
+                    vb[e] = Bv[e * nqp + q];
                 }
                 if (i < nb) {
                     sa += (double)u[t].x * va[0] + (double)u[t].y * va[1] + (double)u[t].z * va[2] +

@@ -45,7 +45,7 @@ struct BlockILU {
     DevBuf<float> op_val, op_dg;
     size_t fused_smem = 0, fused_smem_d = 0, fused_stage = 0;
     bool fused_var_ok[2] = {false, false};   // CGS2 / delayed variant can run
-    int fused_threads = 0, fused_nrmax = 0, fused_nhmax = 0;
+    int fused_threads = 0, fused_nrmax = 0, fused_nhmax = 0, fused_nqp = 0;
     int nb = 0, maxb = 0;
     DevBuf<int> bstart, lu_ptr, lu_src, lu_diag;
     DevBuf<int> lu_row;       // global row of each factor position (colour order inside the blocks)
