@@ -555,12 +555,20 @@ bool fused_prepare(fvm_ctx* c, int m) {
         P->op_lcol.upload(lcol, s);
         P->op_self.upload(self, s);
         P->op_src.upload(opsrc, s);
+        {
+            // the slice position of every Jacobian entry, for fd_gather
+            std::vector<int> opdst(P->nnz, 0);
+            for (size_t e = 0; e < opsrc.size(); ++e)
+                if (opsrc[e] >= 0) opdst[opsrc[e]] = (int)e;
+            P->op_dst.upload(opdst, s);
+        }
         P->halo_ptr.upload(halo_ptr, s);
         P->halo_node.upload(halo_node, s);
         P->nbr_ptr.upload(nbr_ptr, s);
         P->nbr.upload(nbr, s);
         P->flags.alloc(nb);
         P->op_val.alloc(opcol.size());
+        P->op_val.zero(s);   // the padding entries stay zero
         P->op_dg.alloc(c->N);
         P->fused_nrmax = nr_max;
         P->fused_nhmax = nh_max;
@@ -603,7 +611,9 @@ bool fused_prepare(fvm_ctx* c, int m) {
     }
     if (!P->fused_ok || !P->fused_var_ok[fused_variant(c)]) return false;
     if (P->op_setup_id != P->setup_id) {
-        const long ne = (long)P->op_val.n;
+        // the values come from fd_gather once the layout exists; the first
+        // set-up after the layout was built copies them here
+        const long ne = P->op_vals_setup == P->setup_id ? 0 : (long)P->op_val.n;
         const long nt = std::max(ne, (long)c->N);
         fvm_launch(c, k_op_refresh, grid_for(nt, 256), 256, 0, s, ne, P->op_src.p, P->J.p, P->op_val.p, c->N,
                    P->lu_row.p, P->ahhp.p, c->ntype.p, P->op_dg.p);

@@ -38,6 +38,8 @@ struct BlockILU {
     bool op_built = false, fused_ok = false;
     long op_setup_id = -1;
     DevBuf<int> op_slptr, op_blksl, op_src;
+    DevBuf<int> op_dst;                        // [nnz] slice position of each Jacobian entry
+    long op_vals_setup = -1;                   // set-up whose values fd_gather wrote into op_val
     DevBuf<unsigned short> op_lcol, op_self;   // 16-bit columns into each block's node list
     DevBuf<int> halo_ptr, halo_node;           // each block's node list: its rows and halo
     DevBuf<int> nbr_ptr, nbr;                  // blocks whose rows a block's operator reads
@@ -48,6 +50,8 @@ struct BlockILU {
     int fused_threads = 0, fused_nrmax = 0, fused_nhmax = 0, fused_nqp = 0;
     int nb = 0, maxb = 0;
     DevBuf<int> bstart, lu_ptr, lu_src, lu_diag;
+    DevBuf<int> lu_dst;       // [nnz] factor position of each Jacobian entry, -1 off the blocks
+    DevBuf<double> Jw;        // the set-up's Jacobian in factor order (written by fd_gather)
     DevBuf<int> lu_row;       // global row of each factor position (colour order inside the blocks)
     // ILU(0) elimination schedule of the shared-memory factorisation, one
     // contiguous segment per level (upd[seg_ptr[g] .. seg_ptr[g+1]) for the

@@ -214,7 +214,8 @@ __global__ void k_fd_gather(int nnz, const int* __restrict__ rowof, const int* _
                             const double* __restrict__ invV, const double* __restrict__ dstor,
                             const unsigned char* __restrict__ ntype, const double* __restrict__ hD,
                             const double* __restrict__ y, const double* __restrict__ shift,
-                            double* __restrict__ J) {
+                            double* __restrict__ J, const int* __restrict__ lu_dst, double* __restrict__ Jw,
+                            const int* __restrict__ op_dst, float* __restrict__ op_val) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nnz) return;
     const int i = rowof[q], j = col[q];
@@ -229,22 +230,27 @@ __global__ void k_fd_gather(int nnz, const int* __restrict__ rowof, const int* _
         if (i == j) v = v - dstor[i] / shift[i];
     }
     J[q] = v;
+    // the same value where the factorisation reads it (its block's copy
+    // window, so that it loads its block contiguously) and, once the fused
+    // cycle's operator layout exists, in that layout
+    const int pw = lu_dst[q];
+    if (pw >= 0) Jw[pw] = v;
+    if (op_val) op_val[op_dst[q]] = (float)v;
 }
 
 template <class T>
 __global__ void __launch_bounds__(128) k_ilu_factor(const int* __restrict__ bstart,
                                                     const int* __restrict__ lu_ptr,
-                                                    const int* __restrict__ lu_src,
+                                                    const double* __restrict__ Jw,
                                                     const int* __restrict__ lu_diag,
                                                     const unsigned short* __restrict__ lu_col,
                                                     const int* __restrict__ lvl_ptr,
                                                     const int* __restrict__ lvl_rows,
-                                                    const int* __restrict__ blk_lvl,
-                                                    const double* __restrict__ J, T* lu,
+                                                    const int* __restrict__ blk_lvl, T* lu,
                                                     int* status) {
     int b = blockIdx.x;
     int r0 = bstart[b], r1 = bstart[b + 1];
-    for (int p = lu_ptr[r0] + threadIdx.x; p < lu_ptr[r1]; p += blockDim.x) lu[p] = (T)J[lu_src[p]];
+    for (int p = lu_ptr[r0] + threadIdx.x; p < lu_ptr[r1]; p += blockDim.x) lu[p] = (T)Jw[p];
     __syncthreads();
     for (int l = blk_lvl[b]; l < blk_lvl[b + 1]; ++l) {
         for (int q = lvl_ptr[l] + threadIdx.x; q < lvl_ptr[l + 1]; q += blockDim.x) {
@@ -564,7 +570,7 @@ constexpr int kIluFactorPre = 32;
 template <class T>
 __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__ bstart,
                                                          const int* __restrict__ lu_ptr,
-                                                         const int* __restrict__ lu_src,
+                                                         const double* __restrict__ Jw,
                                                          const int* __restrict__ lu_diag,
                                                          const unsigned short* __restrict__ lu_col,
                                                          const int* __restrict__ lvl_ptr,
@@ -572,8 +578,7 @@ __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__
                                                          const int* __restrict__ blk_lvl,
                                                          const int* __restrict__ seg_ptr,
                                                          const unsigned* __restrict__ upd, int scr_off,
-                                                         int scr_words,
-                                                         const double* __restrict__ J, T* __restrict__ lu,
+                                                         int scr_words, T* __restrict__ lu,
                                                          int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int b = blockIdx.x;
@@ -590,7 +595,7 @@ __global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__
     const int lq0 = lvl_ptr[la];
 #pragma unroll 4
     for (int p = e0 + threadIdx.x; p < e1; p += blockDim.x) {
-        val[p - w.base] = (T)J[lu_src[p]];
+        val[p - w.base] = (T)Jw[p];
         col[p - w.base] = lu_col[p];
     }
     for (int i = threadIdx.x; i <= nr; i += blockDim.x) rp[i] = (unsigned short)(lu_ptr[r0 + i] - w.base);
@@ -1061,9 +1066,17 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
     P->h_lu_row = lu_row;
     P->lu_ptr.upload(lu_ptr, s);
     // 8 padding entries so every block's widened copy window stays inside
+    {
+        // where fd_gather puts each Jacobian entry for the factorisation
+        std::vector<int> lu_dst(P->nnz, -1);
+        for (size_t p = 0; p < lu_src.size(); ++p) lu_dst[lu_src[p]] = (int)p;
+        P->lu_dst.upload(lu_dst, s);
+    }
     lu_src.resize(lu_src.size() + 8, 0);
     lu_col.resize(lu_col.size() + 8, 0);
     P->lu_src.upload(lu_src, s);
+    P->Jw.alloc(lu_src.size());
+    P->Jw.zero(s);
     P->lu_diag.upload(lu_diag, s);
     P->lu_row.upload(lu_row, s);
     P->lu_col.upload(lu_col, s);
@@ -1115,8 +1128,12 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
             } else {
                 mz ? go(k_fd_elem<3, 3, false, true, S>) : go(k_fd_elem<3, 3, false, false, S>);
             }
+            // the fused cycle's operator values too, once its layout exists
+            float* opv = P->op_built && P->fused_ok ? P->op_val.p : nullptr;
             fvm_launch(c, k_fd_gather<S>, grid_for(P->nnz, 256), 256, 0, s, P->nnz, P->rowof.p, P->col.p,
-                       P->fd_jptr.p, slots, c->invV.p, P->dstor.p, c->ntype.p, c->hD.p, y, P->shift.p, P->J.p);
+                       P->fd_jptr.p, slots, c->invV.p, P->dstor.p, c->ntype.p, c->hD.p, y, P->shift.p, P->J.p,
+                       P->lu_dst.p, P->Jw.p, opv ? P->op_dst.p : nullptr, opv);
+            P->op_vals_setup = opv ? P->setup_id : -1;
         };
         // the FP64 slot buffer holds the FP32 slots in its first half
         if (precision) run(reinterpret_cast<float*>(P->fd_slots.p));
@@ -1132,24 +1149,24 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
         size_t sm = (size_t)so + 8 * (size_t)sw;
         if (precision) {
             P->lu32.alloc(nlu);
-            fvm_launch(c, k_ilu_factor_smem<float>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p,
+            fvm_launch(c, k_ilu_factor_smem<float>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->Jw.p,
                        P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->seg_ptr.p, P->upd.p,
-                       so, sw, P->J.p, P->lu32.p, P->status.p);
+                       so, sw, P->lu32.p, P->status.p);
         } else {
             P->lu64.alloc(nlu);
-            fvm_launch(c, k_ilu_factor_smem<double>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p,
+            fvm_launch(c, k_ilu_factor_smem<double>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->Jw.p,
                        P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->seg_ptr.p, P->upd.p,
-                       so, sw, P->J.p, P->lu64.p, P->status.p);
+                       so, sw, P->lu64.p, P->status.p);
         }
     } else if (precision) {
         P->lu32.alloc(nlu);
-        fvm_launch(c, k_ilu_factor<float>, P->nb, 128, 0, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p, P->lu_diag.p, P->lu_col.p,
-                                                  P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->J.p, P->lu32.p,
+        fvm_launch(c, k_ilu_factor<float>, P->nb, 128, 0, s, P->bstart.p, P->lu_ptr.p, P->Jw.p, P->lu_diag.p, P->lu_col.p,
+                                                  P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->lu32.p,
                                                   P->status.p);
     } else {
         P->lu64.alloc(nlu);
-        fvm_launch(c, k_ilu_factor<double>, P->nb, 128, 0, s, P->bstart.p, P->lu_ptr.p, P->lu_src.p, P->lu_diag.p, P->lu_col.p,
-                                                   P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->J.p, P->lu64.p,
+        fvm_launch(c, k_ilu_factor<double>, P->nb, 128, 0, s, P->bstart.p, P->lu_ptr.p, P->Jw.p, P->lu_diag.p, P->lu_col.p,
+                                                   P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->lu64.p,
                                                    P->status.p);
     }
     c->tm.end(TM_ILU_FACTOR, s);
