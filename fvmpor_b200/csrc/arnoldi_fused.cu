@@ -105,6 +105,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     // the two combine coefficient sets
     __shared__ double hp[DEL ? 64 : 1], tv[DEL ? 64 : 1], pv[DEL ? 64 : 1], htv[DEL ? 64 : 1],
         c1[DEL ? 64 : 1], c2[DEL ? 64 : 1];
+    // warp partials of the delayed variant's dot pass (two alternating groups)
+    __shared__ double red[DEL ? 2 * (kFusedThreads / 32) * 2 * kCgsGroup : 1];
     __shared__ int s_done;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int b = blockIdx.x, nblk = gridDim.x;
@@ -290,7 +292,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         // four and two; the column of step k is final one step later.
         const int k = j;
         const int nbv = k == 0 ? 1 : k;   // basis vectors this step reads
-        block_dots2_by_warp(a.U, a.ld, Vs, Ws, nqp, r0, r1, nbv, ca);
+        block_dots2_by_quad(a.U, a.ld, Vs, Ws, nqp, r0, r1, nbv, red, ca);
         const int nred = 2 * nbv + 2;
         for (int i = threadIdx.x; i < nred; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
         if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;

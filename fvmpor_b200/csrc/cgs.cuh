@@ -341,6 +341,85 @@ __device__ __forceinline__ void block_dots2_by_warp(const float* __restrict__ U,
     __syncthreads();
 }
 
+// The same two dot-product sets (and the same out[] layout) with one thread
+// per row quad: a thread reads its rows of A and B from shared memory once
+// per kCgsGroup basis vectors and keeps that group's loads in flight
+// together.  The warp's 2 kCgsGroup partial sums are reduced by a
+// transposing butterfly: each exchange hands the partner the half of the
+// values it keeps, so after offsets 16, 8, 4, 2 every lane holds one value
+// (index b1 + 2 b2 + 4 b3 + 8 b4 of its lane bits) summed over 16 lanes, and
+// offset 1 completes it; 16 exchanges instead of 5 per value.  The warps'
+// sums are then added in warp order.  red holds 2 x (warps x 2 kCgsGroup)
+// doubles (alternating groups, so one barrier per group).
+__device__ __forceinline__ void block_dots2_by_quad(const float* __restrict__ U, size_t ld,
+                                                    const double* __restrict__ A, const double* __restrict__ Bv,
+                                                    int nqp, int k0, int k1, int nb, double* red, double* out) {
+    constexpr int G = kCgsGroup, NV = 2 * kCgsGroup;
+    static_assert(NV == 16, "the butterfly below reduces 16 values per lane");
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int a0 = k0 & ~3;
+    const int nq = (k1 - a0 + 3) >> 2;
+    const int idx = ((lane >> 1) & 1) | (((lane >> 2) & 1) << 1) | (((lane >> 3) & 1) << 2) | (((lane >> 4) & 1) << 3);
+    int buf = 0;
+    for (int i0 = 0; i0 <= nb; i0 += G, buf ^= 1) {
+        double v[NV];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) v[j] = 0.0;
+        for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+            float4 u[G];
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int i = i0 + g;
+                u[g] = i < nb ? __ldg(reinterpret_cast<const float4*>(U + ld * i + a0 + 4 * q))
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            double x[4], y[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                x[e] = A[e * nqp + q];
+                y[e] = Bv[e * nqp + q];
+            }
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int i = i0 + g;
+                if (i < nb) {
+                    const double u0 = u[g].x, u1 = u[g].y, u2 = u[g].z, u3 = u[g].w;
+                    v[2 * g] += u0 * x[0] + u1 * x[1] + u2 * x[2] + u3 * x[3];
+                    v[2 * g + 1] += u0 * y[0] + u1 * y[1] + u2 * y[2] + u3 * y[3];
+                } else if (i == nb) {
+                    v[2 * g] += x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3];
+                    v[2 * g + 1] += x[0] * y[0] + x[1] * y[1] + x[2] * y[2] + x[3] * y[3];
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int o = 16 >> s, c = NV >> (s + 1);
+            const bool up = (lane & o) != 0;
+#pragma unroll
+            for (int j = 0; j < c; ++j) {
+                const double send = up ? v[j] : v[j + c];
+                const double keep = up ? v[j + c] : v[j];
+                v[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+            }
+        }
+        v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+        double* rb = red + buf * nw * NV;
+        if (!(lane & 1)) rb[warp * NV + idx] = v[0];
+        __syncthreads();
+        if (threadIdx.x < NV) {
+            const int i = i0 + (threadIdx.x >> 1);
+            if (i <= nb) {
+                double t = 0.0;
+                for (int w2 = 0; w2 < nw; ++w2) t += rb[w2 * NV + threadIdx.x];
+                if (i < nb) out[(threadIdx.x & 1) ? nb + i : i] = t;
+                else out[2 * nb + (threadIdx.x & 1)] = t;
+            }
+        }
+    }
+    __syncthreads();
+}
+
 // acc1[e] = sum_i c1[i] U_i[r + e], acc2[e] = sum_i c2[i] U_i[r + e] (e < 4)
 // from one load of each basis row quad
 template <class B, bool CG>
