@@ -17,13 +17,15 @@
 //     one warp per 32 rows, entry-major slices with 16-bit local columns)
 //     straight into the shared-memory vector the triangular sweeps work on,
 //     runs both sweeps there, scales by ewt, and
-//     orthogonalises its rows (CGS2 in three passes over the basis, row quads,
-//     fixed-order reductions through per-block partials);
+//     orthogonalises its rows (by delayed reorthogonalisation in two passes
+//     over the basis, or by CGS2 in three; row quads, fixed-order reductions
+//     through per-block partials);
 //   - every block computes the Hessenberg column, the rotations and the
 //     stopping test from the same reduced numbers, so all take the same
 //     decision without another barrier; block 0 writes them out for the
 //     host's back substitution.
-// Two bounded grid barriers per step (after each dot pass).  The next
+// One bounded grid barrier per step with delayed reorthogonalisation, two
+// with CGS2 (after each dot pass).  The next
 // direction is published block by block: a block raises its flag once its
 // rows are written, and a block starting the next step waits (bounded) only
 // for the flags of the blocks its operator rows reach, plus its two
@@ -58,6 +60,7 @@ struct FusedArgs {
     const int* nbr_ptr;        // [nb + 1] blocks whose flags a block waits for
     const int* nbr;
     unsigned* flags;           // [nb] last step whose direction rows a block wrote
+    unsigned* sync;            // arrival counter of the cycle's grid barriers (cleared with the flags)
     const float* op_val;
     const float* op_dg;        // [N], factor order: ahh(h + d) on free rows, else 0
     float dcj;                 // cj - cj of the set-up
@@ -72,7 +75,6 @@ struct FusedArgs {
     const int* lu_row;
     const double* beta2;       // ||D P^-1 r||^2 of the cycle's start
     double* partial;
-    unsigned* bar;
     int* err;
     double* H;
     double* cs;
@@ -88,6 +90,48 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ unsigned atom_add_release_gpu(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// Grid barrier of the cycle on a counter that only grows within a launch
+// (cleared with the flags before it): a block adds 1 with release semantics
+// and waits (acquire, bounded) until the counter reaches the next multiple
+// of the grid size.  Its own arrival number says which multiple, so there is
+// no generation word, no reset and no further step for the last block to
+// arrive.  A block that gives up, or meets an error elsewhere, sets
+// kSyncFail (far above any count of one launch): every block sees it at its
+// next barrier and leaves, and err carries the reason to the host.
+constexpr unsigned kSyncFail = 1u << 30;
+__device__ __forceinline__ void fused_fail(unsigned* sync, int* err, int code) {
+    atomicExch(err, code);
+    atomicOr(sync, kSyncFail);
+}
+__device__ __forceinline__ bool fused_sync(unsigned* sync, int* err, int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned old = atom_add_release_gpu(sync, 1u);
+        bool ok = !(old & kSyncFail);
+        if (ok) {
+            const unsigned target = (old / gridDim.x + 1) * gridDim.x;
+            long it = 0;
+            unsigned v;
+            while ((v = ld_acquire_gpu(sync)) < target) {
+                if (++it > (1l << 26)) {
+                    fused_fail(sync, err, 3);
+                    break;
+                }
+            }
+            ok = v >= target && !(v & kSyncFail);
+        }
+        *s_ok = ok ? 1 : 0;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
 // barrier among `count` threads (whole warps) of the block on barrier `id`
 __device__ __forceinline__ void named_barrier(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
@@ -107,7 +151,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         c1[DEL ? 64 : 1], c2[DEL ? 64 : 1];
     // warp partials of the delayed variant's dot pass (two alternating groups)
     __shared__ double red[DEL ? 2 * (kFusedThreads / 32) * 2 * kCgsGroup : 1];
-    __shared__ int s_done;
+    __shared__ int s_done, s_ok;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int b = blockIdx.x, nblk = gridDim.x;
     const int r0 = a.bstart[b], r1 = a.bstart[b + 1], nr = r1 - r0;
@@ -162,7 +206,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     }
     bool ok = tc05::mbar_wait(mbar, 0);
     if (!ok) ok = tc05::mbar_wait(mbar, 0);   // copies in flight get a second bounded chance
-    if (!__syncthreads_and(ok ? 1 : 0) && threadIdx.x == 0) atomicExch(a.err, 2);   // all blocks stop at the next barrier
+    if (!__syncthreads_and(ok ? 1 : 0) && threadIdx.x == 0) fused_fail(a.sync, a.err, 2);   // all blocks stop at the next barrier
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int sl0 = a.blksl[b], nsl = a.blksl[b + 1] - sl0;
     // vector-major partials: pa[v * nblk + b]
@@ -230,7 +274,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         // pass 1: a = U^T W
         block_dots_by_warp(a.U, a.ld, Ws, nqp, r0, r1, nv, false, ca);
         for (int i = threadIdx.x; i < nv; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
-        if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
+        if (!fused_sync(a.sync, a.err, &s_ok)) return;
         block_reduce_all_vmajor(pa, nv, nblk, ca);
         for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = ca[i] * sc[i] * sc[i];
         __syncthreads();
@@ -245,7 +289,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         __syncthreads();
         block_dots_by_warp(a.U, a.ld, Ws, nqp, r0, r1, nv, true, cb);
         for (int i = threadIdx.x; i <= nv; i += blockDim.x) pb[(size_t)i * nblk + b] = cb[i];
-        if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
+        if (!fused_sync(a.sync, a.err, &s_ok)) return;
         block_reduce_all_vmajor(pb, nv + 1, nblk, cb);
         double nrm2 = cb[nv];
         for (int i = 0; i < nv; ++i) {
@@ -295,7 +339,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         block_dots2_by_quad(a.U, a.ld, Vs, Ws, nqp, r0, r1, nbv, red, ca);
         const int nred = 2 * nbv + 2;
         for (int i = threadIdx.x; i < nred; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
-        if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
+        if (!fused_sync(a.sync, a.err, &s_ok)) return;
         block_reduce_all_vmajor(pa, nred, nblk, ca);
         double beta = 1.0, ck = 0.0;
         if (k == 0) {
@@ -390,7 +434,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
                     const unsigned* f = a.flags + a.nbr[kk];
                     long it = 0;
                     while (ld_acquire_gpu(f) < (unsigned)nv) {
-                        if (++it > (1l << 26)) { atomicExch(a.err, 3); break; }
+                        if (++it > (1l << 26)) { fused_fail(a.sync, a.err, 3); break; }
                     }
                 }
             }
@@ -455,6 +499,8 @@ __global__ void k_first_dir(int N, const float* __restrict__ U0, const double* _
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < N) t[k] = (float)(scale[0] * (double)U0[k] / ewt[k]);
 }
+
+static int fused_sync_slot(int nb) { return ((nb + 31) & ~31) + 32; }
 
 static const void* fused_kernel(int lanes, int variant) {
     if (lanes == 8) return variant ? (const void*)k_arnoldi_fused<8, true> : (const void*)k_arnoldi_fused<8, false>;
@@ -568,7 +614,8 @@ bool fused_prepare(fvm_ctx* c, int m) {
         P->halo_node.upload(halo_node, s);
         P->nbr_ptr.upload(nbr_ptr, s);
         P->nbr.upload(nbr, s);
-        P->flags.alloc(nb);
+        // the blocks' flags, then the barrier counter on its own 128-byte line
+        P->flags.alloc(fused_sync_slot(nb) + 32);
         P->op_val.alloc(opcol.size());
         P->op_val.zero(s);   // the padding entries stay zero
         P->op_dg.alloc(c->N);
@@ -655,6 +702,7 @@ void fused_cycle(fvm_ctx* c, Krylov* K, double cj, const double* ewt, double* H_
     a.nbr_ptr = P->nbr_ptr.p;
     a.nbr = P->nbr.p;
     a.flags = P->flags.p;
+    a.sync = P->flags.p + fused_sync_slot(P->nb);
     a.op_val = P->op_val.p;
     a.op_dg = P->op_dg.p;
     a.dcj = (float)(cj - P->cj_setup);
@@ -669,7 +717,6 @@ void fused_cycle(fvm_ctx* c, Krylov* K, double cj, const double* ewt, double* H_
     a.lu_row = P->lu_row.p;
     a.beta2 = K->res.p;
     a.partial = K->partial.p;
-    a.bar = K->bar.p;
     a.err = K->err.p;
     a.H = H_d;
     a.cs = cs_d;
