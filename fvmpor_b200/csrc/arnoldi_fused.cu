@@ -336,7 +336,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         // four and two; the column of step k is final one step later.
         const int k = j;
         const int nbv = k == 0 ? 1 : k;   // basis vectors this step reads
-        block_dots2_by_quad(a.U, a.ld, Vs, Ws, nqp, r0, r1, nbv, red, ca);
+        float4 kept[kCgsGroup];
+        block_dots2_by_quad(a.U, a.ld, Vs, Ws, nqp, r0, r1, nbv, red, ca, kept);
         const int nred = 2 * nbv + 2;
         for (int i = threadIdx.x; i < nred; i += blockDim.x) pa[(size_t)i * nblk + b] = ca[i];
         if (!fused_sync(a.sync, a.err, &s_ok)) return;
@@ -401,7 +402,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
             const double vcoef = k == 0 ? 0.0 : ck * rb;
             for (int r = q0 + 4 * threadIdx.x; r < r1; r += 4 * blockDim.x) {
                 double acc1[4], acc2[4];
-                quad_combine2(UR, c1, c2, nbv, r, acc1, acc2);
+                if (r == q0 + 4 * (int)threadIdx.x) quad_combine2_kept(UR, c1, c2, nbv, r, kept, acc1, acc2);
+                else quad_combine2(UR, c1, c2, nbv, r, acc1, acc2);
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int q = r + e;
@@ -419,10 +421,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         }
         // publish this block's rows of the next direction
         __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            st_release_gpu(a.flags + b, (unsigned)nv);
-        }
+        if (threadIdx.x == 0) st_release_gpu(a.flags + b, (unsigned)nv);   // release: the block's writes before the barrier
         __syncthreads();
         // rotations and stopping test for the finalised column, the same in
         // every block (the same reduced numbers, the same operations), on

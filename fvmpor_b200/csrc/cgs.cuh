@@ -350,10 +350,14 @@ __device__ __forceinline__ void block_dots2_by_warp(const float* __restrict__ U,
 // (index b1 + 2 b2 + 4 b3 + 8 b4 of its lane bits) summed over 16 lanes, and
 // offset 1 completes it; 16 exchanges instead of 5 per value.  The warps'
 // sums are then added in warp order.  red holds 2 x (warps x 2 kCgsGroup)
-// doubles (alternating groups, so one barrier per group).
+// doubles (alternating groups, so one barrier per group).  keep receives
+// the thread's first quad of the last group's vectors (from kept_first(nb)
+// on, zeros past nb - 1), for a later pass over the same rows.
+__host__ __device__ inline int kept_first(int nb) { return nb & ~(kCgsGroup - 1); }
 __device__ __forceinline__ void block_dots2_by_quad(const float* __restrict__ U, size_t ld,
                                                     const double* __restrict__ A, const double* __restrict__ Bv,
-                                                    int nqp, int k0, int k1, int nb, double* red, double* out) {
+                                                    int nqp, int k0, int k1, int nb, double* red, double* out,
+                                                    float4 (&keep)[kCgsGroup]) {
     constexpr int G = kCgsGroup, NV = 2 * kCgsGroup;
     static_assert(NV == 16, "the butterfly below reduces 16 values per lane");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -372,6 +376,10 @@ __device__ __forceinline__ void block_dots2_by_quad(const float* __restrict__ U,
                 const int i = i0 + g;
                 u[g] = i < nb ? __ldg(reinterpret_cast<const float4*>(U + ld * i + a0 + 4 * q))
                               : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            if (i0 + G > nb && q == (int)threadIdx.x) {
+#pragma unroll
+                for (int g = 0; g < G; ++g) keep[g] = u[g];
             }
             double x[4], y[4];
 #pragma unroll
@@ -399,8 +407,8 @@ __device__ __forceinline__ void block_dots2_by_quad(const float* __restrict__ U,
 #pragma unroll
             for (int j = 0; j < c; ++j) {
                 const double send = up ? v[j] : v[j + c];
-                const double keep = up ? v[j + c] : v[j];
-                v[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                const double mine = up ? v[j + c] : v[j];
+                v[j] = mine + __shfl_xor_sync(0xffffffffu, send, o);
             }
         }
         v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
@@ -418,6 +426,45 @@ __device__ __forceinline__ void block_dots2_by_quad(const float* __restrict__ U,
         }
     }
     __syncthreads();
+}
+
+// quad_combine2 for a row quad whose vectors from kept_first(nv) on are
+// already in registers (keep, from block_dots2_by_quad): those first, then
+// the others loaded kCgsGroup at a time
+template <class B, bool CG>
+__device__ __forceinline__ void quad_combine2_kept(const BasisRows<B, CG>& U, const double* c1, const double* c2,
+                                                   int nv, int r, const float4 (&keep)[kCgsGroup], double acc1[4],
+                                                   double acc2[4]) {
+    const int i1 = kept_first(nv);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc1[e] = acc2[e] = 0.0;
+#pragma unroll
+    for (int q = 0; q < kCgsGroup; ++q) {
+        const int i = i1 + q;
+        if (i < nv) {
+            const double u[4] = {keep[q].x, keep[q].y, keep[q].z, keep[q].w};
+            const double a = c1[i], b = c2[i];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                acc1[e] += a * u[e];
+                acc2[e] += b * u[e];
+            }
+        }
+    }
+    for (int i0 = 0; i0 < i1; i0 += kCgsGroup) {
+#pragma unroll
+        for (int q = 0; q < kCgsGroup; ++q) {
+            const int i = i0 + q;
+            double u[4];
+            U.quad(i, r, u);
+            const double a = c1[i], b = c2[i];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                acc1[e] += a * u[e];
+                acc2[e] += b * u[e];
+            }
+        }
+    }
 }
 
 // acc1[e] = sum_i c1[i] U_i[r + e], acc2[e] = sum_i c2[i] U_i[r + e] (e < 4)
