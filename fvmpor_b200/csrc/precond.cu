@@ -564,11 +564,15 @@ static void launch_schur_apply(fvm_ctx* c, BlockILU* P, const T* lu, const doubl
 // Shared-memory factorisation: gather the block's Jacobian entries into the
 // same copy window the apply uses, eliminate level by level in shared
 // memory (IKJ, pivots inverted after their row), write the block back.
-// schedule words of the next level each of the 256 threads holds
-constexpr int kIluFactorPre = 32;
+// 1024 threads: one block per SM, so the copies in and out and the
+// schedule prefetch keep many loads in flight, while a level's rows (one
+// thread each, a few hundred) run on the first warps.  Schedule words of
+// the next level each thread holds:
+constexpr int kIluFactorThreads = 1024;
+constexpr int kIluFactorPre = 8;
 
 template <class T>
-__global__ void __launch_bounds__(256) k_ilu_factor_smem(const int* __restrict__ bstart,
+__global__ void __launch_bounds__(kIluFactorThreads, 1) k_ilu_factor_smem(const int* __restrict__ bstart,
                                                          const int* __restrict__ lu_ptr,
                                                          const double* __restrict__ Jw,
                                                          const int* __restrict__ lu_diag,
@@ -974,12 +978,12 @@ static void build_pattern(fvm_ctx* c, BlockILU* P) {
         }
         P->smem_stage[0] = (fits16 && need64 <= kMaxDynSmem) ? need64 : 0;
         P->smem_stage[1] = (fits16 && need32 <= kMaxDynSmem) ? need32 : 0;
-        // two schedule buffers of scr_words words (at most what 256 threads
-        // hold in kIluFactorPre registers each)
+        // two schedule buffers of scr_words words (at most what the
+        // factorisation's threads hold in kIluFactorPre registers each)
         for (int pr = 0; pr < 2; ++pr) {
             const size_t st = round16(P->smem_stage[pr]);
             const size_t room = P->smem_stage[pr] && st < kMaxDynSmem ? (kMaxDynSmem - st) / 8 : 0;
-            P->scr_words[pr] = (int)std::min<size_t>(std::min<size_t>(seg_max, room), 256 * kIluFactorPre);
+            P->scr_words[pr] = (int)std::min<size_t>(std::min<size_t>(seg_max, room), (size_t)kIluFactorThreads * kIluFactorPre);
         }
         // entries per row held in registers by the staged triangular sweeps:
         // 8 covers the lower or upper part of a 3D row, 4 of a 2D row
@@ -1149,12 +1153,12 @@ void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* 
         size_t sm = (size_t)so + 8 * (size_t)sw;
         if (precision) {
             P->lu32.alloc(nlu);
-            fvm_launch(c, k_ilu_factor_smem<float>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->Jw.p,
+            fvm_launch(c, k_ilu_factor_smem<float>, P->nb, kIluFactorThreads, sm, s, P->bstart.p, P->lu_ptr.p, P->Jw.p,
                        P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->seg_ptr.p, P->upd.p,
                        so, sw, P->lu32.p, P->status.p);
         } else {
             P->lu64.alloc(nlu);
-            fvm_launch(c, k_ilu_factor_smem<double>, P->nb, 256, sm, s, P->bstart.p, P->lu_ptr.p, P->Jw.p,
+            fvm_launch(c, k_ilu_factor_smem<double>, P->nb, kIluFactorThreads, sm, s, P->bstart.p, P->lu_ptr.p, P->Jw.p,
                        P->lu_diag.p, P->lu_col.p, P->lvl_ptr.p, P->lvl_rows.p, P->blk_lvl.p, P->seg_ptr.p, P->upd.p,
                        so, sw, P->lu64.p, P->status.p);
         }
