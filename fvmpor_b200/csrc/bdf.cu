@@ -420,8 +420,9 @@ struct DeviceOps {
     }
     int gmres(double cj, double tol, int* its, double* rn, long* nps, long* njv) {
         GmresCounters gc;
+        // the Newton update reads x next on the same stream: no wait here
         int r = gmres_dev(c, cj, y.p, yp.p, F.p, ewt.p, F.p, x.p, o.krylov_dim, o.max_restarts,
-                          o.precision, tol * tol_scale, its, rn, &gc, o.krylov_operator);
+                          o.precision, tol * tol_scale, its, rn, &gc, o.krylov_operator, false);
         *nps = gc.nps;
         *njv = gc.njv;
         if (ilu_status_seen(c)) return 3;   // zero pivot in the factor this solve used

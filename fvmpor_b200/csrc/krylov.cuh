@@ -64,10 +64,12 @@ double reduce_sumsq(fvm_ctx* c, const double* x, const double* w);
 double reduce_dot(fvm_ctx* c, const double* x, const double* y);
 
 // op 0: J v by the residual's difference quotient; 1: by the assembled
-// Jacobian of the last set-up (jacobian_apply)
+// Jacobian of the last set-up (jacobian_apply).  sync_end false: a converged
+// solve returns with the update of x still queued on the context's stream
 int gmres_dev(fvm_ctx* c, double cj, const double* y, const double* yp, const double* F0,
               const double* ewt, const double* b, double* x, int m, int max_restarts,
-              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt, int op = 0);
+              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt, int op = 0,
+              bool sync_end = true);
 
 // preconditioner (precond.cu)
 void psetup_dev(fvm_ctx* c, double cj, double h, const double* y, const double* yp,

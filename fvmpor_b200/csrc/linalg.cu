@@ -476,7 +476,7 @@ template <class B>
 static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const double* yp,
                       const double* F0, const double* ewt, const double* b, double* x, int m,
                       int max_restarts, double tol, int* iters, double* res_norm,
-                      GmresCounters* cnt, int op) {
+                      GmresCounters* cnt, int op, bool sync_end) {
     cudaStream_t s = c->stream;
     const int N = c->N;
     B* U = reinterpret_cast<B*>(K->U);
@@ -787,7 +787,10 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         fvm_launch(c, k_axpy, grid_for(N, 256), 256, 0, s, N, 1.0, K->t.p, x);
         have_x = true;
         if (conv) {
-            ctx_sync(c);
+            // x is complete once the stream reaches here; a caller that reads
+            // device results next on the same stream (the integrator's Newton
+            // update) need not wait
+            if (sync_end) ctx_sync(c);
             *iters = total;
             *res_norm = rnorm;
             return 0;
@@ -801,12 +804,14 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
 
 int gmres_dev(fvm_ctx* c, double cj, const double* y, const double* yp, const double* F0,
               const double* ewt, const double* b, double* x, int m, int max_restarts,
-              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt, int op) {
+              int precision, double tol, int* iters, double* res_norm, GmresCounters* cnt, int op, bool sync_end) {
     if (m < 1 || m > 60) throw Error("gmres: krylov dimension must be in [1, 60]");
     Krylov* K = krylov_get(c, m, precision);
     const int r = precision
-                      ? gmres_impl<float>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op)
-                      : gmres_impl<double>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op);
+                      ? gmres_impl<float>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op,
+                                          sync_end)
+                      : gmres_impl<double>(c, K, cj, y, yp, F0, ewt, b, x, m, max_restarts, tol, iters, res_norm, cnt, op,
+                                           sync_end);
     // a timed-out barrier of the Schur-coupled apply voids the solve
     if (schur_status(c)) return 2;
     return r;
