@@ -194,7 +194,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     const double beta = sqrt(*a.beta2);
     const double rn0 = beta / sqrtN;
     for (int i = threadIdx.x; i <= m; i += blockDim.x) gs[i] = i == 0 ? beta : 0.0;
-    if (threadIdx.x == 0) sc[0] = a.scale[0];
+    // the scale of U_0 (1 / beta), also for the host's back substitution
+    const double s0 = beta > 0.0 ? 1.0 / beta : 0.0;
+    if (threadIdx.x == 0) {
+        sc[0] = s0;
+        if (b == 0) a.scale[0] = s0;
+    }
     if (!isfinite(beta) || rn0 <= tol) {
         if (b == 0 && threadIdx.x == 0) {
             a.st->rnorm = rn0;
@@ -219,8 +224,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     const int q0 = r0 & ~3;
     const int h0 = a.halo_ptr[b], nh = a.halo_ptr[b + 1] - h0;
     const int nb0 = a.nbr_ptr[b], nb1 = a.nbr_ptr[b + 1];
-    // step 0's direction was written before the launch
-    for (int k = threadIdx.x; k < nh; k += blockDim.x) tl[k] = __ldcg(a.tdir + a.halo_node[h0 + k]);
+    // step 0's direction s_0 U_0 / ewt at the block's own and halo nodes
+    // (U_0 was written before the launch)
+    for (int k = threadIdx.x; k < nh; k += blockDim.x) {
+        const int node = a.halo_node[h0 + k];
+        tl[k] = (float)(s0 * (double)__ldcg(a.U + node) / a.ewt[node]);
+    }
     // the padding rows of the edge quads stay zero
     for (int k = threadIdx.x; k < 4 * nqp; k += blockDim.x) {
         Ws[k] = 0.0;
@@ -492,13 +501,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     }
 }
 
-// t = s_0 U_0 / ewt in FP32 (the cycle's first direction)
-__global__ void k_first_dir(int N, const float* __restrict__ U0, const double* __restrict__ scale,
-                            const double* __restrict__ ewt, float* __restrict__ t) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < N) t[k] = (float)(scale[0] * (double)U0[k] / ewt[k]);
-}
-
 static int fused_sync_slot(int nb) { return ((nb + 31) & ~31) + 32; }
 
 static const void* fused_kernel(int lanes, int variant) {
@@ -678,7 +680,6 @@ void fused_cycle(fvm_ctx* c, Krylov* K, double cj, const double* ewt, double* H_
     cudaStream_t s = c->stream;
     float* U = reinterpret_cast<float*>(K->U);
     if (K->tdir.n < (size_t)c->N) K->tdir.alloc(c->N);
-    fvm_launch(c, k_first_dir, grid_for(c->N, 256), 256, 0, s, c->N, U, K->scale.p, ewt, K->tdir.p);
     FusedArgs a;
     a.N = c->N;
     a.m = K->m;

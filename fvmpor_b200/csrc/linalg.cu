@@ -308,11 +308,11 @@ __global__ void k_unscale(int N, const B* __restrict__ Uj, const double* __restr
     t[k] = scale[j] * ldb(Uj, k) / ewt[k];
 }
 
-// t = (sum_i y_i s_i U_i) / ewt
+// x += (sum_i y_i s_i U_i) / ewt
 template <class B>
 __global__ void k_combine(int N, int nv, const B* __restrict__ U, size_t ld,
                           const double* __restrict__ ys, const double* __restrict__ ewt,
-                          double* __restrict__ t) {
+                          double* __restrict__ x) {
     __shared__ double coef[64];
     for (int i = threadIdx.x; i < nv; i += blockDim.x) coef[i] = ys[i];
     __syncthreads();
@@ -320,7 +320,7 @@ __global__ void k_combine(int N, int nv, const B* __restrict__ U, size_t ld,
     if (k >= N) return;
     double acc = 0.0;
     for (int i = 0; i < nv; ++i) acc += coef[i] * ldb(U + ld * i, k);
-    t[k] = acc / ewt[k];
+    x[k] += acc / ewt[k];
 }
 
 // r~ = ewt * (b - Jx) (Jx may be null -> b); U_0 = r~; out = ||r~||^2
@@ -346,11 +346,6 @@ __global__ void k_init_residual(int N, const double* __restrict__ b, const doubl
         if (threadIdx.x == 0) partial[blockIdx.x] = t;
     }
     last_block_reduce(partial, 1, counter, out);
-}
-
-__global__ void k_axpy(int N, double a, const double* __restrict__ x, double* __restrict__ y) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < N) y[k] += a * x[k];
 }
 
 __global__ void k_sub(int N, const double* __restrict__ a, const double* __restrict__ b,
@@ -501,12 +496,13 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         if (cnt) cnt->nps++;
         fvm_launch(c, k_init_residual<B>, kRedBlocks, kRedThreads, 0, s, N, K->z.p, nullptr, ewt, U,
                                                               K->partial.p, K->counter.p, K->res.p);
-        fvm_launch(c, k_set_scale, 1, 1, 0, s, K->res.p, K->scale.p, 0);
         // the assembled operator with the FP32 factor and basis: the whole
         // cycle in one persistent launch (arnoldi_fused.cu), which also takes
-        // the initial norm from K->res and decides there whether any step is
-        // needed, so the host waits once per cycle
+        // the initial norm from K->res, sets the first scale and direction
+        // and decides there whether any step is needed, so the host waits
+        // once per cycle
         const bool fused = op && sizeof(B) == sizeof(float) && K->coop_grid > 0 && fused_prepare(c, m);
+        if (!fused) fvm_launch(c, k_set_scale, 1, 1, 0, s, K->res.p, K->scale.p, 0);
         std::fill(g.begin(), g.end(), 0.0);
         if (!fused) {
             FVM_CUDA(cudaMemcpyAsync(K->host, K->res.p, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -783,8 +779,7 @@ static int gmres_impl(fvm_ctx* c, Krylov* K, double cj, const double* y, const d
         // batch copied back)
         for (int i = 0; i < kdim; ++i) K->host[i] = yv[i] * K->host[3 * (m + 2) + i];
         FVM_CUDA(cudaMemcpyAsync(K->res.p, K->host, sizeof(double) * kdim, cudaMemcpyHostToDevice, s));
-        fvm_launch(c, k_combine<B>, grid_for(N, 256), 256, 0, s, N, kdim, U, ld, K->res.p, ewt, K->t.p);
-        fvm_launch(c, k_axpy, grid_for(N, 256), 256, 0, s, N, 1.0, K->t.p, x);
+        fvm_launch(c, k_combine<B>, grid_for(N, 256), 256, 0, s, N, kdim, U, ld, K->res.p, ewt, x);
         have_x = true;
         if (conv) {
             // x is complete once the stream reaches here; a caller that reads
