@@ -699,7 +699,7 @@ extern "C" void fvm_opts_default(fvm_opts* o) {
     o->max_order = 5;
     o->krylov_dim = 30;
     o->max_restarts = 5;
-    o->eps_lin = 5e-4;
+    o->eps_lin = 3e-5;
     o->cj_refresh = 1.05;
     o->psetup_age = 1;
 }

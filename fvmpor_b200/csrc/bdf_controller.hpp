@@ -75,8 +75,12 @@ struct BdfOptions {
     // 0.05 leaves Newton iterates whose error pollutes the BDF error
     // estimate: the 30-day 3D run then takes 4246 steps with 489 error-test
     // failures, against 215 steps and none at 5e-4 (the solves then match
-    // the reference's near-exact ones; final heads agree to 2e-5).
-    double eps_lin = 5e-4;
+    // the reference's near-exact ones; final heads agree to 2e-5).  Tighter
+    // still, the estimate is cleaner and the steps longer: 152 steps at
+    // 3e-5 (1e-5: 147), and fewer Krylov iterations in all (4.5k against
+    // 5.1k) although each solve takes more; the 1M-node box goes from 340 to
+    // 199 steps, the 2D problem is unchanged.
+    double eps_lin = 3e-5;
     // preconditioner refresh: when cj has moved by more than this factor
     // since the last set-up, or after this many steps.  Every step by
     // default: a fresh block-ILU(0) set-up costs about five residual

@@ -297,7 +297,7 @@ typedef struct {
     long max_steps;
     double eps_lin;          /* Krylov tolerance factor: GMRES stops at
                                 eps_lin * 0.33 weighted units (IDA's
-                                epslin); default and 0: 5e-4, tighter
+                                epslin); default and 0: 3e-5, tighter
                                 than IDA's 0.05 because block-ILU(0) is
                                 far weaker than the reference's direct
                                 factorisation                            */

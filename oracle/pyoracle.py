@@ -308,7 +308,7 @@ def opts(**kw):
 
     o = Opts()
     o.rtol, o.atol, o.max_order, o.krylov_dim, o.max_restarts = 1e-6, 1e-6, 5, 30, 5
-    o.eps_lin, o.cj_refresh, o.psetup_age = 5e-4, 1.05, 1
+    o.eps_lin, o.cj_refresh, o.psetup_age = 3e-5, 1.05, 1
     for k, v in kw.items():
         if not hasattr(o, k):
             raise TypeError(f"unknown integrator option {k!r}")
