@@ -202,7 +202,20 @@ __device__ __forceinline__ void ilu_sweep(T* x, const T* val, const unsigned sho
                                           const unsigned short* lptr, int l0, int nlv) {
     IluRow<T, KM, UPPER> cur, nxt;
     ilu_fetch(cur, l0, nlv, val, col, rp, dg, rows, lptr);
+    const int wbase = threadIdx.x & ~31;
     for (int l = l0; l < nlv; ++l) {
+        // a warp with no row in this level or the next goes straight to the
+        // level barrier
+        const int nq_cur = lptr[l + 1] - lptr[l];
+        const int nq_nxt = l + 1 < nlv ? lptr[l + 2] - lptr[l + 1] : 0;
+        if (wbase >= nq_cur && wbase >= nq_nxt) {
+            nxt.li = -1;
+#pragma unroll
+            for (int k = 0; k < KM; ++k) nxt.c[k] = 0;
+            __syncthreads();
+            cur = nxt;
+            continue;
+        }
         // issue this level's x loads first (threads without a row read entry
         // 0 and store nothing), then fetch the next level's row while they
         // are in flight, then accumulate
