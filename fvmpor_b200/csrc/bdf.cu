@@ -303,6 +303,7 @@ struct DeviceOps {
     DevBuf<double> &ypred, &yppred, &hprev;
     DevBuf<float>& feat;
     bool f_fresh = false;          // F already holds F(t, y, y')
+    bool forked = false;           // residual() recorded the set-up's fork point
 
     int nm = 1;                    // ensemble members (per-member norms when > 1)
     // Krylov tolerance factor of an ensemble: GMRES stops on the RMS over
@@ -395,6 +396,15 @@ struct DeviceOps {
     double pred_norm() const { return pn; }
     void set_order(int k) { korder = k; err_ready = false; }
     void residual() {
+        // a set-up that follows reads only what is queued up to here (y, y',
+        // ewt, the begin-step flags; not F): it may start from this point
+        if (!c->ev_fork) {
+            FVM_CUDA(cudaStreamCreate(&c->stream2));   // blocking, as the context's stream
+            FVM_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+            FVM_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+        }
+        FVM_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+        forked = true;
         if (f_fresh) {   // the learned-iterate check already evaluated it
             f_fresh = false;
             return;
@@ -415,7 +425,26 @@ struct DeviceOps {
     // the pivot status is copied behind the factorisation and read by
     // gmres() after its wait (status 3 there)
     int psetup(double cj, double h) {
-        psetup_dev(c, cj, h, y.p, yp.p, F.p, ewt.p, o.precision);
+        if (!forked) {
+            psetup_dev(c, cj, h, y.p, yp.p, F.p, ewt.p, o.precision);
+            return 0;
+        }
+        // the set-up (difference quotients and factorisation) runs on the
+        // second stream beside the residual evaluation queued since the fork;
+        // the context's stream waits for it before the Krylov solve
+        forked = false;
+        FVM_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+        cudaStream_t s0 = c->stream;
+        c->stream = c->stream2;
+        try {
+            psetup_dev(c, cj, h, y.p, yp.p, F.p, ewt.p, o.precision);
+        } catch (...) {
+            c->stream = s0;
+            throw;
+        }
+        c->stream = s0;
+        FVM_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+        FVM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
         return 0;
     }
     int gmres(double cj, double tol, int* its, double* rn, long* nps, long* njv) {

@@ -1080,6 +1080,12 @@ extern "C" void fvm_destroy(fvm_ctx* c) {
     fvmb_destroy_krylov(c->kry[1]);
     fvmb_destroy_integ_work(c->work);
     fvmb_destroy_predictor(c->pred);
+    if (c->stream2) {
+        cudaStreamSynchronize(c->stream2);
+        cudaStreamDestroy(c->stream2);
+    }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     cudaStream_t s = c->stream;
     delete c;
     if (s) cudaStreamDestroy(s);

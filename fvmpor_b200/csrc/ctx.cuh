@@ -171,6 +171,11 @@ struct fvm_ctx {
     double rho0 = 1000.0;
     bool recompute = false;
     cudaStream_t stream = nullptr;
+    // the integrator's preconditioner set-up runs on stream2 beside the
+    // residual evaluation it does not depend on (fork at ev_fork, joined by
+    // ev_join before the Krylov solve); made on first use
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int device = 0;
 
     // host copies needed by the preconditioner set-up and the integrator
