@@ -425,7 +425,10 @@ struct DeviceOps {
     // the pivot status is copied behind the factorisation and read by
     // gmres() after its wait (status 3 there)
     int psetup(double cj, double h) {
-        if (!forked) {
+        // (with the per-category timers on, everything stays on one stream so
+        // that each category's events bracket its own kernels only)
+        if (!forked || c->tm.on) {
+            forked = false;
             psetup_dev(c, cj, h, y.p, yp.p, F.p, ewt.p, o.precision);
             return 0;
         }
