@@ -19,6 +19,10 @@
  *     result, Krylov non-convergence, zero pivot), <0 fatal (bad argument,
  *     CUDA error, missing setup).  No C++ exception crosses this boundary.
  *   - One CUDA stream per context; calls on one context are single-threaded.
+ *     Inside fvm_integrate* the preconditioner set-up runs on a second,
+ *     internal stream of the context beside the residual evaluation it does
+ *     not depend on, joined back before the Krylov solve; every call still
+ *     returns with its work ordered on the context's stream.
  *   - Every device-side wait is bounded and reports a status; nothing spins
  *     forever.
  */
