@@ -179,6 +179,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     // unrotated Hessenberg matrix (column c at Hs[64 c ..])
     double* Vs = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(tl) + round16(4 * (size_t)a.nh_max));
     double* Hs = Vs + 4 * (size_t)nqp;
+    // delayed variant: the block's rows of ewt (quad-transposed, 1 in the
+    // edge quads' padding), read by every step's scaling of W and of the
+    // next direction instead of going to L2 for them
+    double* Es = Hs + 64 * 64;
     if (threadIdx.x == 0) {
         tc05::mbar_init(mbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;");
@@ -233,7 +237,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     // the padding rows of the edge quads stay zero
     for (int k = threadIdx.x; k < 4 * nqp; k += blockDim.x) {
         Ws[k] = 0.0;
-        if constexpr (DEL) Vs[k] = 0.0;
+        if constexpr (DEL) {
+            Vs[k] = 0.0;
+            const int e = k / nqp, row = (r0 & ~3) + 4 * (k - e * nqp) + e;   // inverse of quad_pos
+            Es[k] = row >= r0 && row < r1 ? a.ewt[row] : 1.0;
+        }
     }
     __syncthreads();
     for (int j = 0;; ++j) {
@@ -272,7 +280,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
         // preconditioner: both triangular sweeps in shared memory
         ilu_sweep<float, KM, false>(x, val, col, rp, dg, lrow, lptr, 1, nl);
         ilu_sweep<float, KM, true>(x, val, col, rp, dg, urow, uptr, 0, nu);
-        for (int k = threadIdx.x; k < nr; k += blockDim.x) Ws[quad_pos(r0, nqp, r0 + k)] = a.ewt[r0 + k] * (double)x[inv[k]];
+        for (int k = threadIdx.x; k < nr; k += blockDim.x) {
+            const int qp = quad_pos(r0, nqp, r0 + k);
+            Ws[qp] = (DEL ? Es[qp] : a.ewt[r0 + k]) * (double)x[inv[k]];
+        }
         __syncthreads();
         // Hessenberg column finalised by this step (-1: none yet), the entry
         // below its diagonal, and the scale of the basis vector it finalises
@@ -422,7 +433,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
                         if (k >= 1) Uk[q] = (float)(vq - acc1[e]);
                         const double vn = Ws[qp] * rb - vcoef * vq - acc2[e];
                         Vs[qp] = vn;
-                        a.tdir[q] = (float)(vn / a.ewt[q]);
+                        a.tdir[q] = (float)(vn / Es[qp]);
                     }
                 }
             }
@@ -625,14 +636,15 @@ bool fused_prepare(fvm_ctx* c, int m) {
         P->fused_stage = round16(P->smem_stage[1]);
         // CGS2: staged factor | row order | rows of W | direction at the
         // block's nodes; the delayed variant adds the pending vector's rows
-        // and the unrotated Hessenberg matrix (64 x 64)
+        // and the unrotated Hessenberg matrix (64 x 64), then the block's
+        // rows of ewt
         // block row arrays quad-transposed: nqp quads cover any block's rows
         // from its first quad boundary
         P->fused_nqp = nr_max / 4 + 2;
         const size_t rows = 32 * (size_t)P->fused_nqp;
         const size_t base = P->fused_stage + round16(2 * (size_t)nr_max) + rows;
         P->fused_smem = base + 4 * (size_t)nh_max;
-        P->fused_smem_d = base + round16(4 * (size_t)nh_max) + rows + 8 * 64 * 64;
+        P->fused_smem_d = base + round16(4 * (size_t)nh_max) + rows + 8 * 64 * 64 + rows;
         // one thread per row quad of the largest block, whole warps
         P->fused_threads = std::min(kFusedThreads, std::max(128, ((nr_max + 3) / 4 + 1 + 31) / 32 * 32));
         int dev = 0, coop = 0, nsm = 0;
