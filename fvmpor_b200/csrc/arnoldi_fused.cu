@@ -183,6 +183,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     // edge quads' padding), read by every step's scaling of W and of the
     // next direction instead of going to L2 for them
     double* Es = Hs + 64 * 64;
+    // delayed variant: the block's node list (its rows, then its halo), for
+    // the gather of every step's direction
+    int* Hn = reinterpret_cast<int*>(Es + 4 * (size_t)nqp);
     if (threadIdx.x == 0) {
         tc05::mbar_init(mbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;");
@@ -232,6 +235,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
     // (U_0 was written before the launch)
     for (int k = threadIdx.x; k < nh; k += blockDim.x) {
         const int node = a.halo_node[h0 + k];
+        if constexpr (DEL) Hn[k] = node;
         tl[k] = (float)(s0 * (double)__ldcg(a.U + node) / a.ewt[node]);
     }
     // the padding rows of the edge quads stay zero
@@ -459,7 +463,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_arnoldi_fused(FusedArgs a)
             }
             named_barrier(1, blockDim.x - 32);
             for (int kk = threadIdx.x - 32; kk < nh; kk += blockDim.x - 32)
-                tl[kk] = __ldcg(a.tdir + a.halo_node[h0 + kk]);
+                tl[kk] = __ldcg(a.tdir + (DEL ? Hn[kk] : a.halo_node[h0 + kk]));
         } else if (threadIdx.x == 0) {
             int done = 0;
             if (hcol >= 0) {
@@ -637,14 +641,14 @@ bool fused_prepare(fvm_ctx* c, int m) {
         // CGS2: staged factor | row order | rows of W | direction at the
         // block's nodes; the delayed variant adds the pending vector's rows
         // and the unrotated Hessenberg matrix (64 x 64), then the block's
-        // rows of ewt
+        // rows of ewt and its node list
         // block row arrays quad-transposed: nqp quads cover any block's rows
         // from its first quad boundary
         P->fused_nqp = nr_max / 4 + 2;
         const size_t rows = 32 * (size_t)P->fused_nqp;
         const size_t base = P->fused_stage + round16(2 * (size_t)nr_max) + rows;
         P->fused_smem = base + 4 * (size_t)nh_max;
-        P->fused_smem_d = base + round16(4 * (size_t)nh_max) + rows + 8 * 64 * 64 + rows;
+        P->fused_smem_d = base + round16(4 * (size_t)nh_max) + rows + 8 * 64 * 64 + rows + round16(4 * (size_t)nh_max);
         // one thread per row quad of the largest block, whole warps
         P->fused_threads = std::min(kFusedThreads, std::max(128, ((nr_max + 3) / 4 + 1 + 31) / 32 * 32));
         int dev = 0, coop = 0, nsm = 0;
