@@ -58,12 +58,12 @@ CONFIG = {"workload": WORKLOAD, "rtol": 1e-6, "atol": 1e-6, "simulated_s_per_ste
 CHAIN_DRAM_BYTES = 84.0e6
 # DRAM bytes (read + write) of one k_arnoldi_fused launch, as measured by ncu
 # on the --profile-case fused workload: launches 101 (2-3 Arnoldi steps,
-# 44.4 MB read, 0.2 MB written) and 102 (a full 40-step cycle, 44.6 MB read,
-# 4.6 MB written) of the 10-day run, whose mean length (21 steps) is the
+# 44.4 MB read, 0.4 MB written) and 102 (a full 40-step cycle, 44.4 MB read,
+# 2.3 MB written) of the 10-day run, whose mean length (21 steps) is the
 # 30-day run's mean; their mean is used.  The operator and the FP32 basis stay
 # in L2 between steps, so this stays far below the algorithmic bytes, which
 # count every L2 -> SM pass.
-FUSED_DRAM_BYTES = 46.9e6
+FUSED_DRAM_BYTES = 45.7e6
 UNIT = "sim-s/wall-s"
 
 
